@@ -1,0 +1,190 @@
+"""ctypes binding of libfastgpr.so (the C ABI in include/fastgpr.h).
+
+The library is built in-tree (``build.py``) and loaded from ``_lib/``.  There
+is no fallback: if the library is missing or no CUDA device is present, every
+solve raises.  Setting FASTGPR_CHECKED=1 loads the bounds-checked build
+(``libfastgpr_checked.so``), whose kernels test every global access and
+record a violation instead of touching memory out of range.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(_HERE, "_lib")
+
+FG_OK = 0
+FG_ERR_INVALID = 1
+FG_ERR_CUDA = 2
+FG_ERR_WORKSPACE = 3
+FG_ERR_TIMEOUT = 4
+
+# Every entry point include/fastgpr.h declares (checked by the tests).
+EXPORTS = (
+    "fg_plan_create", "fg_plan_destroy", "fg_plan_workspace_bytes", "fg_plan_bind",
+    "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
+)
+
+
+class FgProblem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("shots", ctypes.c_int32),
+        ("nt", ctypes.c_int32), ("th", ctypes.c_int32),
+        ("dx", ctypes.c_float), ("dt", ctypes.c_float),
+        ("nsrc", ctypes.c_int32), ("nrx", ctypes.c_int32),
+        ("src", ctypes.POINTER(ctypes.c_int32)), ("rx", ctypes.POINTER(ctypes.c_int32)),
+        ("srcw", ctypes.POINTER(ctypes.c_float)), ("pml", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+
+class FgTuning(ctypes.Structure):
+    _fields_ = [
+        ("cols_per_thread", ctypes.c_int32), ("shots_per_warp", ctypes.c_int32),
+        ("rows_per_tile", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
+class FastGprError(RuntimeError):
+    """A libfastgpr call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__("libfastgpr error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def checked_build() -> bool:
+    return os.environ.get("FASTGPR_CHECKED", "0") not in ("", "0")
+
+
+def library_path(checked: Optional[bool] = None) -> str:
+    if checked is None:
+        checked = checked_build()
+    name = "libfastgpr_checked.so" if checked else "libfastgpr.so"
+    return os.path.join(LIB_DIR, name)
+
+
+def lib() -> ctypes.CDLL:
+    """Load libfastgpr.so once and declare the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise FastGprError(FG_ERR_INVALID, "%s is not built; run build.py (or __graft_entry__.build())" % path)
+    L = ctypes.CDLL(path)
+    vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    L.fg_plan_create.argtypes = [ctypes.POINTER(FgProblem), ctypes.POINTER(FgTuning), ctypes.POINTER(vp)]
+    L.fg_plan_create.restype = ctypes.c_int
+    L.fg_plan_destroy.argtypes = [vp]
+    L.fg_plan_destroy.restype = ctypes.c_int
+    L.fg_plan_workspace_bytes.argtypes = [vp]
+    L.fg_plan_workspace_bytes.restype = i64
+    L.fg_plan_bind.argtypes = [vp, vp, i64, vp]
+    L.fg_plan_bind.restype = ctypes.c_int
+    L.fg_coefficients.argtypes = [vp, vp, vp, i32, i32, f32, f32, i32, vp, i32, vp]
+    L.fg_coefficients.restype = ctypes.c_int
+    L.fg_forward.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.fg_forward.restype = ctypes.c_int
+    L.fg_adjoint_reference.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]
+    L.fg_adjoint_reference.restype = ctypes.c_int
+    L.fg_plan_check.argtypes = [vp, vp]
+    L.fg_plan_check.restype = ctypes.c_int
+    L.fg_last_error.argtypes = []
+    L.fg_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != FG_OK:
+        raise FastGprError(rc, lib().fg_last_error().decode(errors="replace"))
+
+
+def ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Plan:
+    """A planned solve geometry with its bound device workspace."""
+
+    def __init__(self, nx, ny, shots, nt, th, dx32, dt32, src: np.ndarray, rx: np.ndarray,
+                 srcw: np.ndarray, pml: Optional[np.ndarray], device, tuning=None):
+        L = lib()
+        self.device = torch.device(device)
+        self.nx, self.ny, self.shots, self.nt, self.th = int(nx), int(ny), int(shots), int(nt), int(th)
+        self._src = np.ascontiguousarray(src, dtype=np.int32)
+        self._rx = np.ascontiguousarray(rx, dtype=np.int32)
+        self._srcw = np.ascontiguousarray(srcw, dtype=np.float32)
+        self._pml = None if pml is None else np.ascontiguousarray(pml, dtype=np.float32)
+        self.nsrc = self._src.shape[1] if self._src.ndim == 3 else 0
+        self.nrx = self._rx.shape[1] if self._rx.ndim == 3 else 0
+        prob = FgProblem()
+        prob.nx, prob.ny, prob.shots, prob.nt, prob.th = self.nx, self.ny, self.shots, self.nt, self.th
+        prob.dx, prob.dt = float(dx32), float(dt32)
+        prob.nsrc, prob.nrx = self.nsrc, self.nrx
+        prob.src = self._src.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        prob.rx = self._rx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        prob.srcw = self._srcw.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        prob.pml = (self._pml.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+                    if self._pml is not None else ctypes.POINTER(ctypes.c_float)())
+        tune = None
+        if tuning is not None:
+            tune = FgTuning(int(tuning.get("cols_per_thread", 0)), int(tuning.get("shots_per_warp", 0)),
+                            int(tuning.get("rows_per_tile", 0)), 0)
+        handle = ctypes.c_void_p()
+        check(L.fg_plan_create(ctypes.byref(prob), ctypes.byref(tune) if tune is not None else None,
+                               ctypes.byref(handle)))
+        self._h = handle
+        nbytes = int(L.fg_plan_workspace_bytes(handle))
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        check(L.fg_plan_bind(handle, self.workspace.data_ptr(), nbytes, stream_handle(self.device)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.fg_plan_destroy(h)
+            self._h = None
+
+    def device_check(self):
+        """Synchronise and raise if a kernel recorded a device-side error."""
+        check(lib().fg_plan_check(self._h, stream_handle(self.device)))
+
+    def forward(self, er32, se32, mr32, traces, hist):
+        check(lib().fg_forward(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(traces), ptr(hist),
+                               stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
+    def adjoint_reference(self, er32, se32, mr32, hist, resid, grad_eps, grad_sig, normalize=True, norms=None):
+        check(lib().fg_adjoint_reference(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(hist), ptr(resid),
+                                         ptr(grad_eps), ptr(grad_sig), 1 if normalize else 0, ptr(norms),
+                                         stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
+
+def coefficients(er32, se32, mr32, dt32, dx32, adjoint, pitch=None):
+    """fg_coefficients into a fresh (5, nx+1, pitch) tensor."""
+    nx, ny = er32.shape
+    if pitch is None:
+        pitch = (ny + 1 + 31) // 32 * 32
+    out = torch.empty((5, nx + 1, pitch), dtype=torch.float32, device=er32.device)
+    check(lib().fg_coefficients(ptr(er32), ptr(se32), ptr(mr32), nx, ny, float(dt32), float(dx32),
+                                1 if adjoint else 0, ptr(out), pitch, stream_handle(er32.device)))
+    return out

@@ -1,0 +1,126 @@
+/*
+ * fastgpr.h -- C ABI of the B200 TMz FDTD library (libfastgpr.so).
+ *
+ * One shared library replaces the six the reference builds from
+ * src/lib/*.cu and binds through ctypes (src/__init__.py:30-221).  Where the
+ * reference launches 12 kernels and 10 device-wide synchronisations per time
+ * step from Python, this ABI takes a whole solve per call:
+ *
+ *   fg_coefficients       replaces Ucget / Ucgeta          (src/lib/uc.cu:48, :94)
+ *   fg_forward            replaces, per time step, launch_store_outputs
+ *                         (sourcereceiver.cu:40), h_fields_updates
+ *                         (fields_updates_gpu.cu:183), order1_* H
+ *                         (pml_updates_h.cu:84-661), e_fields_updates
+ *                         (fields_updates_gpu.cu:138), order1_* E
+ *                         (pml_updates_e.cu:80-633), update_hertzian_dipole
+ *                         (sourcereceiver.cu:89) and the Ez history copy
+ *                         (src/compute.py:712) -- the loop of compute.py:574-712
+ *   fg_adjoint_reference  replaces back_source (back.cu:39), the reversed
+ *                         update launches and the imaging/normalisation torch
+ *                         ops -- the loop of compute.py:1048-1180
+ *
+ * Conventions
+ *   - All array arguments are device pointers unless marked HOST.
+ *   - Every call is asynchronous on the given stream (cudaStream_t passed as
+ *     void*; NULL = legacy default stream) and returns an FG_* status; no call
+ *     synchronises the device.  fg_last_error() gives the message of the most
+ *     recent failure on the calling thread.
+ *   - The caller owns every buffer.  A plan owns only host-side tables; its
+ *     device scratch (fields, CPML auxiliaries, event tables, gradient
+ *     accumulators) lives in a caller-allocated workspace of
+ *     fg_plan_workspace_bytes() bytes bound with fg_plan_bind().
+ *   - Distinct plans may be used concurrently from different threads; one
+ *     plan must not run two solves at once (they share its workspace).
+ */
+#ifndef FASTGPR_H
+#define FASTGPR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FG_OK 0
+#define FG_ERR_INVALID 1     /* bad argument, shape or position */
+#define FG_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define FG_ERR_WORKSPACE 3   /* workspace missing or too small */
+#define FG_ERR_TIMEOUT 4     /* a bounded device-side wait gave up */
+
+/* Geometry of one model solved for `shots` shots (the reference's `step`
+ * batch).  Mirrors FDTDGrid after initialization() (src/compute.py:726-872). */
+typedef struct fg_problem {
+    int32_t nx, ny;        /* compute grid: reference G.nx (axis 0), G.ny (axis 1) */
+    int32_t shots;         /* G.step */
+    int32_t nt;            /* G.iterations */
+    int32_t th;            /* CPML cells on each side, 0 = no CPML (G.pmlthick) */
+    float dx;              /* cell size (dx == dy), float32 as the kernels see it */
+    float dt;              /* time step, float32 */
+    int32_t nsrc, nrx;     /* sources / receivers per shot */
+    const int32_t* src;    /* HOST (shots, nsrc, 3) cell indices (i, j, k), G.source */
+    const int32_t* rx;     /* HOST (shots, nrx, 3) cell indices, G.receiver */
+    const float* srcw;     /* HOST (nsrc, nt) waveform times dl/(dx dy dz) */
+    const float* pml;      /* HOST (8, th) ERA ERB ERE ERF HRA HRB HRE HRF, or NULL if th == 0 */
+} fg_problem;
+
+/* Launch shape chosen by the autotuner; NULL selects defaults. */
+typedef struct fg_tuning {
+    int32_t cols_per_thread;   /* 1, 2 or 4 columns per lane */
+    int32_t shots_per_warp;    /* 1, 2, 4 or 8 shots marched together */
+    int32_t rows_per_tile;     /* rows of one tile (>= 2) */
+    int32_t reserved;
+} fg_tuning;
+
+typedef struct fg_plan fg_plan;
+
+/* Build a plan (host tables only).  Positions with k != 0, i == nx or
+ * j == ny address the reference's dead plane / zero frame and are kept as
+ * inert (traces read 0, injections are dropped); negative or larger indices
+ * are rejected with FG_ERR_INVALID. */
+int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out);
+int fg_plan_destroy(fg_plan* plan);
+/* Device scratch a plan needs, in bytes (>= 0), or -1 on a NULL plan. */
+int64_t fg_plan_workspace_bytes(const fg_plan* plan);
+/* Attach a workspace (256-byte aligned device memory of at least
+ * fg_plan_workspace_bytes bytes) and upload the plan's tables into it. */
+int fg_plan_bind(fg_plan* plan, void* workspace, int64_t bytes, void* stream);
+
+/* Per-cell update coefficients, the reference's Ucget (adjoint == 0) or
+ * Ucgeta (adjoint != 0) (src/lib/uc.cu:11-45, :60-91).  er, se, mr: (nx, ny)
+ * float32 row-major.  out: 5 planes of (nx+1, pitch) float32 -- uE0, uE1,
+ * uE4, uH1, uH4 -- zero on the i == nx / j >= ny frame. */
+int fg_coefficients(const float* er, const float* se, const float* mr, int32_t nx, int32_t ny,
+                    float dt, float dx, int32_t adjoint, float* out, int32_t pitch, void* stream);
+
+/* Forward solve (compute.py:574-712).  er, se, mr: (nx, ny) float32.
+ * traces: (shots, nt, nrx) float32, Ez at each receiver at the start of each
+ * step.  hist: (nt, shots, nx, ny) float32 Ez after each step, or NULL. */
+int fg_forward(fg_plan* plan, const float* er, const float* se, const float* mr,
+               float* traces, float* hist, void* stream);
+
+/* Reference-mode adjoint (compute.py:1048-1180): the forward operator run in
+ * reverse time with Ucgeta's uE0, the raw residual injected at the receivers,
+ * and the imaging sums g_eps = sum_t,s (Ez[t]-Ez[t-1]) lambda and
+ * g_sig = sum_t,s Ez[t] lambda dt.  resid: (shots, nt, nrx) float32; hist
+ * from fg_forward.  grad_eps / grad_sig: (nx, ny) float32 outputs, either may
+ * be NULL.  normalize != 0 divides each by its L2 norm as the reference does;
+ * norms (HOST-visible is not required: device double[2]) receives the two L2
+ * norms when not NULL. */
+int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const float* mr,
+                         const float* hist, const float* resid, float* grad_eps, float* grad_sig,
+                         int32_t normalize, double* norms, void* stream);
+
+/* Wait for the plan's work on `stream`, then read and clear the device-side
+ * error word its kernels set (an out-of-range access caught by the checked
+ * build, or a bounded wait that gave up).  Returns FG_OK, FG_ERR_TIMEOUT or
+ * FG_ERR_INVALID.  This is the only call that synchronises. */
+int fg_plan_check(fg_plan* plan, void* stream);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* fg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTGPR_H */

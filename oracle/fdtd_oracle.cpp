@@ -1,0 +1,402 @@
+// CPU oracle for the 2-D TMz FDTD forward solver and its reference-mode adjoint.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the shipped package links or calls this
+// file; tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it
+// as the checker.  It restates, loop by loop, the kernels of the reference
+// Fast-GPR-FWI (paths relative to that project):
+//
+//   store_outputs            src/lib/sourcereceiver.cu:11-36
+//   h_fields_updates_gpu     src/lib/fields_updates_gpu.cu:47-78
+//   Order1_* (H slabs)       src/lib/pml_updates_h.cu:13-74, 129-193, 248-310, 363-426
+//   e_fields_updates_gpu     src/lib/fields_updates_gpu.cu:8-33
+//   Order1_* (E slabs)       src/lib/pml_updates_e.cu:12-77, 105-169, 223-286, 340-402
+//   Update_hertzian_dipole   src/lib/sourcereceiver.cu:59-87
+//   Back_source              src/lib/back.cu:8-37
+//   Forward loop             src/compute.py:574-712
+//   Backward loop + imaging  src/compute.py:1048-1172
+//
+// Only the TMz components are kept (Ez, Hx, Hy and the Ez/Hx/Hy CPML
+// auxiliaries); Ex, Ey, Hz and their PHI arrays stay identically zero in the
+// reference for a TMz source.  The dead k=1 plane of the reference layout is
+// dropped.  Fields are stored as (S, nx+1, ny+1) so the i=nx / j=ny frame
+// (zero coefficients in the reference, src/lib/uc.cu:19) reads as zero.
+//
+// Arithmetic is written with explicit fma() so that, compiled with
+// -ffp-contract=off, the float build rounds exactly as the CUDA kernels of the
+// package do (they use the same fused/unfused operation sequence).  The double
+// build is the FP64 oracle of the same update equations.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern "C" {
+
+// Flat description of one model with S shots.  Every array pointer refers to
+// data of the selected dtype (float when dtype==0, double when dtype==1),
+// except the int position tables.
+typedef struct {
+    int nx, ny;        // compute grid (axis 0 / axis 1 of the reference model)
+    int th;            // CPML thickness in cells on each of the 4 sides (0 = none)
+    int S;             // shots
+    int nt;            // time steps ("iterations" in the reference)
+    int nrx, nsrc;     // receivers / sources per shot
+    int dtype;         // 0 = float, 1 = double
+    double d;          // cell size used by the CPML derivative (dx == dy)
+    double dt;         // time step used in the sigma imaging condition
+    const void *uE0, *uE1, *uE4;   // (nx*ny) forward E coefficients
+    const void *uH1, *uH4;         // (nx*ny) H coefficients (uH0 == 1)
+    const void *uE0a;              // (nx*ny) reference-adjoint E coefficient
+    const void *pml;               // (8*th): ERA ERB ERE ERF HRA HRB HRE HRF
+    const int *src;                // (S*nsrc*2) (i, j); i<0 marks an inert entry
+    const void *srcw;              // (nsrc*nt) waveform already scaled by dl/(dx dy dz)
+    const int *rx;                 // (S*nrx*2) (i, j); i<0 marks an inert entry
+} OracleProblem;
+
+}  // extern "C"
+
+namespace {
+
+template <typename T> inline T fmaT(T a, T b, T c);
+template <> inline float fmaT<float>(float a, float b, float c) { return std::fmaf(a, b, c); }
+template <> inline double fmaT<double>(double a, double b, double c) { return std::fma(a, b, c); }
+
+// a*b + c*d and a*b - c*d with one of the two products fused into the add.
+// The reference is compiled by nvcc with FMA contraction on (src/Makefile:19
+// passes no -fmad flag), so each such expression rounds as one fma plus one
+// product.  ORACLE_FUSE_SECOND selects which product is fused; the default
+// fuses the first, matching the package kernels.
+template <typename T> inline T madd2(T a, T b, T c, T d) {
+#ifdef ORACLE_FUSE_SECOND
+    return fmaT<T>(c, d, a * b);
+#else
+    return fmaT<T>(a, b, c * d);
+#endif
+}
+template <typename T> inline T msub2(T a, T b, T c, T d) {
+#ifdef ORACLE_FUSE_SECOND
+    return fmaT<T>(-c, d, a * b);
+#else
+    return fmaT<T>(a, b, -(c * d));
+#endif
+}
+
+template <typename T>
+struct State {
+    int nx, ny, th, S;
+    size_t F;  // floats per shot field = (nx+1)*(ny+1)
+    std::vector<T> ez, hx, hy;
+    // CPML auxiliaries, one array per slab, compact shapes of the reference
+    // PHI arrays (pml_updates_*.cu INDEX4D_PHI*):
+    //   E x-slabs (Ez, PHI2):  (th, ny)      E y-slabs (Ez, PHI2): (nx, th)
+    //   H x-slabs (Hy, PHI1):  (th, ny)      H y-slabs (Hx, PHI1): (nx, th)
+    std::vector<T> pe_x0, pe_xm, pe_y0, pe_ym, ph_x0, ph_xm, ph_y0, ph_ym;
+    State(int nx_, int ny_, int th_, int S_) : nx(nx_), ny(ny_), th(th_), S(S_) {
+        F = (size_t)(nx + 1) * (ny + 1);
+        ez.assign(F * S, T(0)); hx.assign(F * S, T(0)); hy.assign(F * S, T(0));
+        size_t px = (size_t)S * th * ny, py = (size_t)S * nx * th;
+        pe_x0.assign(px, T(0)); pe_xm.assign(px, T(0)); pe_y0.assign(py, T(0)); pe_ym.assign(py, T(0));
+        ph_x0.assign(px, T(0)); ph_xm.assign(px, T(0)); ph_y0.assign(py, T(0)); ph_ym.assign(py, T(0));
+    }
+    inline size_t at(int s, int i, int j) const { return (size_t)s * F + (size_t)i * (ny + 1) + j; }
+};
+
+template <typename T>
+struct Coeffs {
+    const T *uE0, *uE1, *uE4, *uH1, *uH4;
+    const T *ERA, *ERB, *ERE, *ERF, *HRA, *HRB, *HRE, *HRF;
+    T d;
+    int ny;
+    inline size_t c(int i, int j) const { return (size_t)i * ny + j; }
+};
+
+// ---- H phase: h_fields_updates_gpu then Order1_{xminus,yminus,xplus,yplus} (H)
+template <typename T>
+void h_phase(State<T>& st, const Coeffs<T>& k) {
+    const int nx = st.nx, ny = st.ny, th = st.th, S = st.S;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i) {
+            for (int j = 0; j < ny; ++j) {
+                const size_t a = st.at(s, i, j);
+                const T u1 = k.uH1[k.c(i, j)];
+                // Hx: i in [1, nx), j in [0, ny)   (fields_updates_gpu.cu:162-170)
+                if (i >= 1) {
+                    const T dz = st.ez[st.at(s, i, j + 1)] - st.ez[a];
+                    st.hx[a] = msub2<T>(T(1), st.hx[a], u1, dz);
+                }
+                // Hy: i in [0, nx), j in [1, ny)   (fields_updates_gpu.cu:172-180)
+                if (j >= 1) {
+                    const T dz = st.ez[st.at(s, i + 1, j)] - st.ez[a];
+                    st.hy[a] = madd2<T>(T(1), st.hy[a], u1, dz);
+                }
+            }
+        }
+    if (th <= 0) return;
+    // slab order of G.pmls: x0, y0, xmax, ymax (compute.py:267-313 over PML.boundaryIDs)
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int j = 0; j < ny; ++j) {
+            // x0 (xminus): Hy at ii = th-1-i1 (pml_updates_h.cu:37-54)
+            for (int i1 = 0; i1 < th; ++i1) {
+                const int ii = th - 1 - i1;
+                const size_t a = st.at(s, ii, j);
+                const T dEz = (st.ez[st.at(s, ii + 1, j)] - st.ez[a]) / k.d;
+                T& phi = st.ph_x0[((size_t)s * th + i1) * ny + j];
+                const T ra1 = k.HRA[i1] - T(1);
+                const T t = madd2<T>(ra1, dEz, k.HRB[i1], phi);
+                st.hy[a] = fmaT<T>(k.uH4[k.c(ii, j)], t, st.hy[a]);
+                phi = msub2<T>(k.HRE[i1], phi, k.HRF[i1], dEz);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i) {
+            // y0 (yminus): Hx at jj = th-1-j1 (pml_updates_h.cu:273-290)
+            for (int j1 = 0; j1 < th; ++j1) {
+                const int jj = th - 1 - j1;
+                const size_t a = st.at(s, i, jj);
+                const T dEz = (st.ez[st.at(s, i, jj + 1)] - st.ez[a]) / k.d;
+                T& phi = st.ph_y0[((size_t)s * nx + i) * th + j1];
+                const T ra1 = k.HRA[j1] - T(1);
+                const T t = madd2<T>(ra1, dEz, k.HRB[j1], phi);
+                st.hx[a] = fmaT<T>(-k.uH4[k.c(i, jj)], t, st.hx[a]);
+                phi = msub2<T>(k.HRE[j1], phi, k.HRF[j1], dEz);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int j = 0; j < ny; ++j) {
+            // xmax (xplus): Hy at ii = nx-th+i1 (pml_updates_h.cu:153-171)
+            for (int i1 = 0; i1 < th; ++i1) {
+                const int ii = nx - th + i1;
+                const size_t a = st.at(s, ii, j);
+                const T dEz = (st.ez[st.at(s, ii + 1, j)] - st.ez[a]) / k.d;
+                T& phi = st.ph_xm[((size_t)s * th + i1) * ny + j];
+                const T ra1 = k.HRA[i1] - T(1);
+                const T t = madd2<T>(ra1, dEz, k.HRB[i1], phi);
+                st.hy[a] = fmaT<T>(k.uH4[k.c(ii, j)], t, st.hy[a]);
+                phi = msub2<T>(k.HRE[i1], phi, k.HRF[i1], dEz);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i) {
+            // ymax (yplus): Hx at jj = ny-th+j1 (pml_updates_h.cu:388-405)
+            for (int j1 = 0; j1 < th; ++j1) {
+                const int jj = ny - th + j1;
+                const size_t a = st.at(s, i, jj);
+                const T dEz = (st.ez[st.at(s, i, jj + 1)] - st.ez[a]) / k.d;
+                T& phi = st.ph_ym[((size_t)s * nx + i) * th + j1];
+                const T ra1 = k.HRA[j1] - T(1);
+                const T t = madd2<T>(ra1, dEz, k.HRB[j1], phi);
+                st.hx[a] = fmaT<T>(-k.uH4[k.c(i, jj)], t, st.hx[a]);
+                phi = msub2<T>(k.HRE[j1], phi, k.HRF[j1], dEz);
+            }
+        }
+}
+
+// ---- E phase: e_fields_updates_gpu then Order1_{xminus,yminus,xplus,yplus} (E)
+template <typename T>
+void e_phase(State<T>& st, const Coeffs<T>& k, const T* uE0) {
+    const int nx = st.nx, ny = st.ny, th = st.th, S = st.S;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 1; i < nx; ++i)
+            for (int j = 1; j < ny; ++j) {
+                // fields_updates_gpu.cu:124-134
+                const size_t a = st.at(s, i, j);
+                const size_t c = k.c(i, j);
+                const T dHy = st.hy[a] - st.hy[st.at(s, i - 1, j)];
+                const T dHx = st.hx[a] - st.hx[st.at(s, i, j - 1)];
+                const T e = madd2<T>(uE0[c], st.ez[a], k.uE1[c], dHy);
+                st.ez[a] = fmaT<T>(-k.uE1[c], dHx, e);
+            }
+    if (th <= 0) return;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int j = 0; j < ny; ++j) {
+            // x0 (xminus): Ez at ii = th - i2 (pml_updates_e.cu:58-76)
+            for (int i2 = 0; i2 < th; ++i2) {
+                const int ii = th - i2;
+                const size_t a = st.at(s, ii, j);
+                const T dHy = (st.hy[a] - st.hy[st.at(s, ii - 1, j)]) / k.d;
+                T& phi = st.pe_x0[((size_t)s * th + i2) * ny + j];
+                const T ra1 = k.ERA[i2] - T(1);
+                const T t = madd2<T>(ra1, dHy, k.ERB[i2], phi);
+                st.ez[a] = fmaT<T>(k.uE4[k.c(ii, j)], t, st.ez[a]);
+                phi = msub2<T>(k.ERE[i2], phi, k.ERF[i2], dHy);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i) {
+            // y0 (yminus): Ez at jj = th - j2 (pml_updates_e.cu:267-285)
+            for (int j2 = 0; j2 < th; ++j2) {
+                const int jj = th - j2;
+                const size_t a = st.at(s, i, jj);
+                const T dHx = (st.hx[a] - st.hx[st.at(s, i, jj - 1)]) / k.d;
+                T& phi = st.pe_y0[((size_t)s * nx + i) * th + j2];
+                const T ra1 = k.ERA[j2] - T(1);
+                const T t = madd2<T>(ra1, dHx, k.ERB[j2], phi);
+                st.ez[a] = fmaT<T>(-k.uE4[k.c(i, jj)], t, st.ez[a]);
+                phi = msub2<T>(k.ERE[j2], phi, k.ERF[j2], dHx);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int j = 0; j < ny; ++j) {
+            // xmax (xplus): Ez at ii = nx-th+i2 (pml_updates_e.cu:150-168)
+            for (int i2 = 0; i2 < th; ++i2) {
+                const int ii = nx - th + i2;
+                const size_t a = st.at(s, ii, j);
+                const T dHy = (st.hy[a] - st.hy[st.at(s, ii - 1, j)]) / k.d;
+                T& phi = st.pe_xm[((size_t)s * th + i2) * ny + j];
+                const T ra1 = k.ERA[i2] - T(1);
+                const T t = madd2<T>(ra1, dHy, k.ERB[i2], phi);
+                st.ez[a] = fmaT<T>(k.uE4[k.c(ii, j)], t, st.ez[a]);
+                phi = msub2<T>(k.ERE[i2], phi, k.ERF[i2], dHy);
+            }
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i) {
+            // ymax (yplus): Ez at jj = ny-th+j2 (pml_updates_e.cu:384-401)
+            for (int j2 = 0; j2 < th; ++j2) {
+                const int jj = ny - th + j2;
+                const size_t a = st.at(s, i, jj);
+                const T dHx = (st.hx[a] - st.hx[st.at(s, i, jj - 1)]) / k.d;
+                T& phi = st.pe_ym[((size_t)s * nx + i) * th + j2];
+                const T ra1 = k.ERA[j2] - T(1);
+                const T t = madd2<T>(ra1, dHx, k.ERB[j2], phi);
+                st.ez[a] = fmaT<T>(-k.uE4[k.c(i, jj)], t, st.ez[a]);
+                phi = msub2<T>(k.ERE[j2], phi, k.ERF[j2], dHx);
+            }
+        }
+}
+
+template <typename T>
+Coeffs<T> make_coeffs(const OracleProblem* p) {
+    Coeffs<T> k;
+    k.uE0 = (const T*)p->uE0; k.uE1 = (const T*)p->uE1; k.uE4 = (const T*)p->uE4;
+    k.uH1 = (const T*)p->uH1; k.uH4 = (const T*)p->uH4;
+    const T* pm = (const T*)p->pml;
+    const int th = p->th;
+    k.ERA = pm; k.ERB = pm + th; k.ERE = pm + 2 * th; k.ERF = pm + 3 * th;
+    k.HRA = pm + 4 * th; k.HRB = pm + 5 * th; k.HRE = pm + 6 * th; k.HRF = pm + 7 * th;
+    k.d = (T)p->d;
+    k.ny = p->ny;
+    return k;
+}
+
+// Forward loop, compute.py:574-712.  traces: (S, nt, nrx); hist: (nt, S, nx, ny)
+// holding Ez after each step (the reference's Ez_hist), or NULL.
+template <typename T>
+int forward_impl(const OracleProblem* p, T* traces, T* hist) {
+    const int nx = p->nx, ny = p->ny, S = p->S, nt = p->nt, nrx = p->nrx, nsrc = p->nsrc;
+    State<T> st(nx, ny, p->th, S);
+    Coeffs<T> k = make_coeffs<T>(p);
+    const T* srcw = (const T*)p->srcw;
+    for (int t = 0; t < nt; ++t) {
+        // store_outputs (sourcereceiver.cu:21-35): Ez at the start of the step
+        for (int s = 0; s < S; ++s)
+            for (int r = 0; r < nrx; ++r) {
+                const int i = p->rx[((size_t)s * nrx + r) * 2], j = p->rx[((size_t)s * nrx + r) * 2 + 1];
+                traces[((size_t)s * nt + t) * nrx + r] = (i < 0) ? T(0) : st.ez[st.at(s, i, j)];
+            }
+        h_phase<T>(st, k);
+        e_phase<T>(st, k, k.uE0);
+        // Update_hertzian_dipole (sourcereceiver.cu:68-86), polarisation z
+        for (int s = 0; s < S; ++s)
+            for (int n = 0; n < nsrc; ++n) {
+                const int i = p->src[((size_t)s * nsrc + n) * 2], j = p->src[((size_t)s * nsrc + n) * 2 + 1];
+                if (i < 0) continue;
+                const size_t a = st.at(s, i, j);
+                st.ez[a] = fmaT<T>(-k.uE4[k.c(i, j)], srcw[(size_t)n * nt + t], st.ez[a]);
+            }
+        if (hist) {
+            // Ez[iteration] = G.Ez_gpu[:, :nx, :ny, :nz]  (compute.py:712)
+            for (int s = 0; s < S; ++s)
+                for (int i = 0; i < nx; ++i)
+                    std::memcpy(hist + (((size_t)t * S + s) * nx + i) * ny, &st.ez[st.at(s, i, 0)], sizeof(T) * ny);
+        }
+    }
+    return 0;
+}
+
+// Reference adjoint, compute.py:1048-1172 with backinitialization's source =
+// receivers (compute.py:973) and Ucgeta's uE0 (uc.cu:85).  g: (S, nt, nrx)
+// residual; ge/gs: (nx, ny) UNNORMALISED imaging sums in T, accumulated as the
+// reference does (sum over shots, then add, once per step).
+template <typename T>
+int adjoint_ref_impl(const OracleProblem* p, const T* hist, const T* g, T* ge, T* gs) {
+    const int nx = p->nx, ny = p->ny, S = p->S, nt = p->nt, nrx = p->nrx;
+    State<T> st(nx, ny, p->th, S);
+    Coeffs<T> k = make_coeffs<T>(p);
+    const T* uE0a = (const T*)p->uE0a;
+    const T dt = (T)p->dt;
+    const size_t N = (size_t)nx * ny;
+    for (size_t c = 0; c < N; ++c) { ge[c] = T(0); gs[c] = T(0); }
+    for (int it = nt - 1; it >= 1; --it) {
+        // Back_source (back.cu:124-143): raw residual, no scaling
+        for (int s = 0; s < S; ++s)
+            for (int r = 0; r < nrx; ++r) {
+                const int i = p->rx[((size_t)s * nrx + r) * 2], j = p->rx[((size_t)s * nrx + r) * 2 + 1];
+                if (i < 0) continue;
+                const size_t a = st.at(s, i, j);
+                st.ez[a] = st.ez[a] - g[((size_t)s * nt + it) * nrx + r];
+            }
+        e_phase<T>(st, k, uE0a);
+        h_phase<T>(st, k);
+        // imaging (compute.py:1167-1172)
+        const T* f1 = hist + (size_t)it * S * N;
+        const T* f0 = hist + (size_t)(it - 1) * S * N;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                T se = T(0), ss = T(0);
+                for (int s = 0; s < S; ++s) {
+                    const size_t h = (size_t)s * N + (size_t)i * ny + j;
+                    const T lam = st.ez[st.at(s, i, j)];
+                    se += (f1[h] - f0[h]) * lam;
+                    ss += (f1[h] * lam) * dt;
+                }
+                ge[(size_t)i * ny + j] += se;
+                gs[(size_t)i * ny + j] += ss;
+            }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+int oracle_forward(const OracleProblem* p, void* traces, void* hist) {
+    if (!p || !traces) return -1;
+    if (p->dtype == 0) return forward_impl<float>(p, (float*)traces, (float*)hist);
+    if (p->dtype == 1) return forward_impl<double>(p, (double*)traces, (double*)hist);
+    return -2;
+}
+
+int oracle_adjoint_ref(const OracleProblem* p, const void* hist, const void* g, void* ge, void* gs) {
+    if (!p || !hist || !g || !ge || !gs) return -1;
+    if (p->dtype == 0) return adjoint_ref_impl<float>(p, (const float*)hist, (const float*)g, (float*)ge, (float*)gs);
+    if (p->dtype == 1) return adjoint_ref_impl<double>(p, (const double*)hist, (const double*)g, (double*)ge, (double*)gs);
+    return -2;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+"""The C-ABI library loads and exports every entry point include/fastgpr.h declares."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "fastgpr.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fg_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "fg_forward" in syms and "fg_adjoint_reference" in syms and "fg_coefficients" in syms
+
+
+def test_library_exports_every_declared_symbol(fg):
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    for checked in (False, True):
+        path = nat.library_path(checked)
+        assert os.path.exists(path), "library not built: %s" % path
+        lib = ctypes.CDLL(path)
+        for s in declared_symbols():
+            assert hasattr(lib, s), "%s does not export %s" % (os.path.basename(path), s)
+    assert set(declared_symbols()) == set(nat.EXPORTS)
+
+
+def test_plan_validation_without_gpu(fg):
+    """Host-side argument checks run before any device work."""
+    import numpy as np
+    import pytest
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    L = nat.lib()
+    src = np.zeros((1, 1, 3), np.int32)
+    rx = np.array([[[5, 5, 0]]], np.int32)
+    srcw = np.ones((1, 4), np.float32)
+    prob = nat.FgProblem()
+    prob.nx, prob.ny, prob.shots, prob.nt, prob.th = 8, 8, 1, 4, 0
+    prob.dx, prob.dt = 0.1, 1e-10
+    prob.nsrc, prob.nrx = 1, 1
+    prob.src = src.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    prob.rx = rx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    prob.srcw = srcw.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    h = ctypes.c_void_p()
+    assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_OK
+    assert L.fg_plan_workspace_bytes(h) > 0
+    L.fg_plan_destroy(h)
+    rx[0, 0, 0] = 9   # beyond the i == nx frame
+    assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_ERR_INVALID
+    assert b"receiver" in L.fg_last_error()
+    rx[0, 0, 0] = 8   # on the frame: inert, accepted
+    assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_OK
+    L.fg_plan_destroy(h)
+    prob.th = 5       # 2*th > nx
+    assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_ERR_INVALID
+    with pytest.raises(nat.FastGprError):
+        nat.check(nat.FG_ERR_INVALID)

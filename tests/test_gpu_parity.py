@@ -1,0 +1,204 @@
+"""GPU parity: the CUDA path against the CPU oracle (bit-exact forward) and
+against the reference's own CUDA kernels (oracle/_ref, driven by
+oracle/ref_driver.py): traces and reference-mode gradients within 1e-5
+relative L2, FP32 gradient error against the FP64 oracle stated and bounded
+by 1e-4."""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+TOL_REF = 1e-5     # relative L2 vs the reference kernels (traces, gradients)
+TOL_FP64 = 1e-4    # relative L2 of the FP32 gradient vs the FP64 oracle
+
+
+@pytest.fixture(scope="module")
+def dev():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch.device("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def refdrv():
+    from oracle import ref_driver
+    if not ref_driver.available():
+        pytest.fail("reference kernels not built: run make -C oracle ref")
+    return ref_driver
+
+
+def _cases(fg):
+    return [fg.workloads.small(), fg.workloads.small(seed=3, shots=2, nt=150, nx=40, ny=56, pml=5, nrx=6),
+            fg.workloads.config0()]
+
+
+def _run_package(fg, wl, dev, w, tuning=None, tv=False):
+    er = torch.tensor(wl.er[:, :, None], device=dev, requires_grad=True)
+    se = torch.tensor(wl.se[:, :, None], device=dev, requires_grad=True)
+    traces, dt = fg.compute(**wl.kwargs(dev, er=er, se=se, tv=tv, tuning=tuning))
+    (traces * w).sum().backward()
+    torch.cuda.synchronize()
+    return traces.detach(), er.grad[:, :, 0].detach(), se.grad[:, :, 0].detach()
+
+
+def _run_reference(refdrv, wl, dev, w):
+    kw = wl.kwargs(dev)
+    er = torch.clamp(kw["er"], min=1)
+    se = torch.clamp(kw["se"], min=0)
+    G = refdrv.setup(dev, kw["dx"], kw["ny"], kw["nx"], 1, kw["time_windows"], kw["source_location"],
+                     kw["source_step"], kw["receiver_location"], kw["receiver_step"], kw["pmlthick"],
+                     kw["source_apmlitudes"], kw["step"], er, se, kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"],
+                     kw["Fixedreceiver"])
+    rxs, hist = refdrv.forward(G)
+    ge, gs = refdrv.backward(G, er, se, kw["mr"], hist, w)
+    return G, rxs[:, 2].contiguous(), ge[:, :, 0], gs[:, :, 0]
+
+
+def test_coefficients_bit_exact_vs_reference(fg, dev, refdrv):
+    nat = helpers.native_mod()
+    for wl in _cases(fg):
+        kw = wl.kwargs(dev)
+        er = torch.clamp(kw["er"], min=1)
+        se = torch.clamp(kw["se"], min=0)
+        G = refdrv.setup(dev, kw["dx"], kw["ny"], kw["nx"], 1, kw["time_windows"], kw["source_location"],
+                         kw["source_step"], kw["receiver_location"], kw["receiver_step"], kw["pmlthick"],
+                         kw["source_apmlitudes"], kw["step"], er, se, kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"],
+                         kw["Fixedreceiver"])
+        e32 = er[:, :, 0].float().contiguous()
+        s32 = se[:, :, 0].float().contiguous()
+        m32 = kw["mr"][:, :, 0].float().contiguous()
+        mine = nat.coefficients(e32, s32, m32, float(np.float32(G.dt)), float(np.float32(G.dx)), False)
+        nx, ny = wl.nx, wl.ny
+        ref = G.coef_single   # uE0 uE1 uE4 uH0 uH1 uH4, (nx+1, ny+1, 2)
+        for k, r in ((0, 0), (1, 1), (2, 2), (3, 4), (4, 5)):
+            a = mine[k, :nx, :ny].cpu().numpy()
+            b = ref[r][:nx, :ny, 0].cpu().numpy()
+            assert np.array_equal(a, b), "coefficient plane %d differs (%d cells)" % (k, int((a != b).sum()))
+        H = refdrv.Grid()
+        for k in ("step", "device", "dx", "dy", "dz", "nx", "ny", "nz", "dt"):
+            setattr(H, k, getattr(G, k))
+        refdrv._coefficients(H, er, se, kw["mr"], adjoint=True)
+        mine_a = nat.coefficients(e32, s32, m32, float(np.float32(G.dt)), float(np.float32(G.dx)), True)
+        a = mine_a[0, :nx, :ny].cpu().numpy()
+        b = H.coef_single[0][:nx, :ny, 0].cpu().numpy()
+        mism = int((a != b).sum())
+        ulp = np.abs(a.view(np.int32).astype(np.int64) - b.view(np.int32).astype(np.int64)).max()
+        assert ulp <= 1, "adjoint uE0 differs by %d ulp in %d cells" % (ulp, mism)
+
+
+def test_setup_matches_reference(fg, dev, refdrv):
+    for wl in _cases(fg):
+        kw = wl.kwargs(dev)
+        er = torch.clamp(kw["er"], min=1)
+        se = torch.clamp(kw["se"], min=0)
+        G = refdrv.setup(dev, kw["dx"], kw["ny"], kw["nx"], 1, kw["time_windows"], kw["source_location"],
+                         kw["source_step"], kw["receiver_location"], kw["receiver_step"], kw["pmlthick"],
+                         kw["source_apmlitudes"], kw["step"], er, se, kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"],
+                         kw["Fixedreceiver"])
+        s = helpers.setup_for(wl, dev)
+        assert s.nt == G.iterations
+        assert torch.equal(s.src.cpu(), G.source[:wl.shots].cpu())
+        assert torch.equal(s.rx.cpu(), G.receiver[:wl.shots].cpu())
+        p = G.pmls[0]
+        ref_pml = np.concatenate([t.cpu().numpy() for t in (p.ERA, p.ERB, p.ERE, p.ERF, p.HRA, p.HRB, p.HRE, p.HRF)])
+        assert np.array_equal(s.profile.packed(), ref_pml)
+        d = np.float32(wl.dx)
+        w = G.waveform.cpu().numpy()
+        np.testing.assert_array_equal(s.srcw[0], (w * d) / ((d * d) * d))
+
+
+@pytest.mark.parametrize("tuning", [None, {"cols_per_thread": 2, "shots_per_warp": 1, "rows_per_tile": 7},
+                                    {"cols_per_thread": 4, "shots_per_warp": 2, "rows_per_tile": 33}])
+def test_forward_bit_exact_vs_oracle(fg, orc, dev, tuning):
+    for wl in _cases(fg)[:2]:
+        prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+        solve = fg.Solve(dev, setup, tuning=tuning, tv=False)
+        traces, hist = solve.forward(torch.tensor(wl.er, device=dev), torch.tensor(wl.se, device=dev),
+                                     torch.tensor(wl.mr, device=dev))
+        o_tr, o_hist = orc.forward(prob, np.float32)
+        np.testing.assert_array_equal(traces.cpu().numpy(), o_tr)
+        np.testing.assert_array_equal(hist.cpu().numpy(), o_hist)
+
+
+def test_adjoint_vs_oracle(fg, orc, dev):
+    for wl in _cases(fg)[:2]:
+        prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+        solve = fg.Solve(dev, setup, tv=False)
+        er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+        traces, hist = solve.forward(er, se, mr)
+        rng = np.random.default_rng(5)
+        resid = rng.standard_normal(traces.shape).astype(np.float32)
+        ge, gs = solve.gradient(er, se, mr, hist, torch.tensor(resid, device=dev), normalize=False)
+        o_tr, o_hist = orc.forward(prob, np.float32)
+        oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
+        assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
+        assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
+
+
+def test_traces_and_gradient_vs_reference_kernels(fg, dev, refdrv):
+    for wl in _cases(fg):
+        rng = np.random.default_rng(17)
+        w = torch.tensor(rng.standard_normal((wl.shots, wl.nt, wl.nrx)).astype(np.float32), device=dev)
+        tr, ge, gs = _run_package(fg, wl, dev, w)
+        G, rtr, rge, rgs = _run_reference(refdrv, wl, dev, w)
+        e_tr = helpers.rel_l2(tr.cpu().numpy(), rtr.cpu().numpy())
+        e_ge = helpers.rel_l2(ge.cpu().numpy(), rge.cpu().numpy())
+        e_gs = helpers.rel_l2(gs.cpu().numpy(), rgs.cpu().numpy())
+        print("%s vs reference kernels: traces %.3g, g_eps %.3g, g_sig %.3g" % (wl.name, e_tr, e_ge, e_gs))
+        assert e_tr <= TOL_REF and e_ge <= TOL_REF and e_gs <= TOL_REF
+
+
+def test_gradient_error_vs_fp64_oracle(fg, orc, dev):
+    for wl in _cases(fg):
+        rng = np.random.default_rng(23)
+        w = rng.standard_normal((wl.shots, wl.nt, wl.nrx)).astype(np.float32)
+        tr, ge, gs = _run_package(fg, wl, dev, torch.tensor(w, device=dev))
+        prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+        f64 = orc.coefficients_fp64(np.maximum(wl.er, 1), np.maximum(wl.se, 0), wl.mr, setup.dt32, setup.dx)
+        p64 = prob.cast(np.float64)
+        for k, v in f64.items():
+            setattr(p64, k, v)
+        er_avg = float(np.mean(np.maximum(wl.er, 1)[0, :].astype(np.float64)))
+        p64.pml = orc.cpml_fp64(setup.th, setup.dx, er_avg, 1.0, setup.dt32)
+        p64.srcw = np.zeros_like(prob.srcw, dtype=np.float64)
+        p64.srcw[0] = orc.ricker_fp64(setup.nt, setup.dt32, (wl.nt - 1.5) * wl.dt, 1.0, wl.freq, setup.dx)
+        o_tr, o_hist = orc.forward(p64, np.float64)
+        oe, os_ = orc.adjoint_reference(p64, o_hist, w, np.float64)
+        oe /= np.linalg.norm(oe)
+        os_ /= np.linalg.norm(os_)
+        e_tr = helpers.rel_l2(tr.cpu().numpy(), o_tr)
+        e_ge = helpers.rel_l2(ge.cpu().numpy(), oe)
+        e_gs = helpers.rel_l2(gs.cpu().numpy(), os_)
+        print("%s vs FP64 oracle: traces %.3g, g_eps %.3g, g_sig %.3g" % (wl.name, e_tr, e_ge, e_gs))
+        assert e_ge <= TOL_FP64 and e_gs <= TOL_FP64
+
+
+def test_tiling_invariance(fg, dev):
+    wl = fg.workloads.small(shots=5, nt=100)
+    w = torch.ones((wl.shots, wl.nt, wl.nrx), device=dev)
+    base = _run_package(fg, wl, dev, w)
+    for tuning in ({"cols_per_thread": 1, "shots_per_warp": 8, "rows_per_tile": 5},
+                   {"cols_per_thread": 2, "shots_per_warp": 4, "rows_per_tile": 48},
+                   {"cols_per_thread": 4, "shots_per_warp": 1, "rows_per_tile": 2}):
+        got = _run_package(fg, wl, dev, w, tuning=tuning)
+        assert torch.equal(got[0], base[0])
+        for a, b in zip(got[1:], base[1:]):
+            assert helpers.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6
+
+
+def test_shot_alone_equals_shot_in_batch(fg, dev):
+    wl = fg.workloads.small(shots=4, nt=100)
+    w = torch.ones((wl.shots, wl.nt, wl.nrx), device=dev)
+    tr, _, _ = _run_package(fg, wl, dev, w)
+    setup = helpers.setup_for(wl, dev)
+    for s in range(wl.shots):
+        er = torch.tensor(wl.er[:, :, None], device=dev)
+        se = torch.tensor(wl.se[:, :, None], device=dev)
+        kw = wl.kwargs(dev, er=er, se=se, tv=False, step=1, customsource=setup.src[s:s + 1].clone(),
+                       customreceiver=setup.rx[s:s + 1].clone())
+        tr1, _ = fg.compute(**kw)
+        assert torch.equal(tr1[0], tr[s])
