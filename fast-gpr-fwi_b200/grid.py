@@ -18,8 +18,6 @@ profiles are identical bit for bit:
 """
 from __future__ import annotations
 
-import ctypes
-import ctypes.util
 import math
 from dataclasses import dataclass, field
 from typing import Optional
@@ -32,11 +30,6 @@ C0 = 299792458.0
 EPS0 = 8.8541878128e-12
 MU0 = 1.25663706212e-06
 Z0 = (MU0 / EPS0) ** 0.5  # src/__init__.py:21
-
-_libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
-_libm.expf.restype = ctypes.c_float
-_libm.expf.argtypes = [ctypes.c_float]
-
 
 def cfl_dt(dx):
     """Courant limit of the 2-D TMz leapfrog, compute.py:754.
@@ -90,33 +83,30 @@ def ricker_scaled(nt: int, dt, time_window, amp, freq, d32: np.float32) -> np.nd
     """Ricker samples on whole steps times the Hertzian-dipole factor.
 
     Waveform: compute.py:351-357 with Waveform.calculate_value (:391-400),
-    float32 CPU arithmetic in the reference's op order; exp() is the C
-    library's expf, which is what the reference's 0-d CPU tensor exp calls.
-    Scaling: sourcereceiver.cu:73-75, w * dl / (dx * dy * dz) with dl = dz and
-    dx = dy = dz in float32.
+    float32 CPU tensor arithmetic in the reference's op order (torch's CPU
+    exp, whose vectorised and 0-d forms agree element for element).
+    Scaling: sourcereceiver.cu:73-75, w * dl / (dx * dy * dz) with dl = dz
+    and dx = dy = dz in float32.
     """
-    f = np.float32(float(freq))
-    a = np.float32(float(amp))
-    chi = np.float32(np.sqrt(np.float32(2.0))) / f
-    zeta = np.float32(math.pi ** 2) * (f * f)
-    z2 = np.float32(2) * zeta
-    normalise = np.float32(1) / z2
-    tw = np.float32(float(time_window))
-    d3 = (d32 * d32) * d32
-    out = np.zeros(nt, dtype=np.float32)
-    for it in range(nt):
-        t = dt * it
-        t32 = np.float32(float(t))
-        if not (t32 >= 0 and t32 <= tw):
-            continue
-        delay = t32 - chi
-        d2 = delay * delay
-        inner = (z2 * d2) - np.float32(1)
-        e = np.float32(_libm.expf(float((-zeta) * d2)))
-        v = -((z2 * inner) * e) * normalise
-        v = v * a
-        out[it] = (v * d32) / d3
-    return out
+    f32 = torch.float32
+    freq_t = torch.tensor(float(freq), dtype=f32)
+    amp_t = torch.tensor(float(amp), dtype=f32)
+    chi = torch.sqrt(torch.tensor(2.0)) / freq_t
+    zeta = (math.pi ** 2) * (freq_t ** 2)
+    z2 = 2 * zeta
+    normalise = 1 / z2
+    tw = torch.tensor(float(time_window), dtype=f32)
+    if isinstance(dt, torch.Tensor):
+        t = (dt.to(f32) * torch.arange(nt, dtype=f32))
+    else:
+        t = torch.tensor(float(dt) * np.arange(nt, dtype=np.float64), dtype=f32)
+    delay = t - chi
+    d2 = delay ** 2
+    v = -(z2 * (z2 * d2 - 1) * torch.exp(-zeta * d2)) * normalise
+    v = v * amp_t
+    v = torch.where((t >= 0) & (t <= tw), v, torch.zeros_like(v))
+    d = torch.tensor(float(d32), dtype=f32)
+    return ((v * d) / ((d * d) * d)).numpy()
 
 
 def slab_average(values: torch.Tensor) -> torch.Tensor:
