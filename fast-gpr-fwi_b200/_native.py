@@ -26,7 +26,7 @@ FG_ERR_TIMEOUT = 4
 
 # Every entry point include/fastgpr.h declares (checked by the tests).
 EXPORTS = (
-    "fg_plan_create", "fg_plan_destroy", "fg_plan_workspace_bytes", "fg_plan_bind",
+    "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_pitch", "fg_plan_workspace_bytes", "fg_plan_bind",
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
 )
 
@@ -44,9 +44,11 @@ class FgProblem(ctypes.Structure):
 
 class FgTuning(ctypes.Structure):
     _fields_ = [
-        ("cols_per_thread", ctypes.c_int32), ("shots_per_warp", ctypes.c_int32),
-        ("rows_per_tile", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("kernel", ctypes.c_int32), ("cols_per_thread", ctypes.c_int32), ("shots_per_tile", ctypes.c_int32),
+        ("rows_per_tile", ctypes.c_int32), ("warps_per_tile", ctypes.c_int32), ("stages", ctypes.c_int32),
     ]
+
+    KEYS = ("kernel", "cols_per_thread", "shots_per_tile", "rows_per_tile", "warps_per_tile", "stages")
 
 
 class FastGprError(RuntimeError):
@@ -85,6 +87,8 @@ def lib() -> ctypes.CDLL:
     L.fg_plan_create.restype = ctypes.c_int
     L.fg_plan_destroy.argtypes = [vp]
     L.fg_plan_destroy.restype = ctypes.c_int
+    L.fg_plan_hist_pitch.argtypes = [vp]
+    L.fg_plan_hist_pitch.restype = i32
     L.fg_plan_workspace_bytes.argtypes = [vp]
     L.fg_plan_workspace_bytes.restype = i64
     L.fg_plan_bind.argtypes = [vp, vp, i64, vp]
@@ -141,12 +145,15 @@ class Plan:
                     if self._pml is not None else ctypes.POINTER(ctypes.c_float)())
         tune = None
         if tuning is not None:
-            tune = FgTuning(int(tuning.get("cols_per_thread", 0)), int(tuning.get("shots_per_warp", 0)),
-                            int(tuning.get("rows_per_tile", 0)), 0)
+            unknown = set(tuning) - set(FgTuning.KEYS)
+            if unknown:
+                raise ValueError("unknown tuning keys: %s" % sorted(unknown))
+            tune = FgTuning(*[int(tuning.get(k, 0)) for k in FgTuning.KEYS])
         handle = ctypes.c_void_p()
         check(L.fg_plan_create(ctypes.byref(prob), ctypes.byref(tune) if tune is not None else None,
                                ctypes.byref(handle)))
         self._h = handle
+        self.hist_pitch = int(L.fg_plan_hist_pitch(handle))
         nbytes = int(L.fg_plan_workspace_bytes(handle))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         check(L.fg_plan_bind(handle, self.workspace.data_ptr(), nbytes, stream_handle(self.device)))

@@ -72,7 +72,8 @@ class Solve:
         traces = torch.empty((s.shots, s.nt, self.plan.nrx), dtype=torch.float32, device=self.device)
         hist = None
         if keep_history:
-            hist = torch.empty((s.nt, s.shots, s.nx, s.ny), dtype=torch.float32, device=self.device)
+            hist = torch.empty((s.nt, s.shots, s.nx, self.plan.hist_pitch), dtype=torch.float32,
+                               device=self.device)
         self.plan.forward(er32, se32, mr32, traces, hist)
         return traces, hist
 

@@ -3,11 +3,13 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/fastgpr.h"
 #include "fdtd_kernels.cuh"
+#include "fdtd_tma.cuh"
 
 using fg::Ev;
 using fg::GridDev;
@@ -42,8 +44,8 @@ struct fg_plan {
     std::vector<int32_t> src, rx;
     std::vector<float> srcw, pml;
     // tiling
-    int V, G, TI;
-    int P, TY, nb, nc, ngroups, ntiles;
+    int kernel, V, G, TI, NW, D;
+    int P, TY, Ph, nb, nc, ngroups, ntiles, bw;
     std::vector<int> chunk_row;
     std::vector<Ev> src_ev, rx_ev, inj_ev, injh_ev;
     std::vector<int> src_off, rx_off, inj_off, injh_off;
@@ -72,14 +74,16 @@ int classify(const fg_plan* p, int i, int j, int k) {
 void build_tiles(fg_plan* p) {
     p->P = (int)align_up((size_t)p->ny + 1, 32);
     p->TY = std::max(p->th, 1);
-    p->nb = (p->ny + 32 * p->V - 1) / (32 * p->V);
+    p->Ph = (int)align_up((size_t)p->ny, 4);
+    p->bw = p->kernel == 0 ? p->NW * 32 * p->V : 32 * p->V;
+    p->nb = (p->ny + p->bw - 1) / p->bw;
     p->nc = std::max(1, (p->nx + p->TI - 1) / p->TI);
     p->ngroups = (p->S + p->G - 1) / p->G;
     p->ntiles = p->ngroups * p->nc * p->nb;
     p->chunk_row.resize(p->nc + 1);
     for (int c = 0; c <= p->nc; ++c) p->chunk_row[c] = (int)((long long)c * p->nx / p->nc);
 
-    const int bw = 32 * p->V;
+    const int bw = p->bw;
     auto tile_events = [&](std::vector<Ev>& out, std::vector<int>& off, auto&& gen) {
         out.clear();
         off.assign(p->ntiles + 1, 0);
@@ -197,7 +201,7 @@ void fill_grid(fg_plan* p) {
     std::memset(&g, 0, sizeof(g));
     char* w = p->ws;
     g.nx = p->nx; g.ny = p->ny; g.P = p->P; g.th = p->th; g.TY = p->TY;
-    g.S = p->S; g.nt = p->nt; g.nrx = p->nrx;
+    g.S = p->S; g.nt = p->nt; g.nrx = p->nrx; g.Ph = p->Ph;
     g.d = p->dx; g.dt = p->dt;
     g.plane = p->plane; g.pxs = p->pxs; g.pys = p->pys;
     float* coef = (float*)(w + p->o_coef);
@@ -238,6 +242,69 @@ template <int V, int G>
 void launch_adjoint(const GridDev& g, int it, int rp, cudaStream_t st) {
     const int blocks = (g.ntiles + 3) / 4;
     fg::k_adjoint_step<V, G><<<blocks, 128, 0, st>>>(g, it, rp);
+}
+
+template <int V, int G>
+cudaError_t launch_forward_tma(const GridDev& g, int t, int nw, int D, cudaStream_t st) {
+    const int RW = nw * 32 * V + 8;
+    const size_t smem = fg::ring_smem_bytes(D, 3 + 3 * G, RW);
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(fg::k_forward_tma<V, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (attr != cudaSuccess) return attr;
+    fg::k_forward_tma<V, G><<<g.ntiles, (nw + 1) * 32, smem, st>>>(g, t, D);
+    return cudaSuccess;
+}
+template <int V, int G>
+cudaError_t launch_adjoint_tma(const GridDev& g, int it, int rp, int nw, int D, cudaStream_t st) {
+    const int RW = nw * 32 * V + 8;
+    const size_t smem = fg::ring_smem_bytes(D, 3 + 5 * G, RW);
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(fg::k_adjoint_tma<V, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (attr != cudaSuccess) return attr;
+    fg::k_adjoint_tma<V, G><<<g.ntiles, (nw + 1) * 32, smem, st>>>(g, it, rp, D);
+    return cudaSuccess;
+}
+using FwdTmaFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
+using AdjTmaFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
+template <int V>
+FwdTmaFn pick_fwd_tma_g(int G) {
+    switch (G) {
+        case 1: return launch_forward_tma<V, 1>;
+        case 2: return launch_forward_tma<V, 2>;
+        case 4: return launch_forward_tma<V, 4>;
+    }
+    return nullptr;
+}
+FwdTmaFn pick_fwd_tma(int V, int G) {
+    switch (V) {
+        case 1: return pick_fwd_tma_g<1>(G);
+        case 2: return pick_fwd_tma_g<2>(G);
+        case 4: return pick_fwd_tma_g<4>(G);
+    }
+    return nullptr;
+}
+template <int V>
+AdjTmaFn pick_adj_tma_g(int G) {
+    switch (G) {
+        case 1: return launch_adjoint_tma<V, 1>;
+        case 2: return launch_adjoint_tma<V, 2>;
+        case 4: return launch_adjoint_tma<V, 4>;
+    }
+    return nullptr;
+}
+AdjTmaFn pick_adj_tma(int V, int G) {
+    switch (V) {
+        case 1: return pick_adj_tma_g<1>(G);
+        case 2: return pick_adj_tma_g<2>(G);
+        case 4: return pick_adj_tma_g<4>(G);
+    }
+    return nullptr;
 }
 
 using FwdFn = void (*)(const GridDev&, int, cudaStream_t);
@@ -342,12 +409,30 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             delete p;
             return fail(FG_ERR_INVALID, "receiver position outside the grid");
         }
+    p->kernel = tune ? tune->kernel : 0;
     p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : 1;
-    p->G = tune && tune->shots_per_warp ? tune->shots_per_warp : std::min(4, q.shots >= 4 ? 4 : (q.shots >= 2 ? 2 : 1));
+    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile : (q.shots >= 2 ? 2 : 1);
     p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 16;
-    if (!(p->V == 1 || p->V == 2 || p->V == 4) || !(p->G == 1 || p->G == 2 || p->G == 4 || p->G == 8) || p->TI < 2) {
+    p->NW = tune && tune->warps_per_tile ? tune->warps_per_tile : 0;
+    p->D = tune && tune->stages ? tune->stages : 4;
+    if (p->kernel == 0 && p->NW == 0) {
+        // default: one band covering the row when it fits in 16 warps
+        p->NW = std::min(16, std::max(1, (q.ny + 32 * p->V - 1) / (32 * p->V)));
+    }
+    const bool ok_common = (p->V == 1 || p->V == 2 || p->V == 4) && p->TI >= 2;
+    const bool ok_k0 = p->kernel == 0 && (p->G == 1 || p->G == 2 || p->G == 4) && p->NW >= 1 && p->NW <= 16 &&
+                       p->D >= 3 && p->D <= 8;
+    const bool ok_k1 = p->kernel == 1 && (p->G == 1 || p->G == 2 || p->G == 4 || p->G == 8);
+    if (!ok_common || !(ok_k0 || ok_k1)) {
         delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning (cols_per_thread 1/2/4, shots_per_warp 1/2/4/8, rows >= 2)");
+        return fail(FG_ERR_INVALID, "unsupported tuning");
+    }
+    if (p->kernel == 0) {
+        const size_t smem = fg::ring_smem_bytes(p->D, 3 + 5 * p->G, p->NW * 32 * p->V + 8);
+        if (smem > 227 * 1024) {
+            delete p;
+            return fail(FG_ERR_INVALID, "tuning needs more than 227 KB of shared memory");
+        }
     }
     build_tiles(p);
     layout(p);
@@ -361,6 +446,8 @@ int fg_plan_destroy(fg_plan* plan) {
 }
 
 int64_t fg_plan_workspace_bytes(const fg_plan* plan) { return plan ? (int64_t)plan->total : -1; }
+
+int32_t fg_plan_hist_pitch(const fg_plan* plan) { return plan ? plan->Ph : -1; }
 
 int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     if (!p) return fail(FG_ERR_INVALID, "fg_plan_bind: NULL plan");
@@ -412,9 +499,19 @@ int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, fl
     GridDev g = p->g;
     g.traces = traces;
     g.hist = hist;
-    FwdFn fn = pick_fwd(p->V, p->G);
-    if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-    for (int t = 0; t < p->nt; ++t) fn(g, t, st);
+    if (hist) {
+        g.out_lo = (const char*)hist;
+        g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
+    }
+    if (p->kernel == 0) {
+        FwdTmaFn fn = pick_fwd_tma(p->V, p->G);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->NW, p->D, st));
+    } else {
+        FwdFn fn = pick_fwd(p->V, p->G);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = 0; t < p->nt; ++t) fn(g, t, st);
+    }
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }
@@ -433,10 +530,18 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_gacc, 0, (size_t)p->ngroups * 2 * n * sizeof(double), st));
     GridDev g = p->g;
     g.hist = const_cast<float*>(hist);
+    g.out_lo = (const char*)hist;
+    g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
     g.resid = resid;
-    AdjFn fn = pick_adj(p->V, p->G);
-    if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-    for (int it = p->nt - 1; it >= 1; --it) fn(g, it, (p->nt - 1 - it) & 1, st);
+    if (p->kernel == 0) {
+        AdjTmaFn fn = pick_adj_tma(p->V, p->G);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->NW, p->D, st));
+    } else {
+        AdjFn fn = pick_adj(p->V, p->G);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = p->nt - 1; it >= 1; --it) fn(g, it, (p->nt - 1 - it) & 1, st);
+    }
     double* sums = (double*)(p->ws + p->o_sums);
     double* partial = (double*)(p->ws + p->o_partial);
     double* nrm = norms ? norms : (double*)(p->ws + p->o_norms);

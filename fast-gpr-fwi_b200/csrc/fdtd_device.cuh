@@ -31,6 +31,7 @@ struct GridDev {
     int th;              // CPML thickness
     int TY;              // row pitch of y-slab CPML auxiliaries (>= th)
     int S, nt, nrx;      // shots, time steps, receivers per shot
+    int Ph;              // row pitch of the Ez history (floats, multiple of 4, >= ny)
     float d;             // cell size (CPML derivative divisor)
     float dt;            // time step (sigma imaging factor)
     long long plane;     // floats in one (nx+1) x P plane
@@ -56,6 +57,7 @@ struct GridDev {
     double* gacc;        // (ngroups, 2, nx, ny)
     // bounds of every buffer the kernels touch (checked builds)
     const char* ws_lo; const char* ws_hi;
+    const char* out_lo; const char* out_hi;   // the history buffer
     int* err;            // device error word
 };
 
@@ -66,6 +68,7 @@ struct GridDev {
 __device__ __forceinline__ bool in_ws(const GridDev& g, const void* p, int bytes) {
     const char* c = (const char*)p;
     if (c >= g.ws_lo && c + bytes <= g.ws_hi) return true;
+    if (g.out_lo && c >= g.out_lo && c + bytes <= g.out_hi) return true;
     atomicCAS(g.err, 0, 100);
     return false;
 }

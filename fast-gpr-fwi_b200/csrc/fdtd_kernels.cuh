@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(128) k_forward_step(const GridDev g, const int
     const int se = g.src_off[tile + 1];
     int rc = g.rx_off[tile];
     const int re = g.rx_off[tile + 1];
-    const long long hstride = (long long)nx * ny;
+    const long long hstride = (long long)nx * g.Ph;
 
     for (int i = ti.i0; i < ti.i1; ++i) {
         float cav[V], cbv[V], chv[V];
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(128) k_forward_step(const GridDev g, const int
                 st_state<V>(g, g.hy[wp] + ro + jb, hyn);
             }
             if (g.hist) {
-                float* hrow = g.hist + ((long long)t * g.S + s) * hstride + (long long)i * ny;
+                float* hrow = g.hist + ((long long)t * g.S + s) * hstride + (long long)i * g.Ph;
 #pragma unroll
                 for (int v = 0; v < V; ++v)
                     if (jb + v < ny) hrow[jb + v] = ezw[v];
@@ -336,11 +336,12 @@ __global__ void __launch_bounds__(128) k_adjoint_step(const GridDev g, const int
         }
     }
 
-    const long long hstride = (long long)nx * ny;
+    const long long hstride = (long long)nx * g.Ph;
+    const long long gstride = (long long)nx * ny;
     const float* f1b = g.hist + (long long)it * g.S * hstride;
     const float* f0b = g.hist + (long long)(it - 1) * g.S * hstride;
-    double* gae = g.gacc + (long long)ti.grp * 2 * hstride;
-    double* gas = gae + hstride;
+    double* gae = g.gacc + (long long)ti.grp * 2 * gstride;
+    double* gas = gae + gstride;
 
     for (int i = ti.i0; i < ti.i1; ++i) {
         const int r = i + 1;
@@ -431,7 +432,7 @@ __global__ void __launch_bounds__(128) k_adjoint_step(const GridDev g, const int
                     const float dzy = __fsub_rn(ezr[v], ezc[q][v]);
                     h_update<true, true, true>(g, i, j, hxn[v], hyn[v], dzx, dzy, chv[v], rd, wr);
                     // imaging, compute.py:1167-1172
-                    const long long hidx = (long long)s * hstride + (long long)i * ny + j;
+                    const long long hidx = (long long)s * hstride + (long long)i * g.Ph + j;
                     const float f1 = __ldg(f1b + hidx), f0 = __ldg(f0b + hidx);
                     acc_e[v] = __fadd_rn(acc_e[v], __fmul_rn(__fsub_rn(f1, f0), ezc[q][v]));
                     acc_s[v] = __fadd_rn(acc_s[v], __fmul_rn(__fmul_rn(f1, ezc[q][v]), g.dt));

@@ -63,12 +63,14 @@ typedef struct fg_problem {
     const float* pml;      /* HOST (8, th) ERA ERB ERE ERF HRA HRB HRE HRF, or NULL if th == 0 */
 } fg_problem;
 
-/* Launch shape chosen by the autotuner; NULL selects defaults. */
+/* Launch shape chosen by the autotuner; NULL or zero fields select defaults. */
 typedef struct fg_tuning {
-    int32_t cols_per_thread;   /* 1, 2 or 4 columns per lane */
-    int32_t shots_per_warp;    /* 1, 2, 4 or 8 shots marched together */
+    int32_t kernel;            /* 0 = TMA row-streaming tiles (default), 1 = per-warp register march */
+    int32_t cols_per_thread;   /* 1, 2 or 4 columns per thread */
+    int32_t shots_per_tile;    /* shots marched together: 1, 2 or 4 (register march also 8) */
     int32_t rows_per_tile;     /* rows of one tile (>= 2) */
-    int32_t reserved;
+    int32_t warps_per_tile;    /* TMA tiles: consumer warps, 1..16 */
+    int32_t stages;            /* TMA tiles: shared-memory ring depth, 3..8 */
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
@@ -79,6 +81,9 @@ typedef struct fg_plan fg_plan;
  * are rejected with FG_ERR_INVALID. */
 int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out);
 int fg_plan_destroy(fg_plan* plan);
+/* Row pitch (floats) of the Ez history fg_forward writes: the history is
+ * (nt, shots, nx, pitch) with columns >= ny unused.  -1 on a NULL plan. */
+int32_t fg_plan_hist_pitch(const fg_plan* plan);
 /* Device scratch a plan needs, in bytes (>= 0), or -1 on a NULL plan. */
 int64_t fg_plan_workspace_bytes(const fg_plan* plan);
 /* Attach a workspace (256-byte aligned device memory of at least
@@ -94,7 +99,8 @@ int fg_coefficients(const float* er, const float* se, const float* mr, int32_t n
 
 /* Forward solve (compute.py:574-712).  er, se, mr: (nx, ny) float32.
  * traces: (shots, nt, nrx) float32, Ez at each receiver at the start of each
- * step.  hist: (nt, shots, nx, ny) float32 Ez after each step, or NULL. */
+ * step.  hist: (nt, shots, nx, fg_plan_hist_pitch) float32 Ez after each
+ * step, or NULL. */
 int fg_forward(fg_plan* plan, const float* er, const float* se, const float* mr,
                float* traces, float* hist, void* stream);
 
