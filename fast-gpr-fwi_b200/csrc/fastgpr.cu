@@ -73,7 +73,7 @@ int classify(const fg_plan* p, int i, int j, int k) {
 
 void build_tiles(fg_plan* p) {
     p->P = (int)align_up((size_t)p->ny + 1, 32);
-    p->TY = std::max(p->th, 1);
+    p->TY = (int)align_up((size_t)std::max(p->th, 1), 4);
     p->Ph = (int)align_up((size_t)p->ny, 4);
     p->bw = p->kernel == 0 ? p->NW * 32 * p->V : 32 * p->V;
     p->nb = (p->ny + p->bw - 1) / p->bw;
@@ -246,8 +246,7 @@ void launch_adjoint(const GridDev& g, int it, int rp, cudaStream_t st) {
 
 template <int V, int G>
 cudaError_t launch_forward_tma(const GridDev& g, int t, int nw, int D, cudaStream_t st) {
-    const int RW = nw * 32 * V + 8;
-    const size_t smem = fg::ring_smem_bytes(D, 3 + 3 * G, RW);
+    const size_t smem = fg::ring_smem_bytes(D, 5 + 6 * G, fg::ring_slot_width(nw * 32 * V, g.TY), g.th);
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
@@ -259,8 +258,7 @@ cudaError_t launch_forward_tma(const GridDev& g, int t, int nw, int D, cudaStrea
 }
 template <int V, int G>
 cudaError_t launch_adjoint_tma(const GridDev& g, int it, int rp, int nw, int D, cudaStream_t st) {
-    const int RW = nw * 32 * V + 8;
-    const size_t smem = fg::ring_smem_bytes(D, 3 + 5 * G, RW);
+    const size_t smem = fg::ring_smem_bytes(D, 5 + 8 * G, fg::ring_slot_width(nw * 32 * V, g.TY), g.th);
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
@@ -427,8 +425,15 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning");
     }
+    // The row-streaming tiles keep one x-slab auxiliary row per stage; with
+    // 2*th >= nx a row lies in both x-slabs and the register march is used.
+    if (p->kernel == 0 && 2 * q.th >= q.nx) {
+        p->kernel = 1;
+        if (p->G > 8) p->G = 8;
+    }
     if (p->kernel == 0) {
-        const size_t smem = fg::ring_smem_bytes(p->D, 3 + 5 * p->G, p->NW * 32 * p->V + 8);
+        const int TY = (int)align_up((size_t)std::max(q.th, 1), 4);
+        const size_t smem = fg::ring_smem_bytes(p->D, 5 + 8 * p->G, fg::ring_slot_width(p->NW * 32 * p->V, TY), q.th);
         if (smem > 227 * 1024) {
             delete p;
             return fail(FG_ERR_INVALID, "tuning needs more than 227 KB of shared memory");

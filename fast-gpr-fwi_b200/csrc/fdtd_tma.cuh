@@ -1,21 +1,31 @@
-// Row-streaming time-step kernels: rows of state, coefficients and history
-// are moved into a shared-memory ring by cp.async.bulk (TMA bulk copies)
-// issued by a producer warp, completing on mbarriers; the consumer warps of
-// the CTA compute one row of a tile per iteration from shared memory and store
-// the new state straight to global memory.
+// Row-streaming time-step kernels: every operand of a row -- coefficient
+// rows, the old Ez/Hx/Hy rows, the CPML auxiliaries of that row and, in the
+// adjoint, the stored forward Ez rows -- is moved into a shared-memory ring by
+// cp.async.bulk (TMA bulk copies) issued by a producer warp and completing on
+// mbarriers.  The consumer warps compute one row of the tile per iteration
+// entirely from shared memory and store the new state (and new CPML
+// auxiliaries) straight to global memory, so no global load sits in the
+// dependency chain of a row.
 //
 // Tile = (shot group of G shots, row chunk [i0, i1), column band [b0, b0+W)),
-// W = (consumer warps) * 32 * V.  Each ring stage holds, for one row r, the
-// coefficient rows uE0 uE1 uH1 and, per shot, the old Ez, Hx, Hy rows (and in
-// the adjoint the two stored forward Ez rows), each with 4 halo columns on
-// either side.  The per-cell arithmetic is the same device code as the
-// register-march kernels (fdtd_device.cuh): results are bit-identical.
+// W = (consumer warps) * 32 * V.  Stage slots (SW floats each):
+//   0..4             uE0 uE1 uE4 uH1 uH4 of the row
+//   5+6q .. 10+6q    shot q: Ez, Hx, Hy, x-slab E auxiliary row, x-slab H
+//                    auxiliary row, y-slab block [E y0 | E ymax | H y0 | H ymax]
+//   5+6G+2q, +1      adjoint only: forward Ez of steps it and it-1
+// Field and coefficient slots hold columns b0-4 .. b0+W+3 (4 halo columns on
+// each side).  The per-cell arithmetic is the same operation sequence as
+// fdtd_device.cuh, so results are bit-identical to the register-march
+// kernels and to the reference.
 //
 // Forward, per row i:  H of row i (Hx written back into the stage in place),
 // consumer barrier, E of row i reading Hx_new[j-1] from the stage.
 // Adjoint, per row i:  E of row i+1 (written back into the stage in place,
 // plus the column just past the band, recomputed), consumer barrier, H of
 // row i and imaging from the stage.
+//
+// Requires 2*th < nx (a row lies in at most one x-slab); the plan falls back
+// to the register-march kernels otherwise.
 #pragma once
 
 #include "fdtd_device.cuh"
@@ -88,30 +98,40 @@ __device__ __forceinline__ bool wait_bounded(const GridDev& g, uint64_t* bar, ui
 }
 
 struct Ring {
-    float* base;      // D stages of SROWS rows of RW floats
+    float* base;      // D stages of SROWS slots of SW floats
     uint64_t* full;   // D barriers, count 1 (+tx)
     uint64_t* empty;  // D barriers, count = consumer warps
     volatile int* abort_flag;
-    int D, SROWS, RW;
-    __device__ __forceinline__ float* row(int n, int k) const { return base + ((long long)(n % D) * SROWS + k) * RW; }
+    float* pml;       // (8, th) CPML vectors
+    int D, SROWS, SW;
+    __device__ __forceinline__ float* row(int n, int k) const { return base + ((long long)(n % D) * SROWS + k) * SW; }
 };
 
-// Carve the dynamic shared memory: barriers first (8-byte aligned), then the
-// ring at a 128-byte boundary.
-__device__ __forceinline__ Ring carve_ring(unsigned char* smem, int D, int SROWS, int RW) {
+__host__ __device__ inline int ring_slot_width(int W, int TY) {
+    const int rw = W + 8;
+    const int yw = 4 * TY;
+    return rw > yw ? rw : yw;
+}
+__host__ __device__ inline size_t ring_head_bytes(int D, int th) {
+    return 128 * ((2 * (size_t)D * 8 + 16 + 8 * (size_t)th * 4 + 127) / 128);
+}
+__host__ __device__ inline size_t ring_smem_bytes(int D, int SROWS, int SW, int th) {
+    return ring_head_bytes(D, th) + (size_t)D * SROWS * SW * sizeof(float);
+}
+
+// Carve the dynamic shared memory: barriers, abort flag and CPML vectors,
+// then the ring at a 128-byte boundary.
+__device__ __forceinline__ Ring carve_ring(unsigned char* smem, int D, int SROWS, int SW, int th) {
     Ring R;
     R.full = reinterpret_cast<uint64_t*>(smem);
     R.empty = R.full + D;
     R.abort_flag = reinterpret_cast<volatile int*>(R.empty + D);
-    R.base = reinterpret_cast<float*>(smem + 128 * ((2 * D * 8 + 16 + 127) / 128));
+    R.pml = reinterpret_cast<float*>(smem + 2 * D * 8 + 16);
+    R.base = reinterpret_cast<float*>(smem + ring_head_bytes(D, th));
     R.D = D;
     R.SROWS = SROWS;
-    R.RW = RW;
+    R.SW = SW;
     return R;
-}
-
-__host__ __device__ inline size_t ring_smem_bytes(int D, int SROWS, int RW) {
-    return 128 * ((2 * (size_t)D * 8 + 16 + 127) / 128) + (size_t)D * SROWS * RW * sizeof(float);
 }
 
 struct TileTma {
@@ -135,9 +155,23 @@ __device__ __forceinline__ TileTma tma_tile(const GridDev& g, int W) {
     return t;
 }
 
+// x-slab membership of row r for the E (1..th, nx-th..nx-1) and H
+// (0..th-1, nx-th..nx-1) auxiliaries: returns the auxiliary row index
+// slab*th + k, or -1.
+__device__ __forceinline__ int ex_row(const GridDev& g, int r) {
+    if (g.th <= 0 || r >= g.nx) return -1;
+    if (r >= 1 && r <= g.th) return g.th - r;
+    if (r >= g.nx - g.th) return g.th + (r - (g.nx - g.th));
+    return -1;
+}
+__device__ __forceinline__ int hx_row(const GridDev& g, int r) {
+    if (g.th <= 0 || r >= g.nx) return -1;
+    if (r <= g.th - 1) return g.th - 1 - r;
+    if (r >= g.nx - g.th) return g.th + (r - (g.nx - g.th));
+    return -1;
+}
+
 // Producer: stream rows r_first..r_last of the tile into the ring.
-// Stage rows: 0 uE0, 1 uE1, 2 uH1, then per shot q: 3+3q Ez, 4+3q Hx, 5+3q Hy,
-// and for the adjoint 3+3G+2q Ez_fwd[it], 4+3G+2q Ez_fwd[it-1].
 template <int G, bool ADJ>
 __device__ void tma_producer(const GridDev& g, const Ring& R, const TileTma& T, int r_first, int r_last, int rp,
                              int it) {
@@ -145,6 +179,7 @@ __device__ void tma_producer(const GridDev& g, const Ring& R, const TileTma& T, 
     const uint32_t seg = (uint32_t)(T.hi - T.lo) * 4u;
     const int hw_hi = min(T.b0 + T.W, g.Ph);
     const uint32_t hseg = (uint32_t)max(hw_hi - T.b0, 0) * 4u;
+    const uint32_t yseg = (uint32_t)g.TY * 4u;
     int issued = 0;
     for (int r = r_first; r <= r_last; ++r) {
         const int n = r - r_first;
@@ -152,31 +187,49 @@ __device__ void tma_producer(const GridDev& g, const Ring& R, const TileTma& T, 
             if (!wait_bounded(g, &R.empty[n % R.D], ((n / R.D) - 1) & 1, R.abort_flag, ERR_WAIT_EMPTY)) break;
         }
         fence_proxy_async();
-        int rows = 3;
-        for (int q = 0; q < G; ++q) rows += (s0 + q < g.S) ? 3 : 0;
+        const int ek = ex_row(g, r), hk = hx_row(g, r);
+        const bool ypsi = g.th > 0 && r < g.nx;
         const bool hrow = ADJ && r >= T.i0 && r < T.i1 && r < g.nx;
-        uint32_t bytes = seg * rows;
-        if (hrow)
-            for (int q = 0; q < G; ++q)
-                if (s0 + q < g.S) bytes += 2 * hseg;
+        int nsh = 0;
+        for (int q = 0; q < G; ++q) nsh += (s0 + q < g.S) ? 1 : 0;
+        uint32_t per_shot = 3 * seg + (ek >= 0 ? seg : 0) + (hk >= 0 ? seg : 0) + (ypsi ? 4 * yseg : 0) +
+                            (hrow ? 2 * hseg : 0);
         uint64_t* bar = &R.full[n % R.D];
-        mbar_expect_tx(bar, bytes);
+        mbar_expect_tx(bar, 5 * seg + nsh * per_shot);
         const long long ro = (long long)r * g.P + T.lo;
         bulk_g2s(R.row(n, 0) + T.soff, g.ca + ro, seg, bar);
         bulk_g2s(R.row(n, 1) + T.soff, g.cb + ro, seg, bar);
-        bulk_g2s(R.row(n, 2) + T.soff, g.ch + ro, seg, bar);
+        bulk_g2s(R.row(n, 2) + T.soff, g.cd + ro, seg, bar);
+        bulk_g2s(R.row(n, 3) + T.soff, g.ch + ro, seg, bar);
+        bulk_g2s(R.row(n, 4) + T.soff, g.ci + ro, seg, bar);
         for (int q = 0; q < G; ++q) {
             const int s = s0 + q;
             if (s >= g.S) continue;
+            const int b = 5 + 6 * q;
             const long long so = (long long)s * g.plane + ro;
-            bulk_g2s(R.row(n, 3 + 3 * q) + T.soff, g.ez[rp] + so, seg, bar);
-            bulk_g2s(R.row(n, 4 + 3 * q) + T.soff, g.hx[rp] + so, seg, bar);
-            bulk_g2s(R.row(n, 5 + 3 * q) + T.soff, g.hy[rp] + so, seg, bar);
+            bulk_g2s(R.row(n, b + 0) + T.soff, g.ez[rp] + so, seg, bar);
+            bulk_g2s(R.row(n, b + 1) + T.soff, g.hx[rp] + so, seg, bar);
+            bulk_g2s(R.row(n, b + 2) + T.soff, g.hy[rp] + so, seg, bar);
+            if (ek >= 0)
+                bulk_g2s(R.row(n, b + 3) + T.soff, g.pex[rp] + (long long)s * g.pxs + (long long)ek * g.P + T.lo, seg,
+                         bar);
+            if (hk >= 0)
+                bulk_g2s(R.row(n, b + 4) + T.soff, g.phx[rp] + (long long)s * g.pxs + (long long)hk * g.P + T.lo, seg,
+                         bar);
+            if (ypsi) {
+                float* yb = R.row(n, b + 5);
+                const long long y0 = (long long)s * g.pys + (long long)r * g.TY;
+                const long long y1 = (long long)s * g.pys + (long long)(g.nx + 1 + r) * g.TY;
+                bulk_g2s(yb, g.pey[rp] + y0, yseg, bar);
+                bulk_g2s(yb + g.TY, g.pey[rp] + y1, yseg, bar);
+                bulk_g2s(yb + 2 * g.TY, g.phy[rp] + y0, yseg, bar);
+                bulk_g2s(yb + 3 * g.TY, g.phy[rp] + y1, yseg, bar);
+            }
             if (hrow) {
                 const long long ho = (((long long)it * g.S + s) * g.nx + r) * g.Ph + T.b0;
                 const long long hs = (long long)g.S * g.nx * g.Ph;
-                bulk_g2s(R.row(n, 3 + 3 * G + 2 * q) + 4, g.hist + ho, hseg, bar);
-                bulk_g2s(R.row(n, 4 + 3 * G + 2 * q) + 4, g.hist + ho - hs, hseg, bar);
+                bulk_g2s(R.row(n, 5 + 6 * G + 2 * q) + 4, g.hist + ho, hseg, bar);
+                bulk_g2s(R.row(n, 6 + 6 * G + 2 * q) + 4, g.hist + ho - hs, hseg, bar);
             }
         }
         ++issued;
@@ -204,6 +257,126 @@ __device__ __forceinline__ void lds(float (&x)[V], const float* p) {
     }
 }
 
+// One HORIPML correction with the coefficient vectors in shared memory.
+template <bool PLUS>
+__device__ __forceinline__ float cpml_s(float f, float deriv, float u4, float& psi, const float* R, int th, int k) {
+    const float ra1 = __fsub_rn(R[k], 1.0f);
+    const float t = madd2(ra1, deriv, R[th + k], psi);
+    const float out = __fmaf_rn(PLUS ? u4 : -u4, t, f);
+    psi = msub2(R[2 * th + k], psi, R[3 * th + k], deriv);
+    return out;
+}
+
+// Global destinations of one shot's new CPML auxiliaries (parity wp).
+struct PsiOut {
+    float* ex;   // E x-slab auxiliary row of this row (NULL if none) -- indexed by column j
+    float* ey0;  // E y0 / ymax auxiliaries of this row -- indexed by k
+    float* eym;
+    float* hx;   // H x-slab auxiliary row
+    float* hy0;
+    float* hym;
+};
+__device__ __forceinline__ PsiOut psi_out(const GridDev& g, int wp, int s, int r) {
+    PsiOut o;
+    const int ek = ex_row(g, r), hk = hx_row(g, r);
+    o.ex = ek >= 0 ? g.pex[wp] + (long long)s * g.pxs + (long long)ek * g.P : nullptr;
+    o.hx = hk >= 0 ? g.phx[wp] + (long long)s * g.pxs + (long long)hk * g.P : nullptr;
+    const long long y0 = (long long)s * g.pys + (long long)r * g.TY;
+    const long long y1 = (long long)s * g.pys + (long long)(g.nx + 1 + r) * g.TY;
+    o.ey0 = g.pey[wp] + y0;
+    o.eym = g.pey[wp] + y1;
+    o.hy0 = g.phy[wp] + y0;
+    o.hym = g.phy[wp] + y1;
+    return o;
+}
+
+// E update of cell (i, j), operands in shared memory (see e_update).
+//   pE: the row's x-slab E auxiliary slot (indexed by smem column c)
+//   yp: the row's y-slab block
+template <bool STORE>
+__device__ __forceinline__ float e_cell_s(const GridDev& g, const float* pml, int i, int j, int c, float ez, float dhy,
+                                          float dhx, float ca, float cb, float cd, const float* pE, const float* yp,
+                                          const PsiOut& o) {
+    if (i >= 1 && j >= 1) ez = __fmaf_rn(-cb, dhx, madd2(ca, ez, cb, dhy));
+    const int th = g.th;
+    if (th > 0) {
+        const int nx = g.nx, ny = g.ny, TY = g.TY;
+        if (i >= 1 && i <= th) {
+            float psi = pE[c];
+            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, th - i);
+            if (STORE) __stcg(o.ex + j, psi);
+        }
+        if (j >= 1 && j <= th) {
+            const int k = th - j;
+            float psi = yp[k];
+            ez = cpml_s<false>(ez, __fdiv_rn(dhx, g.d), cd, psi, pml, th, k);
+            if (STORE) __stcg(o.ey0 + k, psi);
+        }
+        if (i >= nx - th) {
+            float psi = pE[c];
+            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, i - (nx - th));
+            if (STORE) __stcg(o.ex + j, psi);
+        }
+        if (j >= ny - th) {
+            const int k = j - (ny - th);
+            float psi = yp[TY + k];
+            ez = cpml_s<false>(ez, __fdiv_rn(dhx, g.d), cd, psi, pml, th, k);
+            if (STORE) __stcg(o.eym + k, psi);
+        }
+    }
+    return ez;
+}
+
+// H update of cell (i, j), operands in shared memory (see h_update).
+template <bool STORE, bool DO_HX, bool DO_HY>
+__device__ __forceinline__ void h_cell_s(const GridDev& g, const float* pml, int i, int j, int c, float& hx, float& hy,
+                                         float dzx, float dzy, float ch, float ci, const float* pH, const float* yp,
+                                         const PsiOut& o) {
+    if (DO_HX && i >= 1) hx = msub2(1.0f, hx, ch, dzx);
+    if (DO_HY && j >= 1) hy = madd2(1.0f, hy, ch, dzy);
+    const int th = g.th;
+    if (th > 0) {
+        const int nx = g.nx, ny = g.ny, TY = g.TY;
+        const float* HR = pml + 4 * th;
+        if (DO_HY && i <= th - 1) {
+            float psi = pH[c];
+            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, th - 1 - i);
+            if (STORE) __stcg(o.hx + j, psi);
+        }
+        if (DO_HX && j <= th - 1) {
+            const int k = th - 1 - j;
+            float psi = yp[2 * TY + k];
+            hx = cpml_s<false>(hx, __fdiv_rn(dzx, g.d), ci, psi, HR, th, k);
+            if (STORE) __stcg(o.hy0 + k, psi);
+        }
+        if (DO_HY && i >= nx - th) {
+            float psi = pH[c];
+            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, i - (nx - th));
+            if (STORE) __stcg(o.hx + j, psi);
+        }
+        if (DO_HX && j >= ny - th) {
+            const int k = j - (ny - th);
+            float psi = yp[3 * TY + k];
+            hx = cpml_s<false>(hx, __fdiv_rn(dzx, g.d), ci, psi, HR, th, k);
+            if (STORE) __stcg(o.hym + k, psi);
+        }
+    }
+}
+
+// Shared set-up of both kernels: barriers, CPML vectors, role split.
+__device__ __forceinline__ void ring_init(const GridDev& g, const Ring& R, int nw) {
+    for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) R.pml[k] = g.pml[k];
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < R.D; ++k) {
+            mbar_init(&R.full[k], 1);
+            mbar_init(&R.empty[k], nw);
+        }
+        *R.abort_flag = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // Forward step
 // ---------------------------------------------------------------------------
@@ -212,34 +385,27 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int nw = (blockDim.x >> 5) - 1;      // consumer warps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int W = nw * 32 * V, RW = W + 8;
-    const int SROWS = 3 + 3 * G;
-    const Ring R = carve_ring(smem, D, SROWS, RW);
+    const int W = nw * 32 * V;
+    const int SROWS = 5 + 6 * G;
+    const Ring R = carve_ring(smem, D, SROWS, ring_slot_width(W, g.TY), g.th);
     const TileTma T = tma_tile(g, W);
     if (T.grp * G >= g.S) return;
     const int rp = t & 1, wp = rp ^ 1;
     const int r_first = T.i0 >= 1 ? T.i0 - 1 : T.i0, r_last = T.i1;
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < D; ++k) {
-            mbar_init(&R.full[k], 1);
-            mbar_init(&R.empty[k], nw);
-        }
-        *R.abort_flag = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
+    ring_init(g, R, nw);
     if (warp == nw) {
         if (lane == 0) tma_producer<G, false>(g, R, T, r_first, r_last, rp, 0);
         return;
     }
 
-    const int nx = g.nx, ny = g.ny, P = g.P;
+    const int ny = g.ny, P = g.P;
     const int tid = threadIdx.x;           // consumer thread index
     const int c0 = 4 + tid * V;            // smem column of this thread's first cell
     const int jb = T.b0 + tid * V;         // its global column
     const int s0 = T.grp * G;
     const int ncons = nw * 32;
-    const long long hstride = (long long)nx * g.Ph;
+    const long long hstride = (long long)g.nx * g.Ph;
+    const float* pml = R.pml;
 
     float hyu[G][V];
 #pragma unroll
@@ -252,21 +418,21 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
         wait_bounded(g, &R.full[0], 0, R.abort_flag, ERR_WAIT_FULL);
         wait_bounded(g, &R.full[1 % D], (1 / D) & 1, R.abort_flag, ERR_WAIT_FULL);
         const int ih = T.i0 - 1;
-        const float* chr = R.row(0, 2);
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             if (s0 + q >= g.S) continue;
-            const PsiShot rd = psi_shot(g, rp, s0 + q);
-            const float* ezh = R.row(0, 3 + 3 * q);
-            const float* hyh = R.row(0, 5 + 3 * q);
-            const float* ez0 = R.row(1, 3 + 3 * q);
+            const int b = 5 + 6 * q;
+            const float* ezh = R.row(0, b);
+            const float* hyh = R.row(0, b + 2);
+            const float* ez0 = R.row(1, b);
+            const PsiOut o = psi_out(g, wp, s0 + q, ih);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int j = jb + v;
-                float hx_unused = 0.f, hy = hyh[c0 + v];
+                const int j = jb + v, c = c0 + v;
+                float hx_unused = 0.f, hy = hyh[c];
                 if (j < ny)
-                    h_update<false, false, true>(g, ih, j, hx_unused, hy, 0.f, __fsub_rn(ez0[c0 + v], ezh[c0 + v]),
-                                                 chr[c0 + v], rd, rd);
+                    h_cell_s<false, false, true>(g, pml, ih, j, c, hx_unused, hy, 0.f, __fsub_rn(ez0[c], ezh[c]),
+                                                 R.row(0, 3)[c], R.row(0, 4)[c], R.row(0, b + 4), R.row(0, b + 5), o);
                 hyu[q][v] = hy;
             }
         }
@@ -286,39 +452,43 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
         wait_bounded(g, &R.full[(n + 1) % D], ((n + 1) / D) & 1, R.abort_flag, ERR_WAIT_FULL);
         const float* car = R.row(n, 0);
         const float* cbr = R.row(n, 1);
-        const float* chr = R.row(n, 2);
+        const float* cdr = R.row(n, 2);
+        const float* chr = R.row(n, 3);
+        const float* cir = R.row(n, 4);
         float hyn[G][V];
         // --- H of row i
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             if (s0 + q >= g.S) continue;
             const int s = s0 + q;
-            const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-            const float* ezc = R.row(n, 3 + 3 * q);
-            float* hxr = R.row(n, 4 + 3 * q);
-            const float* hyr = R.row(n, 5 + 3 * q);
-            const float* ezn = R.row(n + 1, 3 + 3 * q);
+            const int b = 5 + 6 * q;
+            const PsiOut o = psi_out(g, wp, s, i);
+            const float* ezc = R.row(n, b);
+            float* hxr = R.row(n, b + 1);
+            const float* hyr = R.row(n, b + 2);
+            const float* pH = R.row(n, b + 4);
+            const float* yp = R.row(n, b + 5);
+            const float* ezn = R.row(n + 1, b);
             float ez[V + 1], en[V], hx[V], hy[V], ch[V];
             lds<V>(en, ezn + c0);
             lds<V>(hx, hxr + c0);
             lds<V>(hy, hyr + c0);
             lds<V>(ch, chr + c0);
 #pragma unroll
-            for (int v = 0; v < V; ++v) ez[v] = ezc[c0 + v];
-            ez[V] = ezc[c0 + V];
+            for (int v = 0; v <= V; ++v) ez[v] = ezc[c0 + v];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const int j = jb + v;
                 if (j < ny)
-                    h_update<true, true, true>(g, i, j, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
-                                               __fsub_rn(en[v], ez[v]), ch[v], rd, wr);
+                    h_cell_s<true, true, true>(g, pml, i, j, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
+                                               __fsub_rn(en[v], ez[v]), ch[v], cir[c0 + v], pH, yp, o);
                 hyn[q][v] = hy[v];
             }
-            // Hx of the column left of the band: from the old state, read-only auxiliaries
+            // Hx of the column left of the band: from the old state, auxiliaries read only
             if (tid == 0 && T.b0 > 0) {
                 float hxl = hxr[3], hy_unused = 0.f;
-                h_update<false, true, false>(g, i, T.b0 - 1, hxl, hy_unused, __fsub_rn(ez[0], ezc[3]), 0.f, chr[3],
-                                             rd, rd);
+                h_cell_s<false, true, false>(g, pml, i, T.b0 - 1, 3, hxl, hy_unused, __fsub_rn(ez[0], ezc[3]), 0.f,
+                                             chr[3], cir[3], pH, yp, o);
                 hxr[3] = hxl;
             }
 #pragma unroll
@@ -330,9 +500,12 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
         for (int q = 0; q < G; ++q) {
             if (s0 + q >= g.S) continue;
             const int s = s0 + q;
-            const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-            const float* ezc = R.row(n, 3 + 3 * q);
-            const float* hxr = R.row(n, 4 + 3 * q);
+            const int b = 5 + 6 * q;
+            const PsiOut o = psi_out(g, wp, s, i);
+            const float* ezc = R.row(n, b);
+            const float* hxr = R.row(n, b + 1);
+            const float* pE = R.row(n, b + 3);
+            const float* yp = R.row(n, b + 5);
             float ez[V], hx[V], ca[V], cb[V];
             lds<V>(ez, ezc + c0);
             lds<V>(hx, hxr + c0);
@@ -346,8 +519,8 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
                 ezw[v] = ez[v];
                 if (j < ny) {
                     const float hxl = (v > 0) ? hx[(v + V - 1) % V] : hxl0;
-                    ezw[v] = e_update<true>(g, i, j, ez[v], __fsub_rn(hyn[q][v], hyu[q][v]), __fsub_rn(hx[v], hxl),
-                                            ca[v], cb[v], rd, wr);
+                    ezw[v] = e_cell_s<true>(g, pml, i, j, c0 + v, ez[v], __fsub_rn(hyn[q][v], hyu[q][v]),
+                                            __fsub_rn(hx[v], hxl), ca[v], cb[v], cdr[c0 + v], pE, yp, o);
                 }
             }
             while (sc < se) {
@@ -355,10 +528,8 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
                 if (e.x != i || e.y != q) break;
 #pragma unroll
                 for (int v = 0; v < V; ++v)
-                    if (jb + v == e.z) {
-                        const float cd = ldc1(g, g.cd + (long long)i * P + e.z);
-                        ezw[v] = __fmaf_rn(-cd, ldc1(g, g.srcw + (long long)e.w * g.nt + t), ezw[v]);
-                    }
+                    if (jb + v == e.z)
+                        ezw[v] = __fmaf_rn(-cdr[c0 + v], __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
                 ++sc;
             }
             if (jb < P) {
@@ -393,21 +564,26 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
 // Reference-mode adjoint step
 // ---------------------------------------------------------------------------
 
-// E_new of one row of one shot for this thread's columns, written back into
-// the stage's Ez row.  hyp: the stage row holding Hy_old of row r-1 (NULL when
-// r == 0).  STORE selects whether the CPML auxiliaries are written (owned
-// rows).  Events consumed from *cur.
+// E_new of row r of one shot for this thread's columns, written back into the
+// stage's Ez slot.  sr: stage slot base of this shot in row r's stage; hyp:
+// Hy_old of row r-1 (NULL when r == 0).  Injection events consumed from *cur.
 template <int V>
-__device__ __forceinline__ void adj_e_row(const GridDev& g, int r, int q, int s, int jb, int c0, float* ezr,
-                                          const float* hxr, const float* hyr, const float* hyp, const float* car,
-                                          const float* cbr, const PsiShot& rd, const PsiShot& wr, bool store,
+__device__ __forceinline__ void adj_e_row(const GridDev& g, const Ring& R, int nr, int r, int q, int s, int jb,
+                                          int c0, const float* hyp, const PsiOut& o, bool store,
                                           const float* resid_t, int& cur, int end) {
+    const int b = 5 + 6 * q;
+    float* ezr = R.row(nr, b);
+    const float* hxr = R.row(nr, b + 1);
+    const float* hyr = R.row(nr, b + 2);
+    const float* pE = R.row(nr, b + 3);
+    const float* yp = R.row(nr, b + 5);
+    const float* cdr = R.row(nr, 2);
     float ez[V], hx[V], hy[V], hu[V], ca[V], cb[V];
     lds<V>(ez, ezr + c0);
     lds<V>(hx, hxr + c0);
     lds<V>(hy, hyr + c0);
-    lds<V>(ca, car + c0);
-    lds<V>(cb, cbr + c0);
+    lds<V>(ca, R.row(nr, 0) + c0);
+    lds<V>(cb, R.row(nr, 1) + c0);
     if (hyp) {
         lds<V>(hu, hyp + c0);
     } else {
@@ -430,22 +606,24 @@ __device__ __forceinline__ void adj_e_row(const GridDev& g, int r, int q, int s,
         out[v] = ez[v];
         if (j < g.ny) {
             const float hxl = (v > 0) ? hx[(v + V - 1) % V] : hxl0;
-            out[v] = store ? e_update<true>(g, r, j, ez[v], __fsub_rn(hy[v], hu[v]), __fsub_rn(hx[v], hxl), ca[v],
-                                            cb[v], rd, wr)
-                           : e_update<false>(g, r, j, ez[v], __fsub_rn(hy[v], hu[v]), __fsub_rn(hx[v], hxl), ca[v],
-                                             cb[v], rd, rd);
+            const float dhy = __fsub_rn(hy[v], hu[v]), dhx = __fsub_rn(hx[v], hxl);
+            out[v] = store ? e_cell_s<true>(g, R.pml, r, j, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], cdr[c0 + v], pE,
+                                            yp, o)
+                           : e_cell_s<false>(g, R.pml, r, j, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], cdr[c0 + v], pE,
+                                             yp, o);
         }
     }
 #pragma unroll
     for (int v = 0; v < V; ++v) ezr[c0 + v] = out[v];
 }
 
-// E_new of the column just past the band (be), from the stage (old values),
-// with the halo-column injections of row r.
-__device__ __forceinline__ void adj_e_halo(const GridDev& g, int r, int q, int s, int be, int cbe, float* ezr,
-                                           const float* hxr, const float* hyr, const float* hyp, const float* car,
-                                           const float* cbr, const PsiShot& rd, const float* resid_t, int& cur,
+// E_new of the column just past the band (be) of row r, from the stage (old
+// values), with the halo-column injections of row r.
+__device__ __forceinline__ void adj_e_halo(const GridDev& g, const Ring& R, int nr, int r, int q, int s, int be,
+                                           int cbe, const float* hyp, const PsiOut& o, const float* resid_t, int& cur,
                                            int end, bool active) {
+    const int b = 5 + 6 * q;
+    float* ezr = R.row(nr, b);
     float ez = active ? ezr[cbe] : 0.f;
     while (cur < end) {
         const Ev e = __ldg(g.injh_ev + cur);
@@ -455,9 +633,12 @@ __device__ __forceinline__ void adj_e_halo(const GridDev& g, int r, int q, int s
     }
     if (!active) return;
     if (be < g.ny) {
+        const float* hxr = R.row(nr, b + 1);
+        const float* hyr = R.row(nr, b + 2);
         const float hu = hyp ? hyp[cbe] : 0.f;
-        ez = e_update<false>(g, r, be, ez, __fsub_rn(hyr[cbe], hu), __fsub_rn(hxr[cbe], hxr[cbe - 1]), car[cbe],
-                             cbr[cbe], rd, rd);
+        ez = e_cell_s<false>(g, R.pml, r, be, cbe, ez, __fsub_rn(hyr[cbe], hu), __fsub_rn(hxr[cbe], hxr[cbe - 1]),
+                             R.row(nr, 0)[cbe], R.row(nr, 1)[cbe], R.row(nr, 2)[cbe], R.row(nr, b + 3),
+                             R.row(nr, b + 5), o);
     } else {
         ez = 0.f;
     }
@@ -469,23 +650,15 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
     extern __shared__ __align__(128) unsigned char smem[];
     const int nw = (blockDim.x >> 5) - 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int W = nw * 32 * V, RW = W + 8;
-    const int SROWS = 3 + 5 * G;
-    const Ring R = carve_ring(smem, D, SROWS, RW);
+    const int W = nw * 32 * V;
+    const int SROWS = 5 + 8 * G;
+    const Ring R = carve_ring(smem, D, SROWS, ring_slot_width(W, g.TY), g.th);
     const TileTma T = tma_tile(g, W);
     if (T.grp * G >= g.S) return;
     const int wp = rp ^ 1;
     const int r_first = T.i0 >= 1 ? T.i0 - 1 : T.i0;
     const int r_last = min(T.i1, g.nx - 1);   // row nx is the zero frame: never loaded
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < D; ++k) {
-            mbar_init(&R.full[k], 1);
-            mbar_init(&R.empty[k], nw);
-        }
-        *R.abort_flag = 0;
-        fence_mbar_init();
-    }
-    __syncthreads();
+    ring_init(g, R, nw);
     if (warp == nw) {
         if (lane == 0) tma_producer<G, true>(g, R, T, r_first, r_last, rp, it);
         return;
@@ -501,6 +674,7 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
     const int cbe = 4 + W;
     const bool halo_thread = (tid == ncons - 1);
     const float* resid_t = g.resid + (long long)it * g.nrx;
+    const float* pml = R.pml;
     int ic = g.inj_off[blockIdx.x];
     const int ie = g.inj_off[blockIdx.x + 1];
     int hc = g.injh_off[blockIdx.x];
@@ -521,12 +695,10 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
     for (int q = 0; q < G; ++q) {
         const int s = s0 + q;
         if (s >= g.S) continue;
-        const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-        const float* hyp = (T.i0 >= 1) ? R.row(0, 5 + 3 * q) : nullptr;
-        adj_e_row<V>(g, T.i0, q, s, jb, c0, R.row(n, 3 + 3 * q), R.row(n, 4 + 3 * q), R.row(n, 5 + 3 * q), hyp,
-                     R.row(n, 0), R.row(n, 1), rd, wr, true, resid_t, ic, ie);
-        adj_e_halo(g, T.i0, q, s, be, cbe, R.row(n, 3 + 3 * q), R.row(n, 4 + 3 * q), R.row(n, 5 + 3 * q), hyp,
-                   R.row(n, 0), R.row(n, 1), rd, resid_t, hc, he, halo_thread);
+        const PsiOut o = psi_out(g, wp, s, T.i0);
+        const float* hyp = (T.i0 >= 1) ? R.row(0, 5 + 6 * q + 2) : nullptr;
+        adj_e_row<V>(g, R, n, T.i0, q, s, jb, c0, hyp, o, true, resid_t, ic, ie);
+        adj_e_halo(g, R, n, T.i0, q, s, be, cbe, hyp, o, resid_t, hc, he, halo_thread);
     }
     if (T.i0 >= 1) {
         __syncwarp();
@@ -543,20 +715,16 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
             for (int q = 0; q < G; ++q) {
                 const int s = s0 + q;
                 if (s >= g.S) continue;
-                const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-                const float* hyp = R.row(n, 5 + 3 * q);
-                adj_e_row<V>(g, r, q, s, jb, c0, R.row(n + 1, 3 + 3 * q), R.row(n + 1, 4 + 3 * q),
-                             R.row(n + 1, 5 + 3 * q), hyp, R.row(n + 1, 0), R.row(n + 1, 1), rd, wr, r < T.i1,
-                             resid_t, ic, ie);
-                if (r < T.i1)
-                    adj_e_halo(g, r, q, s, be, cbe, R.row(n + 1, 3 + 3 * q), R.row(n + 1, 4 + 3 * q),
-                               R.row(n + 1, 5 + 3 * q), hyp, R.row(n + 1, 0), R.row(n + 1, 1), rd, resid_t, hc, he,
-                               halo_thread);
+                const PsiOut o = psi_out(g, wp, s, r);
+                const float* hyp = R.row(n, 5 + 6 * q + 2);
+                adj_e_row<V>(g, R, n + 1, r, q, s, jb, c0, hyp, o, r < T.i1, resid_t, ic, ie);
+                if (r < T.i1) adj_e_halo(g, R, n + 1, r, q, s, be, cbe, hyp, o, resid_t, hc, he, halo_thread);
             }
         }
         consumer_sync(ncons);
         // --- H of row i and imaging
-        const float* chr = R.row(n, 2);
+        const float* chr = R.row(n, 3);
+        const float* cir = R.row(n, 4);
         float acc_e[V], acc_s[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) { acc_e[v] = 0.f; acc_s[v] = 0.f; }
@@ -564,28 +732,31 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
         for (int q = 0; q < G; ++q) {
             const int s = s0 + q;
             if (s >= g.S) continue;
-            const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-            const float* ezc = R.row(n, 3 + 3 * q);
+            const int b = 5 + 6 * q;
+            const PsiOut o = psi_out(g, wp, s, i);
+            const float* ezc = R.row(n, b);
+            const float* pH = R.row(n, b + 4);
+            const float* yp = R.row(n, b + 5);
             float ez[V + 1], en[V], hx[V], hy[V], ch[V], f1[V], f0[V];
 #pragma unroll
             for (int v = 0; v <= V; ++v) ez[v] = ezc[c0 + v];
             if (have_r) {
-                lds<V>(en, R.row(n + 1, 3 + 3 * q) + c0);
+                lds<V>(en, R.row(n + 1, b) + c0);
             } else {
 #pragma unroll
                 for (int v = 0; v < V; ++v) en[v] = 0.f;
             }
-            lds<V>(hx, R.row(n, 4 + 3 * q) + c0);
-            lds<V>(hy, R.row(n, 5 + 3 * q) + c0);
+            lds<V>(hx, R.row(n, b + 1) + c0);
+            lds<V>(hy, R.row(n, b + 2) + c0);
             lds<V>(ch, chr + c0);
-            lds<V>(f1, R.row(n, 3 + 3 * G + 2 * q) + c0);
-            lds<V>(f0, R.row(n, 4 + 3 * G + 2 * q) + c0);
+            lds<V>(f1, R.row(n, 5 + 6 * G + 2 * q) + c0);
+            lds<V>(f0, R.row(n, 6 + 6 * G + 2 * q) + c0);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const int j = jb + v;
                 if (j < ny) {
-                    h_update<true, true, true>(g, i, j, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
-                                               __fsub_rn(en[v], ez[v]), ch[v], rd, wr);
+                    h_cell_s<true, true, true>(g, pml, i, j, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
+                                               __fsub_rn(en[v], ez[v]), ch[v], cir[c0 + v], pH, yp, o);
                     acc_e[v] = __fadd_rn(acc_e[v], __fmul_rn(__fsub_rn(f1[v], f0[v]), ez[v]));
                     acc_s[v] = __fadd_rn(acc_s[v], __fmul_rn(__fmul_rn(f1[v], ez[v]), g.dt));
                 }
