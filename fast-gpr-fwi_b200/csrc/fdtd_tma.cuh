@@ -267,103 +267,111 @@ __device__ __forceinline__ float cpml_s(float f, float deriv, float u4, float& p
     return out;
 }
 
-// Global destinations of one shot's new CPML auxiliaries (parity wp).
-struct PsiOut {
-    float* ex;   // E x-slab auxiliary row of this row (NULL if none) -- indexed by column j
-    float* ey0;  // E y0 / ymax auxiliaries of this row -- indexed by k
-    float* eym;
-    float* hx;   // H x-slab auxiliary row
-    float* hy0;
-    float* hym;
-};
-__device__ __forceinline__ PsiOut psi_out(const GridDev& g, int wp, int s, int r) {
-    PsiOut o;
-    const int ek = ex_row(g, r), hk = hx_row(g, r);
-    o.ex = ek >= 0 ? g.pex[wp] + (long long)s * g.pxs + (long long)ek * g.P : nullptr;
-    o.hx = hk >= 0 ? g.phx[wp] + (long long)s * g.pxs + (long long)hk * g.P : nullptr;
-    const long long y0 = (long long)s * g.pys + (long long)r * g.TY;
-    const long long y1 = (long long)s * g.pys + (long long)(g.nx + 1 + r) * g.TY;
-    o.ey0 = g.pey[wp] + y0;
-    o.eym = g.pey[wp] + y1;
-    o.hy0 = g.phy[wp] + y0;
-    o.hym = g.phy[wp] + y1;
-    return o;
-}
+// x-slab auxiliary row index of row r, or -1 (see ex_row / hx_row): rows
+// 0..th-1 of the auxiliary array are slab x0 (k = index), rows th..2th-1 slab
+// xmax (k = index - th).
 
-// E update of cell (i, j), operands in shared memory (see e_update).
-//   pE: the row's x-slab E auxiliary slot (indexed by smem column c)
-//   yp: the row's y-slab block
+// E update of cell (i, j), operands in shared memory; same operation
+// sequence as e_update.  ek: x-slab E auxiliary row of row i (or -1);
+// y0 / ym: this column lies in the y0 / ymax E slab.  New auxiliaries of
+// shot s go to parity wp.
 template <bool STORE>
 __device__ __forceinline__ float e_cell_s(const GridDev& g, const float* pml, int i, int j, int c, float ez, float dhy,
-                                          float dhx, float ca, float cb, float cd, const float* pE, const float* yp,
-                                          const PsiOut& o) {
+                                          float dhx, float ca, float cb, const float* cdr, int ek, bool y0, bool ym,
+                                          const float* pE, const float* yp, int s, int wp) {
     if (i >= 1 && j >= 1) ez = __fmaf_rn(-cb, dhx, madd2(ca, ez, cb, dhy));
-    const int th = g.th;
-    if (th > 0) {
-        const int nx = g.nx, ny = g.ny, TY = g.TY;
-        if (i >= 1 && i <= th) {
+    if (ek >= 0 || y0 || ym) {
+        const int th = g.th;
+        const float cd = cdr[c];
+        if (ek >= 0 && ek < th) {
             float psi = pE[c];
-            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, th - i);
-            if (STORE) __stcg(o.ex + j, psi);
+            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, ek);
+            if (STORE) __stcg(g.pex[wp] + (long long)s * g.pxs + (long long)ek * g.P + j, psi);
         }
-        if (j >= 1 && j <= th) {
+        if (y0) {
             const int k = th - j;
             float psi = yp[k];
             ez = cpml_s<false>(ez, __fdiv_rn(dhx, g.d), cd, psi, pml, th, k);
-            if (STORE) __stcg(o.ey0 + k, psi);
+            if (STORE) __stcg(g.pey[wp] + (long long)s * g.pys + (long long)i * g.TY + k, psi);
         }
-        if (i >= nx - th) {
+        if (ek >= th) {
             float psi = pE[c];
-            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, i - (nx - th));
-            if (STORE) __stcg(o.ex + j, psi);
+            ez = cpml_s<true>(ez, __fdiv_rn(dhy, g.d), cd, psi, pml, th, ek - th);
+            if (STORE) __stcg(g.pex[wp] + (long long)s * g.pxs + (long long)ek * g.P + j, psi);
         }
-        if (j >= ny - th) {
-            const int k = j - (ny - th);
-            float psi = yp[TY + k];
+        if (ym) {
+            const int k = j - (g.ny - th);
+            float psi = yp[g.TY + k];
             ez = cpml_s<false>(ez, __fdiv_rn(dhx, g.d), cd, psi, pml, th, k);
-            if (STORE) __stcg(o.eym + k, psi);
+            if (STORE) __stcg(g.pey[wp] + (long long)s * g.pys + (long long)(g.nx + 1 + i) * g.TY + k, psi);
         }
     }
     return ez;
 }
 
-// H update of cell (i, j), operands in shared memory (see h_update).
+// H update of cell (i, j), operands in shared memory; same operation
+// sequence as h_update.  hk: x-slab H auxiliary row of row i (or -1);
+// y0 / ym: this column lies in the y0 / ymax H slab.
 template <bool STORE, bool DO_HX, bool DO_HY>
 __device__ __forceinline__ void h_cell_s(const GridDev& g, const float* pml, int i, int j, int c, float& hx, float& hy,
-                                         float dzx, float dzy, float ch, float ci, const float* pH, const float* yp,
-                                         const PsiOut& o) {
+                                         float dzx, float dzy, float ch, const float* cir, int hk, bool y0, bool ym,
+                                         const float* pH, const float* yp, int s, int wp) {
     if (DO_HX && i >= 1) hx = msub2(1.0f, hx, ch, dzx);
     if (DO_HY && j >= 1) hy = madd2(1.0f, hy, ch, dzy);
-    const int th = g.th;
-    if (th > 0) {
-        const int nx = g.nx, ny = g.ny, TY = g.TY;
+    const bool xs = DO_HY && hk >= 0;
+    const bool ys0 = DO_HX && y0, ysm = DO_HX && ym;
+    if (xs || ys0 || ysm) {
+        const int th = g.th;
         const float* HR = pml + 4 * th;
-        if (DO_HY && i <= th - 1) {
+        const float ci = cir[c];
+        if (xs && hk < th) {
             float psi = pH[c];
-            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, th - 1 - i);
-            if (STORE) __stcg(o.hx + j, psi);
+            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, hk);
+            if (STORE) __stcg(g.phx[wp] + (long long)s * g.pxs + (long long)hk * g.P + j, psi);
         }
-        if (DO_HX && j <= th - 1) {
+        if (ys0) {
             const int k = th - 1 - j;
-            float psi = yp[2 * TY + k];
+            float psi = yp[2 * g.TY + k];
             hx = cpml_s<false>(hx, __fdiv_rn(dzx, g.d), ci, psi, HR, th, k);
-            if (STORE) __stcg(o.hy0 + k, psi);
+            if (STORE) __stcg(g.phy[wp] + (long long)s * g.pys + (long long)i * g.TY + k, psi);
         }
-        if (DO_HY && i >= nx - th) {
+        if (xs && hk >= th) {
             float psi = pH[c];
-            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, i - (nx - th));
-            if (STORE) __stcg(o.hx + j, psi);
+            hy = cpml_s<true>(hy, __fdiv_rn(dzy, g.d), ci, psi, HR, th, hk - th);
+            if (STORE) __stcg(g.phx[wp] + (long long)s * g.pxs + (long long)hk * g.P + j, psi);
         }
-        if (DO_HX && j >= ny - th) {
-            const int k = j - (ny - th);
-            float psi = yp[3 * TY + k];
+        if (ysm) {
+            const int k = j - (g.ny - th);
+            float psi = yp[3 * g.TY + k];
             hx = cpml_s<false>(hx, __fdiv_rn(dzx, g.d), ci, psi, HR, th, k);
-            if (STORE) __stcg(o.hym + k, psi);
+            if (STORE) __stcg(g.phy[wp] + (long long)s * g.pys + (long long)(g.nx + 1 + i) * g.TY + k, psi);
         }
     }
 }
 
-// Shared set-up of both kernels: barriers, CPML vectors, role split.
+// y-slab membership bits of a thread's V columns (bit v for column jb+v).
+struct YBits {
+    unsigned valid, e0, em, h0, hm;
+};
+template <int V>
+__device__ __forceinline__ YBits ybits(const GridDev& g, int jb) {
+    YBits b{0u, 0u, 0u, 0u, 0u};
+    const int th = g.th, ny = g.ny;
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        const int j = jb + v;
+        if (j < ny) b.valid |= 1u << v;
+        if (th > 0 && j < ny) {
+            if (j >= 1 && j <= th) b.e0 |= 1u << v;
+            if (j >= ny - th) b.em |= 1u << v;
+            if (j <= th - 1) b.h0 |= 1u << v;
+            if (j >= ny - th) b.hm |= 1u << v;
+        }
+    }
+    return b;
+}
+
+// Shared set-up of both kernels: barriers, CPML vectors.
 __device__ __forceinline__ void ring_init(const GridDev& g, const Ring& R, int nw) {
     for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) R.pml[k] = g.pml[k];
     if (threadIdx.x == 0) {
@@ -381,13 +389,14 @@ __device__ __forceinline__ void ring_init(const GridDev& g, const Ring& R, int n
 // Forward step
 // ---------------------------------------------------------------------------
 template <int V, int G>
-__global__ void k_forward_tma(const GridDev g, const int t, const int D) {
+__global__ void __launch_bounds__(512) k_forward_tma(const GridDev g, const int t, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int nw = (blockDim.x >> 5) - 1;      // consumer warps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = nw * 32 * V;
     const int SROWS = 5 + 6 * G;
-    const Ring R = carve_ring(smem, D, SROWS, ring_slot_width(W, g.TY), g.th);
+    const int SW = ring_slot_width(W, g.TY);
+    const Ring R = carve_ring(smem, D, SROWS, SW, g.th);
     const TileTma T = tma_tile(g, W);
     if (T.grp * G >= g.S) return;
     const int rp = t & 1, wp = rp ^ 1;
@@ -398,13 +407,16 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
         return;
     }
 
-    const int ny = g.ny, P = g.P;
+    const int P = g.P;
     const int tid = threadIdx.x;           // consumer thread index
     const int c0 = 4 + tid * V;            // smem column of this thread's first cell
     const int jb = T.b0 + tid * V;         // its global column
     const int s0 = T.grp * G;
     const int ncons = nw * 32;
-    const long long hstride = (long long)g.nx * g.Ph;
+    const int stage_floats = SROWS * SW;
+    const YBits yb = ybits<V>(g, jb);
+    const bool act = jb < P;
+    const bool hist_act = g.hist != nullptr && jb < g.Ph;
     const float* pml = R.pml;
 
     float hyu[G][V];
@@ -413,48 +425,50 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
 #pragma unroll
         for (int v = 0; v < V; ++v) hyu[q][v] = 0.f;
 
-    int n = 0;  // ring index of the current row
+    int slot = 0;  // ring slot of the current row
     if (T.i0 >= 1) {
         wait_bounded(g, &R.full[0], 0, R.abort_flag, ERR_WAIT_FULL);
         wait_bounded(g, &R.full[1 % D], (1 / D) & 1, R.abort_flag, ERR_WAIT_FULL);
         const int ih = T.i0 - 1;
+        const float* st0 = R.base;
+        const float* st1 = R.base + (1 % D) * stage_floats;
+        const int hk = hx_row(g, ih);
 #pragma unroll
         for (int q = 0; q < G; ++q) {
             if (s0 + q >= g.S) continue;
             const int b = 5 + 6 * q;
-            const float* ezh = R.row(0, b);
-            const float* hyh = R.row(0, b + 2);
-            const float* ez0 = R.row(1, b);
-            const PsiOut o = psi_out(g, wp, s0 + q, ih);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int j = jb + v, c = c0 + v;
-                float hx_unused = 0.f, hy = hyh[c];
-                if (j < ny)
-                    h_cell_s<false, false, true>(g, pml, ih, j, c, hx_unused, hy, 0.f, __fsub_rn(ez0[c], ezh[c]),
-                                                 R.row(0, 3)[c], R.row(0, 4)[c], R.row(0, b + 4), R.row(0, b + 5), o);
+                const int c = c0 + v;
+                float hx_unused = 0.f, hy = st0[b * SW + 2 * SW + c];
+                if (yb.valid >> v & 1)
+                    h_cell_s<false, false, true>(g, pml, ih, jb + v, c, hx_unused, hy, 0.f,
+                                                 __fsub_rn(st1[b * SW + c], st0[b * SW + c]), st0[3 * SW + c],
+                                                 st0 + 4 * SW, hk, false, false, st0 + (b + 4) * SW,
+                                                 st0 + (b + 5) * SW, s0 + q, wp);
                 hyu[q][v] = hy;
             }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&R.empty[0]);
-        n = 1;
+        slot = 1 % D;
     } else {
         wait_bounded(g, &R.full[0], 0, R.abort_flag, ERR_WAIT_FULL);
     }
+    int n = slot;  // ring sequence number of the current row (for barrier parity)
 
     int sc = g.src_off[blockIdx.x];
     const int se = g.src_off[blockIdx.x + 1];
     int rc = g.rx_off[blockIdx.x];
     const int re = g.rx_off[blockIdx.x + 1];
+    const long long hplane = (long long)g.nx * g.Ph;
 
     for (int i = T.i0; i < T.i1; ++i, ++n) {
-        wait_bounded(g, &R.full[(n + 1) % D], ((n + 1) / D) & 1, R.abort_flag, ERR_WAIT_FULL);
-        const float* car = R.row(n, 0);
-        const float* cbr = R.row(n, 1);
-        const float* cdr = R.row(n, 2);
-        const float* chr = R.row(n, 3);
-        const float* cir = R.row(n, 4);
+        const int nslot = (slot + 1 == D) ? 0 : slot + 1;
+        wait_bounded(g, &R.full[nslot], ((n + 1) / D) & 1, R.abort_flag, ERR_WAIT_FULL);
+        float* st = R.base + slot * stage_floats;
+        const float* stn = R.base + nslot * stage_floats;
+        const int hk = hx_row(g, i), ek = ex_row(g, i);
         float hyn[G][V];
         // --- H of row i
 #pragma unroll
@@ -462,33 +476,30 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
             if (s0 + q >= g.S) continue;
             const int s = s0 + q;
             const int b = 5 + 6 * q;
-            const PsiOut o = psi_out(g, wp, s, i);
-            const float* ezc = R.row(n, b);
-            float* hxr = R.row(n, b + 1);
-            const float* hyr = R.row(n, b + 2);
-            const float* pH = R.row(n, b + 4);
-            const float* yp = R.row(n, b + 5);
-            const float* ezn = R.row(n + 1, b);
+            const float* ezc = st + b * SW;
+            float* hxr = st + (b + 1) * SW;
             float ez[V + 1], en[V], hx[V], hy[V], ch[V];
-            lds<V>(en, ezn + c0);
+            lds<V>(en, stn + b * SW + c0);
             lds<V>(hx, hxr + c0);
-            lds<V>(hy, hyr + c0);
-            lds<V>(ch, chr + c0);
-#pragma unroll
-            for (int v = 0; v <= V; ++v) ez[v] = ezc[c0 + v];
+            lds<V>(hy, st + (b + 2) * SW + c0);
+            lds<V>(ch, st + 3 * SW + c0);
+            lds<V>(*reinterpret_cast<float(*)[V]>(ez), ezc + c0);
+            ez[V] = ezc[c0 + V];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int j = jb + v;
-                if (j < ny)
-                    h_cell_s<true, true, true>(g, pml, i, j, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
-                                               __fsub_rn(en[v], ez[v]), ch[v], cir[c0 + v], pH, yp, o);
+                if (yb.valid >> v & 1)
+                    h_cell_s<true, true, true>(g, pml, i, jb + v, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
+                                               __fsub_rn(en[v], ez[v]), ch[v], st + 4 * SW, hk, yb.h0 >> v & 1,
+                                               yb.hm >> v & 1, st + (b + 4) * SW, st + (b + 5) * SW, s, wp);
                 hyn[q][v] = hy[v];
             }
             // Hx of the column left of the band: from the old state, auxiliaries read only
             if (tid == 0 && T.b0 > 0) {
+                const int j = T.b0 - 1;
                 float hxl = hxr[3], hy_unused = 0.f;
-                h_cell_s<false, true, false>(g, pml, i, T.b0 - 1, 3, hxl, hy_unused, __fsub_rn(ez[0], ezc[3]), 0.f,
-                                             chr[3], cir[3], pH, yp, o);
+                h_cell_s<false, true, false>(g, pml, i, j, 3, hxl, hy_unused, __fsub_rn(ez[0], ezc[3]), 0.f,
+                                             st[3 * SW + 3], st + 4 * SW, -1, g.th > 0 && j <= g.th - 1,
+                                             g.th > 0 && j >= g.ny - g.th, st + (b + 4) * SW, st + (b + 5) * SW, s, wp);
                 hxr[3] = hxl;
             }
 #pragma unroll
@@ -501,26 +512,22 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
             if (s0 + q >= g.S) continue;
             const int s = s0 + q;
             const int b = 5 + 6 * q;
-            const PsiOut o = psi_out(g, wp, s, i);
-            const float* ezc = R.row(n, b);
-            const float* hxr = R.row(n, b + 1);
-            const float* pE = R.row(n, b + 3);
-            const float* yp = R.row(n, b + 5);
+            const float* hxr = st + (b + 1) * SW;
             float ez[V], hx[V], ca[V], cb[V];
-            lds<V>(ez, ezc + c0);
+            lds<V>(ez, st + b * SW + c0);
             lds<V>(hx, hxr + c0);
-            lds<V>(ca, car + c0);
-            lds<V>(cb, cbr + c0);
+            lds<V>(ca, st + c0);
+            lds<V>(cb, st + SW + c0);
             const float hxl0 = hxr[c0 - 1];
             float ezw[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int j = jb + v;
                 ezw[v] = ez[v];
-                if (j < ny) {
+                if (yb.valid >> v & 1) {
                     const float hxl = (v > 0) ? hx[(v + V - 1) % V] : hxl0;
-                    ezw[v] = e_cell_s<true>(g, pml, i, j, c0 + v, ez[v], __fsub_rn(hyn[q][v], hyu[q][v]),
-                                            __fsub_rn(hx[v], hxl), ca[v], cb[v], cdr[c0 + v], pE, yp, o);
+                    ezw[v] = e_cell_s<true>(g, pml, i, jb + v, c0 + v, ez[v], __fsub_rn(hyn[q][v], hyu[q][v]),
+                                            __fsub_rn(hx[v], hxl), ca[v], cb[v], st + 2 * SW, ek, yb.e0 >> v & 1,
+                                            yb.em >> v & 1, st + (b + 3) * SW, st + (b + 5) * SW, s, wp);
                 }
             }
             while (sc < se) {
@@ -529,19 +536,17 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
 #pragma unroll
                 for (int v = 0; v < V; ++v)
                     if (jb + v == e.z)
-                        ezw[v] = __fmaf_rn(-cdr[c0 + v], __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
+                        ezw[v] = __fmaf_rn(-st[2 * SW + c0 + v], __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
                 ++sc;
             }
-            if (jb < P) {
+            if (act) {
                 const long long ro = (long long)s * g.plane + (long long)i * P + jb;
                 st_state<V>(g, g.ez[wp] + ro, ezw);
                 st_state<V>(g, g.hx[wp] + ro, hx);
                 st_state<V>(g, g.hy[wp] + ro, hyn[q]);
             }
-            if (g.hist && jb < g.Ph) {
-                float* hrow = g.hist + ((long long)t * g.S + s) * hstride + (long long)i * g.Ph + jb;
-                st_state<V>(g, hrow, ezw);
-            }
+            if (hist_act)
+                st_state<V>(g, g.hist + ((long long)t * g.S + s) * hplane + (long long)i * g.Ph + jb, ezw);
             while (rc < re) {
                 const Ev e = __ldg(g.rx_ev + rc);
                 if (e.x != i || e.y != q) break;
@@ -556,7 +561,8 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
             for (int v = 0; v < V; ++v) hyu[q][v] = hyn[q][v];
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&R.empty[n % D]);
+        if (lane == 0) mbar_arrive(&R.empty[slot]);
+        slot = nslot;
     }
 }
 
@@ -565,25 +571,21 @@ __global__ void k_forward_tma(const GridDev g, const int t, const int D) {
 // ---------------------------------------------------------------------------
 
 // E_new of row r of one shot for this thread's columns, written back into the
-// stage's Ez slot.  sr: stage slot base of this shot in row r's stage; hyp:
-// Hy_old of row r-1 (NULL when r == 0).  Injection events consumed from *cur.
+// stage's Ez slot.  sr: row r's stage; hyp: Hy_old of row r-1 (NULL when
+// r == 0).  Injection events consumed from *cur.
 template <int V>
-__device__ __forceinline__ void adj_e_row(const GridDev& g, const Ring& R, int nr, int r, int q, int s, int jb,
-                                          int c0, const float* hyp, const PsiOut& o, bool store,
-                                          const float* resid_t, int& cur, int end) {
+__device__ __forceinline__ void adj_e_row(const GridDev& g, const float* pml, float* sr, int SW, int r, int q, int s,
+                                          int jb, int c0, const YBits& yb, const float* hyp, bool store, int wp,
+                                          const float* resid_s, int& cur, int end) {
     const int b = 5 + 6 * q;
-    float* ezr = R.row(nr, b);
-    const float* hxr = R.row(nr, b + 1);
-    const float* hyr = R.row(nr, b + 2);
-    const float* pE = R.row(nr, b + 3);
-    const float* yp = R.row(nr, b + 5);
-    const float* cdr = R.row(nr, 2);
+    float* ezr = sr + b * SW;
+    const float* hxr = sr + (b + 1) * SW;
     float ez[V], hx[V], hy[V], hu[V], ca[V], cb[V];
     lds<V>(ez, ezr + c0);
     lds<V>(hx, hxr + c0);
-    lds<V>(hy, hyr + c0);
-    lds<V>(ca, R.row(nr, 0) + c0);
-    lds<V>(cb, R.row(nr, 1) + c0);
+    lds<V>(hy, sr + (b + 2) * SW + c0);
+    lds<V>(ca, sr + c0);
+    lds<V>(cb, sr + SW + c0);
     if (hyp) {
         lds<V>(hu, hyp + c0);
     } else {
@@ -596,21 +598,22 @@ __device__ __forceinline__ void adj_e_row(const GridDev& g, const Ring& R, int n
         if (e.x != r || e.y != q) break;
 #pragma unroll
         for (int v = 0; v < V; ++v)
-            if (jb + v == e.z) ez[v] = __fsub_rn(ez[v], resid_t[(long long)s * g.nt * g.nrx + e.w]);
+            if (jb + v == e.z) ez[v] = __fsub_rn(ez[v], resid_s[e.w]);
         ++cur;
     }
+    const int ek = ex_row(g, r);
     float out[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
-        const int j = jb + v;
         out[v] = ez[v];
-        if (j < g.ny) {
+        if (yb.valid >> v & 1) {
             const float hxl = (v > 0) ? hx[(v + V - 1) % V] : hxl0;
             const float dhy = __fsub_rn(hy[v], hu[v]), dhx = __fsub_rn(hx[v], hxl);
-            out[v] = store ? e_cell_s<true>(g, R.pml, r, j, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], cdr[c0 + v], pE,
-                                            yp, o)
-                           : e_cell_s<false>(g, R.pml, r, j, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], cdr[c0 + v], pE,
-                                             yp, o);
+            out[v] = store ? e_cell_s<true>(g, pml, r, jb + v, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], sr + 2 * SW, ek,
+                                            yb.e0 >> v & 1, yb.em >> v & 1, sr + (b + 3) * SW, sr + (b + 5) * SW, s, wp)
+                           : e_cell_s<false>(g, pml, r, jb + v, c0 + v, ez[v], dhy, dhx, ca[v], cb[v], sr + 2 * SW,
+                                             ek, yb.e0 >> v & 1, yb.em >> v & 1, sr + (b + 3) * SW, sr + (b + 5) * SW,
+                                             s, wp);
         }
     }
 #pragma unroll
@@ -619,26 +622,27 @@ __device__ __forceinline__ void adj_e_row(const GridDev& g, const Ring& R, int n
 
 // E_new of the column just past the band (be) of row r, from the stage (old
 // values), with the halo-column injections of row r.
-__device__ __forceinline__ void adj_e_halo(const GridDev& g, const Ring& R, int nr, int r, int q, int s, int be,
-                                           int cbe, const float* hyp, const PsiOut& o, const float* resid_t, int& cur,
-                                           int end, bool active) {
+__device__ __forceinline__ void adj_e_halo(const GridDev& g, const float* pml, float* sr, int SW, int r, int q, int s,
+                                           int be, int cbe, const float* hyp, const float* resid_s, int& cur, int end,
+                                           bool active, int wp) {
     const int b = 5 + 6 * q;
-    float* ezr = R.row(nr, b);
+    float* ezr = sr + b * SW;
     float ez = active ? ezr[cbe] : 0.f;
     while (cur < end) {
         const Ev e = __ldg(g.injh_ev + cur);
         if (e.x != r || e.y != q) break;
-        if (active) ez = __fsub_rn(ez, resid_t[(long long)s * g.nt * g.nrx + e.w]);
+        if (active) ez = __fsub_rn(ez, resid_s[e.w]);
         ++cur;
     }
     if (!active) return;
     if (be < g.ny) {
-        const float* hxr = R.row(nr, b + 1);
-        const float* hyr = R.row(nr, b + 2);
+        const float* hxr = sr + (b + 1) * SW;
         const float hu = hyp ? hyp[cbe] : 0.f;
-        ez = e_cell_s<false>(g, R.pml, r, be, cbe, ez, __fsub_rn(hyr[cbe], hu), __fsub_rn(hxr[cbe], hxr[cbe - 1]),
-                             R.row(nr, 0)[cbe], R.row(nr, 1)[cbe], R.row(nr, 2)[cbe], R.row(nr, b + 3),
-                             R.row(nr, b + 5), o);
+        const int th = g.th;
+        ez = e_cell_s<false>(g, pml, r, be, cbe, ez, __fsub_rn(sr[(b + 2) * SW + cbe], hu),
+                             __fsub_rn(hxr[cbe], hxr[cbe - 1]), sr[cbe], sr[SW + cbe], sr + 2 * SW, ex_row(g, r),
+                             th > 0 && be >= 1 && be <= th, th > 0 && be >= g.ny - th, sr + (b + 3) * SW,
+                             sr + (b + 5) * SW, s, wp);
     } else {
         ez = 0.f;
     }
@@ -646,13 +650,14 @@ __device__ __forceinline__ void adj_e_halo(const GridDev& g, const Ring& R, int 
 }
 
 template <int V, int G>
-__global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const int D) {
+__global__ void __launch_bounds__(512) k_adjoint_tma(const GridDev g, const int it, const int rp, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int nw = (blockDim.x >> 5) - 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int W = nw * 32 * V;
     const int SROWS = 5 + 8 * G;
-    const Ring R = carve_ring(smem, D, SROWS, ring_slot_width(W, g.TY), g.th);
+    const int SW = ring_slot_width(W, g.TY);
+    const Ring R = carve_ring(smem, D, SROWS, SW, g.th);
     const TileTma T = tma_tile(g, W);
     if (T.grp * G >= g.S) return;
     const int wp = rp ^ 1;
@@ -673,7 +678,9 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
     const int be = T.b0 + W;
     const int cbe = 4 + W;
     const bool halo_thread = (tid == ncons - 1);
-    const float* resid_t = g.resid + (long long)it * g.nrx;
+    const int stage_floats = SROWS * SW;
+    const YBits yb = ybits<V>(g, jb);
+    const bool act = jb < P;
     const float* pml = R.pml;
     int ic = g.inj_off[blockIdx.x];
     const int ie = g.inj_off[blockIdx.x + 1];
@@ -681,50 +688,59 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
     const int he = g.injh_off[blockIdx.x + 1];
     double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
     double* gas = gae + (long long)nx * ny;
+    const long long rstride = (long long)g.nt * g.nrx;
+    const float* resid_t = g.resid + (long long)it * g.nrx;
 
     // Prologue: E_new of row i0.
-    int n = 0;
+    int slot = 0;
     if (T.i0 >= 1) {
         wait_bounded(g, &R.full[0], 0, R.abort_flag, ERR_WAIT_FULL);
         wait_bounded(g, &R.full[1 % D], (1 / D) & 1, R.abort_flag, ERR_WAIT_FULL);
-        n = 1;
+        slot = 1 % D;
     } else {
         wait_bounded(g, &R.full[0], 0, R.abort_flag, ERR_WAIT_FULL);
     }
+    {
+        float* st = R.base + slot * stage_floats;
 #pragma unroll
-    for (int q = 0; q < G; ++q) {
-        const int s = s0 + q;
-        if (s >= g.S) continue;
-        const PsiOut o = psi_out(g, wp, s, T.i0);
-        const float* hyp = (T.i0 >= 1) ? R.row(0, 5 + 6 * q + 2) : nullptr;
-        adj_e_row<V>(g, R, n, T.i0, q, s, jb, c0, hyp, o, true, resid_t, ic, ie);
-        adj_e_halo(g, R, n, T.i0, q, s, be, cbe, hyp, o, resid_t, hc, he, halo_thread);
+        for (int q = 0; q < G; ++q) {
+            const int s = s0 + q;
+            if (s >= g.S) continue;
+            const float* hyp = (T.i0 >= 1) ? R.base + (5 + 6 * q + 2) * SW : nullptr;
+            adj_e_row<V>(g, pml, st, SW, T.i0, q, s, jb, c0, yb, hyp, true, wp, resid_t + s * rstride, ic, ie);
+            adj_e_halo(g, pml, st, SW, T.i0, q, s, be, cbe, hyp, resid_t + s * rstride, hc, he, halo_thread, wp);
+        }
     }
     if (T.i0 >= 1) {
         __syncwarp();
         if (lane == 0) mbar_arrive(&R.empty[0]);
     }
+    int n = slot;
 
     for (int i = T.i0; i < T.i1; ++i, ++n) {
         const int r = i + 1;
         const bool have_r = r < nx;
-        if (have_r) wait_bounded(g, &R.full[(n + 1) % D], ((n + 1) / D) & 1, R.abort_flag, ERR_WAIT_FULL);
+        const int nslot = (slot + 1 == D) ? 0 : slot + 1;
+        float* st = R.base + slot * stage_floats;
+        float* stn = R.base + nslot * stage_floats;
+        if (have_r) wait_bounded(g, &R.full[nslot], ((n + 1) / D) & 1, R.abort_flag, ERR_WAIT_FULL);
         // --- E of row r (row i1 is the next chunk's: computed, auxiliaries not stored)
         if (have_r) {
 #pragma unroll
             for (int q = 0; q < G; ++q) {
                 const int s = s0 + q;
                 if (s >= g.S) continue;
-                const PsiOut o = psi_out(g, wp, s, r);
-                const float* hyp = R.row(n, 5 + 6 * q + 2);
-                adj_e_row<V>(g, R, n + 1, r, q, s, jb, c0, hyp, o, r < T.i1, resid_t, ic, ie);
-                if (r < T.i1) adj_e_halo(g, R, n + 1, r, q, s, be, cbe, hyp, o, resid_t, hc, he, halo_thread);
+                const float* hyp = st + (5 + 6 * q + 2) * SW;
+                adj_e_row<V>(g, pml, stn, SW, r, q, s, jb, c0, yb, hyp, r < T.i1, wp, resid_t + s * rstride, ic,
+                             ie);
+                if (r < T.i1)
+                    adj_e_halo(g, pml, stn, SW, r, q, s, be, cbe, hyp, resid_t + s * rstride, hc, he, halo_thread,
+                               wp);
             }
         }
         consumer_sync(ncons);
         // --- H of row i and imaging
-        const float* chr = R.row(n, 3);
-        const float* cir = R.row(n, 4);
+        const int hk = hx_row(g, i);
         float acc_e[V], acc_s[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) { acc_e[v] = 0.f; acc_s[v] = 0.f; }
@@ -733,55 +749,49 @@ __global__ void k_adjoint_tma(const GridDev g, const int it, const int rp, const
             const int s = s0 + q;
             if (s >= g.S) continue;
             const int b = 5 + 6 * q;
-            const PsiOut o = psi_out(g, wp, s, i);
-            const float* ezc = R.row(n, b);
-            const float* pH = R.row(n, b + 4);
-            const float* yp = R.row(n, b + 5);
+            const float* ezc = st + b * SW;
             float ez[V + 1], en[V], hx[V], hy[V], ch[V], f1[V], f0[V];
-#pragma unroll
-            for (int v = 0; v <= V; ++v) ez[v] = ezc[c0 + v];
+            lds<V>(*reinterpret_cast<float(*)[V]>(ez), ezc + c0);
+            ez[V] = ezc[c0 + V];
             if (have_r) {
-                lds<V>(en, R.row(n + 1, b) + c0);
+                lds<V>(en, stn + b * SW + c0);
             } else {
 #pragma unroll
                 for (int v = 0; v < V; ++v) en[v] = 0.f;
             }
-            lds<V>(hx, R.row(n, b + 1) + c0);
-            lds<V>(hy, R.row(n, b + 2) + c0);
-            lds<V>(ch, chr + c0);
-            lds<V>(f1, R.row(n, 5 + 6 * G + 2 * q) + c0);
-            lds<V>(f0, R.row(n, 6 + 6 * G + 2 * q) + c0);
+            lds<V>(hx, st + (b + 1) * SW + c0);
+            lds<V>(hy, st + (b + 2) * SW + c0);
+            lds<V>(ch, st + 3 * SW + c0);
+            lds<V>(f1, st + (5 + 6 * G + 2 * q) * SW + c0);
+            lds<V>(f0, st + (6 + 6 * G + 2 * q) * SW + c0);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
-                const int j = jb + v;
-                if (j < ny) {
-                    h_cell_s<true, true, true>(g, pml, i, j, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
-                                               __fsub_rn(en[v], ez[v]), ch[v], cir[c0 + v], pH, yp, o);
+                if (yb.valid >> v & 1) {
+                    h_cell_s<true, true, true>(g, pml, i, jb + v, c0 + v, hx[v], hy[v], __fsub_rn(ez[v + 1], ez[v]),
+                                               __fsub_rn(en[v], ez[v]), ch[v], st + 4 * SW, hk, yb.h0 >> v & 1,
+                                               yb.hm >> v & 1, st + (b + 4) * SW, st + (b + 5) * SW, s, wp);
                     acc_e[v] = __fadd_rn(acc_e[v], __fmul_rn(__fsub_rn(f1[v], f0[v]), ez[v]));
                     acc_s[v] = __fadd_rn(acc_s[v], __fmul_rn(__fmul_rn(f1[v], ez[v]), g.dt));
                 }
             }
-            if (jb < P) {
+            if (act) {
                 const long long ro = (long long)s * g.plane + (long long)i * P + jb;
-                float ezo[V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) ezo[v] = ez[v];
-                st_state<V>(g, g.ez[wp] + ro, ezo);
+                st_state<V>(g, g.ez[wp] + ro, *reinterpret_cast<float(*)[V]>(ez));
                 st_state<V>(g, g.hx[wp] + ro, hx);
                 st_state<V>(g, g.hy[wp] + ro, hy);
             }
         }
 #pragma unroll
         for (int v = 0; v < V; ++v) {
-            const int j = jb + v;
-            if (j < ny) {
-                const long long o = (long long)i * ny + j;
+            if (yb.valid >> v & 1) {
+                const long long o = (long long)i * ny + jb + v;
                 gae[o] += (double)acc_e[v];
                 gas[o] += (double)acc_s[v];
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&R.empty[n % D]);
+        if (lane == 0) mbar_arrive(&R.empty[slot]);
+        slot = nslot;
     }
 }
 
