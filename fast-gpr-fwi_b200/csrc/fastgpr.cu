@@ -10,6 +10,7 @@
 #include "../../include/fastgpr.h"
 #include "fdtd_kernels.cuh"
 #include "fdtd_tma.cuh"
+#include "fdtd_tile.cuh"
 
 using fg::Ev;
 using fg::GridDev;
@@ -75,7 +76,7 @@ void build_tiles(fg_plan* p) {
     p->P = (int)align_up((size_t)p->ny + 1, 32);
     p->TY = (int)align_up((size_t)std::max(p->th, 1), 4);
     p->Ph = (int)align_up((size_t)p->ny, 4);
-    p->bw = p->kernel == 0 ? p->NW * 32 * p->V : 32 * p->V;
+    p->bw = p->kernel == 0 ? p->NW * 32 * p->V : 32 * p->V;   // register march and tiles: one warp wide
     p->nb = (p->ny + p->bw - 1) / p->bw;
     p->nc = std::max(1, (p->nx + p->TI - 1) / p->TI);
     p->ngroups = (p->S + p->G - 1) / p->G;
@@ -268,6 +269,35 @@ cudaError_t launch_adjoint_tma(const GridDev& g, int it, int rp, int nw, int D, 
     fg::k_adjoint_tma<V, G><<<g.ntiles, (nw + 1) * 32, smem, st>>>(g, it, rp, D);
     return cudaSuccess;
 }
+template <int V>
+cudaError_t launch_forward_tile(const GridDev& g, int t, int TH, int G, cudaStream_t st) {
+    fg::k_forward_tile<V><<<g.ntiles, 32 * TH, fg::tile_fwd_smem(TH, V), st>>>(g, t, G);
+    return cudaSuccess;
+}
+template <int V>
+cudaError_t launch_adjoint_tile(const GridDev& g, int it, int rp, int TH, int G, cudaStream_t st) {
+    fg::k_adjoint_tile<V><<<g.ntiles, 32 * TH, fg::tile_adj_smem(TH, V), st>>>(g, it, rp, G);
+    return cudaSuccess;
+}
+using FwdTileFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
+using AdjTileFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
+FwdTileFn pick_fwd_tile(int V) {
+    switch (V) {
+        case 1: return launch_forward_tile<1>;
+        case 2: return launch_forward_tile<2>;
+        case 4: return launch_forward_tile<4>;
+    }
+    return nullptr;
+}
+AdjTileFn pick_adj_tile(int V) {
+    switch (V) {
+        case 1: return launch_adjoint_tile<1>;
+        case 2: return launch_adjoint_tile<2>;
+        case 4: return launch_adjoint_tile<4>;
+    }
+    return nullptr;
+}
+
 using FwdTmaFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
 using AdjTmaFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
 template <int V>
@@ -407,10 +437,10 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             delete p;
             return fail(FG_ERR_INVALID, "receiver position outside the grid");
         }
-    p->kernel = tune ? tune->kernel : 0;
-    p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : 1;
-    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile : (q.shots >= 2 ? 2 : 1);
-    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 16;
+    p->kernel = tune ? tune->kernel : 2;
+    p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : (p->kernel == 2 ? 2 : 1);
+    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile : (p->kernel == 2 ? std::min(q.shots, 4) : (q.shots >= 2 ? 2 : 1));
+    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : (p->kernel == 2 ? 8 : 16);
     p->NW = tune && tune->warps_per_tile ? tune->warps_per_tile : 0;
     p->D = tune && tune->stages ? tune->stages : 4;
     if (p->kernel == 0 && p->NW == 0) {
@@ -421,7 +451,8 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     const bool ok_k0 = p->kernel == 0 && (p->G == 1 || p->G == 2 || p->G == 4) && p->NW >= 1 && p->NW <= 16 &&
                        p->D >= 3 && p->D <= 8;
     const bool ok_k1 = p->kernel == 1 && (p->G == 1 || p->G == 2 || p->G == 4 || p->G == 8);
-    if (!ok_common || !(ok_k0 || ok_k1)) {
+    const bool ok_k2 = p->kernel == 2 && p->G >= 1 && p->G <= 64 && p->TI <= 16;
+    if (!ok_common || !(ok_k0 || ok_k1 || ok_k2)) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning");
     }
@@ -508,7 +539,11 @@ int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, fl
         g.out_lo = (const char*)hist;
         g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
     }
-    if (p->kernel == 0) {
+    if (p->kernel == 2) {
+        FwdTileFn fn = pick_fwd_tile(p->V);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->TI, p->G, st));
+    } else if (p->kernel == 0) {
         FwdTmaFn fn = pick_fwd_tma(p->V, p->G);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->NW, p->D, st));
@@ -538,7 +573,11 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     g.out_lo = (const char*)hist;
     g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
     g.resid = resid;
-    if (p->kernel == 0) {
+    if (p->kernel == 2) {
+        AdjTileFn fn = pick_adj_tile(p->V);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->TI, p->G, st));
+    } else if (p->kernel == 0) {
         AdjTmaFn fn = pick_adj_tma(p->V, p->G);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->NW, p->D, st));
