@@ -11,6 +11,7 @@
 #include "fdtd_kernels.cuh"
 #include "fdtd_tma.cuh"
 #include "fdtd_tile.cuh"
+#include "fdtd_march.cuh"
 
 using fg::Ev;
 using fg::GridDev;
@@ -279,13 +280,50 @@ cudaError_t launch_adjoint_tile(const GridDev& g, int it, int rp, int TH, int G,
     fg::k_adjoint_tile<V><<<g.ntiles, 32 * TH, fg::tile_adj_smem(TH, V), st>>>(g, it, rp, G);
     return cudaSuccess;
 }
+template <int V>
+cudaError_t launch_forward_march(const GridDev& g, int t, int TI, int G, cudaStream_t st) {
+    (void)TI;
+    const int blocks = (g.ntiles + fg::MARCH_WARPS - 1) / fg::MARCH_WARPS;
+    fg::k_forward_march<V><<<blocks, 32 * fg::MARCH_WARPS, 0, st>>>(g, t, G);
+    return cudaSuccess;
+}
+template <int V>
+cudaError_t launch_adjoint_march(const GridDev& g, int it, int rp, int TI, int G, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(fg::k_adjoint_march<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    if (attr != cudaSuccess) return attr;
+    const int blocks = (g.ntiles + fg::MARCH_WARPS - 1) / fg::MARCH_WARPS;
+    fg::k_adjoint_march<V><<<blocks, 32 * fg::MARCH_WARPS, fg::march_adj_smem(TI, V), st>>>(g, it, rp, G, TI);
+    return cudaSuccess;
+}
+
 using FwdTileFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
 using AdjTileFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
+FwdTileFn pick_fwd_march(int V) {
+    switch (V) {
+        case 1: return launch_forward_march<1>;
+        case 2: return launch_forward_march<2>;
+        case 4: return launch_forward_march<4>;
+    }
+    return nullptr;
+}
+AdjTileFn pick_adj_march(int V);
 FwdTileFn pick_fwd_tile(int V) {
     switch (V) {
         case 1: return launch_forward_tile<1>;
         case 2: return launch_forward_tile<2>;
         case 4: return launch_forward_tile<4>;
+    }
+    return nullptr;
+}
+AdjTileFn pick_adj_march(int V) {
+    switch (V) {
+        case 1: return launch_adjoint_march<1>;
+        case 2: return launch_adjoint_march<2>;
+        case 4: return launch_adjoint_march<4>;
     }
     return nullptr;
 }
@@ -437,9 +475,10 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             delete p;
             return fail(FG_ERR_INVALID, "receiver position outside the grid");
         }
-    p->kernel = tune ? tune->kernel : 2;
-    p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : (p->kernel == 2 ? 2 : 1);
-    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile : (p->kernel == 2 ? std::min(q.shots, 4) : (q.shots >= 2 ? 2 : 1));
+    p->kernel = tune ? tune->kernel : 3;
+    p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : (p->kernel >= 2 ? 2 : 1);
+    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile
+                                        : (p->kernel >= 2 ? std::min(q.shots, 4) : (q.shots >= 2 ? 2 : 1));
     p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : (p->kernel == 2 ? 8 : 16);
     p->NW = tune && tune->warps_per_tile ? tune->warps_per_tile : 0;
     p->D = tune && tune->stages ? tune->stages : 4;
@@ -452,7 +491,9 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
                        p->D >= 3 && p->D <= 8;
     const bool ok_k1 = p->kernel == 1 && (p->G == 1 || p->G == 2 || p->G == 4 || p->G == 8);
     const bool ok_k2 = p->kernel == 2 && p->G >= 1 && p->G <= 64 && p->TI <= 16;
-    if (!ok_common || !(ok_k0 || ok_k1 || ok_k2)) {
+    const bool ok_k3 = p->kernel == 3 && p->G >= 1 && p->G <= 64 &&
+                       fg::march_adj_smem(p->TI, p->V) <= 227 * 1024;
+    if (!ok_common || !(ok_k0 || ok_k1 || ok_k2 || ok_k3)) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning");
     }
@@ -539,7 +580,11 @@ int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, fl
         g.out_lo = (const char*)hist;
         g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
     }
-    if (p->kernel == 2) {
+    if (p->kernel == 3) {
+        FwdTileFn fn = pick_fwd_march(p->V);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->TI, p->G, st));
+    } else if (p->kernel == 2) {
         FwdTileFn fn = pick_fwd_tile(p->V);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->TI, p->G, st));
@@ -573,7 +618,11 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     g.out_lo = (const char*)hist;
     g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
     g.resid = resid;
-    if (p->kernel == 2) {
+    if (p->kernel == 3) {
+        AdjTileFn fn = pick_adj_march(p->V);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->TI, p->G, st));
+    } else if (p->kernel == 2) {
         AdjTileFn fn = pick_adj_tile(p->V);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->TI, p->G, st));

@@ -65,10 +65,10 @@ typedef struct fg_problem {
 
 /* Launch shape chosen by the autotuner; NULL or zero fields select defaults. */
 typedef struct fg_tuning {
-    int32_t kernel;            /* 2 = staged 2-D tiles (default), 0 = TMA row-streaming tiles,
-                                  1 = per-warp register march */
+    int32_t kernel;            /* 3 = prefetching warp march (default), 2 = staged 2-D tiles,
+                                  0 = TMA row-streaming tiles, 1 = per-warp register march */
     int32_t cols_per_thread;   /* 1, 2 or 4 columns per thread */
-    int32_t shots_per_tile;    /* shots per tile: 2-D tiles 1..64; TMA tiles 1, 2, 4; march 1, 2, 4, 8 */
+    int32_t shots_per_tile;    /* shots per tile: kernels 2, 3: 1..64; TMA tiles 1, 2, 4; register march 1, 2, 4, 8 */
     int32_t rows_per_tile;     /* rows of one tile (>= 2; 2-D tiles <= 16, one warp per row) */
     int32_t warps_per_tile;    /* TMA tiles: consumer warps, 1..16 */
     int32_t stages;            /* TMA tiles: shared-memory ring depth, 3..8 */

@@ -113,6 +113,9 @@ def test_setup_matches_reference(fg, dev, refdrv):
 
 TUNINGS = [
     None,
+    {"kernel": 3, "cols_per_thread": 1, "shots_per_tile": 1, "rows_per_tile": 3},
+    {"kernel": 3, "cols_per_thread": 4, "shots_per_tile": 3, "rows_per_tile": 24},
+    {"kernel": 3, "cols_per_thread": 2, "shots_per_tile": 2, "rows_per_tile": 7},
     {"kernel": 2, "cols_per_thread": 1, "shots_per_tile": 1, "rows_per_tile": 3},
     {"kernel": 2, "cols_per_thread": 4, "shots_per_tile": 3, "rows_per_tile": 16},
     {"kernel": 2, "cols_per_thread": 2, "shots_per_tile": 2, "rows_per_tile": 7},
