@@ -69,6 +69,18 @@ __device__ __forceinline__ void ldcv(const GridDev& g, float (&x)[V], const floa
     }
 }
 
+// Advance an event cursor (events sorted by row, then shot slot) to the first
+// event of (row, slot) or past it; returns true while such an event is current.
+__device__ __forceinline__ bool ev_seek(const Ev* ev, int& cur, int end, int row, int slot) {
+    while (cur < end) {
+        const Ev e = __ldg(ev + cur);
+        if (e.x > row || (e.x == row && e.y > slot)) return false;
+        if (e.x == row && e.y == slot) return true;
+        ++cur;
+    }
+    return false;
+}
+
 // ---------------------------------------------------------------------------
 // Forward step
 // ---------------------------------------------------------------------------
@@ -82,7 +94,7 @@ struct FwdRow {            // operands of row r: Ez_old[r+1], Hx_old[r], Hy_old[
 template <int V>
 __device__ __forceinline__ void fwd_row_load(const GridDev& g, FwdRow<V>& B, const float* ez, const float* hx,
                                              const float* hy, int r, int jb, int lane, int b0, int be, bool act) {
-    const long long o = (long long)r * g.P + jb;
+    const int o = r * g.P + jb;
     ldv<V>(g, B.en, ez + o + g.P, act);
     ldv<V>(g, B.hx, hx + o, act);
     ldv<V>(g, B.hy, hy + o, act);
@@ -93,12 +105,119 @@ __device__ __forceinline__ void fwd_row_load(const GridDev& g, FwdRow<V>& B, con
     B.ezL = 0.f;
     B.hxL = 0.f;
     B.chL = 0.f;
-    if (lane == 31 && be < g.P) B.ezR = ld1(g, ez + (long long)r * g.P + be);
+    if (lane == 31 && be < g.P) B.ezR = ld1(g, ez + r * g.P + be);
     if (lane == 0 && b0 > 0) {
-        const long long ol = (long long)r * g.P + b0 - 1;
+        const int ol = r * g.P + b0 - 1;
         B.ezL = ld1(g, ez + ol);
         B.hxL = ld1(g, hx + ol);
         B.chL = ldc1(g, g.ch + ol);
+    }
+}
+
+// Per-warp state of a forward march over one shot.
+template <int V>
+struct FwdMarch {
+    float ezc[V];   // Ez_old of the current row
+    float hyu[V];   // Hy_new of the row above
+};
+
+template <int V>
+__device__ __forceinline__ void fwd_row(const GridDev& g, FwdMarch<V>& M, const FwdRow<V>& B, int i, int t, int q,
+                                        int s, long long so, int jb, int lane, int b0, bool bcore, bool act,
+                                        const PsiShot& rd, const PsiShot& wr, int& sc, int se, int& rc, int re) {
+    const int P = g.P, ny = g.ny;
+    const int wp = (t & 1) ^ 1;
+    const bool core = bcore && core_row(g, i);
+    // ---- H of row i
+    float right = __shfl_down_sync(FULL, M.ezc[0], 1);
+    if (lane == 31) right = B.ezR;
+    float hx[V], hy[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        hx[v] = B.hx[v];
+        hy[v] = B.hy[v];
+    }
+    float hxl;
+    if (core) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float er = (v + 1 < V) ? M.ezc[(v + 1) % V] : right;
+            hx[v] = __fsub_rn(hx[v], __fmul_rn(B.ch[v], __fsub_rn(er, M.ezc[v])));
+            hy[v] = __fadd_rn(hy[v], __fmul_rn(B.ch[v], __fsub_rn(B.en[v], M.ezc[v])));
+        }
+        hxl = __shfl_up_sync(FULL, hx[V - 1], 1);
+        // column b0-1 is interior too (b0 >= th+1): the lean Hx update
+        if (lane == 0) hxl = __fsub_rn(B.hxL, __fmul_rn(B.chL, __fsub_rn(M.ezc[0], B.ezL)));
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float er = (v + 1 < V) ? M.ezc[(v + 1) % V] : right;
+            if (jb + v < ny)
+                h_update<true, true, true>(g, i, jb + v, hx[v], hy[v], __fsub_rn(er, M.ezc[v]),
+                                           __fsub_rn(B.en[v], M.ezc[v]), B.ch[v], rd, wr);
+        }
+        hxl = __shfl_up_sync(FULL, hx[V - 1], 1);
+        if (lane == 0) {
+            hxl = 0.f;
+            if (b0 > 0) {
+                float h = B.hxL, hy_unused = 0.f;
+                h_update<false, true, false>(g, i, b0 - 1, h, hy_unused, __fsub_rn(M.ezc[0], B.ezL), 0.f, B.chL, rd,
+                                             rd);
+                hxl = h;
+            }
+        }
+    }
+    // ---- E of row i
+    float ezw[V];
+    if (core) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float l = (v > 0) ? hx[(v + V - 1) % V] : hxl;
+            ezw[v] = __fmaf_rn(-B.cb[v], __fsub_rn(hx[v], l),
+                               madd2(B.ca[v], M.ezc[v], B.cb[v], __fsub_rn(hy[v], M.hyu[v])));
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const float l = (v > 0) ? hx[(v + V - 1) % V] : hxl;
+            ezw[v] = M.ezc[v];
+            if (jb + v < ny)
+                ezw[v] = e_update<true>(g, i, jb + v, M.ezc[v], __fsub_rn(hy[v], M.hyu[v]), __fsub_rn(hx[v], l),
+                                        B.ca[v], B.cb[v], rd, wr);
+        }
+    }
+    // Hertzian dipole (sourcereceiver.cu:84)
+    while (ev_seek(g.src_ev, sc, se, i, q)) {
+        const Ev e = __ldg(g.src_ev + sc);
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            if (jb + v == e.z) {
+                const float cd = ldc1(g, g.cd + (long long)i * P + e.z);
+                ezw[v] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
+            }
+        ++sc;
+    }
+    if (act) {
+        const long long o = so + (long long)i * P + jb;
+        st_state<V>(g, g.ez[wp] + o, ezw);
+        st_state<V>(g, g.hx[wp] + o, hx);
+        st_state<V>(g, g.hy[wp] + o, hy);
+    }
+    if (g.hist && jb < g.Ph)
+        st_state<V>(g, g.hist + ((long long)t * g.S + s) * ((long long)g.nx * g.Ph) + (long long)i * g.Ph + jb, ezw);
+    while (ev_seek(g.rx_ev, rc, re, i, q)) {
+        const Ev e = __ldg(g.rx_ev + rc);
+        if (t + 1 < g.nt) {
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                if (jb + v == e.z) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezw[v];
+        }
+        ++rc;
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        M.ezc[v] = B.en[v];
+        M.hyu[v] = hy[v];
     }
 }
 
@@ -106,14 +225,13 @@ template <int V>
 __global__ void __launch_bounds__(32 * MARCH_WARPS) k_forward_march(const GridDev g, const int t, const int G) {
     const int lane = threadIdx.x & 31;
     TileM T;
-    if (!march_tile(g, V, blockIdx.x * MARCH_WARPS + (threadIdx.x >> 5), T)) return;
     const int tile = blockIdx.x * MARCH_WARPS + (threadIdx.x >> 5);
+    if (!march_tile(g, V, tile, T)) return;
     const int P = g.P, ny = g.ny;
     const int rp = t & 1, wp = rp ^ 1;
     const int jb = T.b0 + lane * V;
     const bool act = jb < P;
     const bool bcore = core_band(g, T.b0, T.be);
-    const long long hplane = (long long)g.nx * g.Ph;
     const int sc0 = g.src_off[tile], se = g.src_off[tile + 1];
     const int rc0 = g.rx_off[tile], re = g.rx_off[tile + 1];
 
@@ -125,125 +243,36 @@ __global__ void __launch_bounds__(32 * MARCH_WARPS) k_forward_march(const GridDe
         const float* hxR = g.hx[rp] + so;
         const float* hyR = g.hy[rp] + so;
         const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-
-        float ezc[V], hyu[V];
-        ldv<V>(g, ezc, ezR + (long long)T.i0 * P + jb, act);
+        FwdMarch<V> M;
+        ldv<V>(g, M.ezc, ezR + T.i0 * P + jb, act);
 #pragma unroll
-        for (int v = 0; v < V; ++v) hyu[v] = 0.f;
+        for (int v = 0; v < V; ++v) M.hyu[v] = 0.f;
         if (T.i0 >= 1) {
             // new Hy of the row above the chunk, from the old state (auxiliaries read only)
             const int ih = T.i0 - 1;
             float ea[V], ha[V], ca[V];
-            ldv<V>(g, ea, ezR + (long long)ih * P + jb, act);
-            ldv<V>(g, ha, hyR + (long long)ih * P + jb, act);
-            ldcv<V>(g, ca, g.ch + (long long)ih * P + jb, act);
+            ldv<V>(g, ea, ezR + ih * P + jb, act);
+            ldv<V>(g, ha, hyR + ih * P + jb, act);
+            ldcv<V>(g, ca, g.ch + ih * P + jb, act);
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 float hx_unused = 0.f, h = ha[v];
                 if (jb + v < ny)
-                    h_update<false, false, true>(g, ih, jb + v, hx_unused, h, 0.f, __fsub_rn(ezc[v], ea[v]), ca[v],
+                    h_update<false, false, true>(g, ih, jb + v, hx_unused, h, 0.f, __fsub_rn(M.ezc[v], ea[v]), ca[v],
                                                  rd, rd);
-                hyu[v] = h;
+                M.hyu[v] = h;
             }
         }
-        FwdRow<V> B, Bn;
-        fwd_row_load<V>(g, B, ezR, hxR, hyR, T.i0, jb, lane, T.b0, T.be, act);
         int sc = sc0, rc = rc0;
-
-        for (int i = T.i0; i < T.i1; ++i) {
-            if (i + 1 < T.i1) fwd_row_load<V>(g, Bn, ezR, hxR, hyR, i + 1, jb, lane, T.b0, T.be, act);
-            const bool core = bcore && core_row(g, i);
-            // ---- H of row i
-            float right = __shfl_down_sync(FULL, ezc[0], 1);
-            if (lane == 31) right = B.ezR;
-            float hx[V], hy[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                hx[v] = B.hx[v];
-                hy[v] = B.hy[v];
-            }
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;
-                    hx[v] = __fsub_rn(hx[v], __fmul_rn(B.ch[v], __fsub_rn(er, ezc[v])));
-                    hy[v] = __fadd_rn(hy[v], __fmul_rn(B.ch[v], __fsub_rn(B.en[v], ezc[v])));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;
-                    if (jb + v < ny)
-                        h_update<true, true, true>(g, i, jb + v, hx[v], hy[v], __fsub_rn(er, ezc[v]),
-                                                   __fsub_rn(B.en[v], ezc[v]), B.ch[v], rd, wr);
-                }
-            }
-            // new Hx of column b0-1: the previous lane's, or recomputed by lane 0
-            float hxl = __shfl_up_sync(FULL, hx[V - 1], 1);
-            if (lane == 0) {
-                hxl = 0.f;
-                if (T.b0 > 0) {
-                    float h = B.hxL, hy_unused = 0.f;
-                    h_update<false, true, false>(g, i, T.b0 - 1, h, hy_unused, __fsub_rn(ezc[0], B.ezL), 0.f, B.chL,
-                                                 rd, rd);
-                    hxl = h;
-                }
-            }
-            // ---- E of row i
-            float ezw[V];
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float l = (v > 0) ? hx[(v + V - 1) % V] : hxl;
-                    ezw[v] = __fmaf_rn(-B.cb[v], __fsub_rn(hx[v], l),
-                                       madd2(B.ca[v], ezc[v], B.cb[v], __fsub_rn(hy[v], hyu[v])));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float l = (v > 0) ? hx[(v + V - 1) % V] : hxl;
-                    ezw[v] = ezc[v];
-                    if (jb + v < ny)
-                        ezw[v] = e_update<true>(g, i, jb + v, ezc[v], __fsub_rn(hy[v], hyu[v]), __fsub_rn(hx[v], l),
-                                                B.ca[v], B.cb[v], rd, wr);
-                }
-            }
-            // Hertzian dipole (sourcereceiver.cu:84)
-            while (sc < se) {
-                const Ev e = __ldg(g.src_ev + sc);
-                if (e.x != i || e.y != q) break;
-#pragma unroll
-                for (int v = 0; v < V; ++v)
-                    if (jb + v == e.z) {
-                        const float cd = ldc1(g, g.cd + (long long)i * P + e.z);
-                        ezw[v] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
-                    }
-                ++sc;
-            }
-            if (act) {
-                const long long o = so + (long long)i * P + jb;
-                st_state<V>(g, g.ez[wp] + o, ezw);
-                st_state<V>(g, g.hx[wp] + o, hx);
-                st_state<V>(g, g.hy[wp] + o, hy);
-            }
-            if (g.hist && jb < g.Ph)
-                st_state<V>(g, g.hist + ((long long)t * g.S + s) * hplane + (long long)i * g.Ph + jb, ezw);
-            while (rc < re) {
-                const Ev e = __ldg(g.rx_ev + rc);
-                if (e.x != i || e.y != q) break;
-                if (t + 1 < g.nt) {
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        if (jb + v == e.z) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezw[v];
-                }
-                ++rc;
-            }
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                ezc[v] = B.en[v];
-                hyu[v] = hy[v];
-            }
-            B = Bn;
+        // double-buffered row operands: X holds row i, Y is being loaded with row i+1
+        FwdRow<V> X, Y;
+        fwd_row_load<V>(g, X, ezR, hxR, hyR, T.i0, jb, lane, T.b0, T.be, act);
+        for (int i = T.i0; i < T.i1; i += 2) {
+            if (i + 1 < T.i1) fwd_row_load<V>(g, Y, ezR, hxR, hyR, i + 1, jb, lane, T.b0, T.be, act);
+            fwd_row<V>(g, M, X, i, t, q, s, so, jb, lane, T.b0, bcore, act, rd, wr, sc, se, rc, re);
+            if (i + 1 >= T.i1) break;
+            if (i + 2 < T.i1) fwd_row_load<V>(g, X, ezR, hxR, hyR, i + 2, jb, lane, T.b0, T.be, act);
+            fwd_row<V>(g, M, Y, i + 1, t, q, s, so, jb, lane, T.b0, bcore, act, rd, wr, sc, se, rc, re);
         }
     }
 }
@@ -295,9 +324,8 @@ __device__ __forceinline__ void adj_e_march(const GridDev& g, const AdjRow<V>& B
     float ez[V];
 #pragma unroll
     for (int v = 0; v < V; ++v) ez[v] = B.ez[v];
-    while (cur < end) {
+    while (ev_seek(g.inj_ev, cur, end, r, q)) {
         const Ev e = __ldg(g.inj_ev + cur);
-        if (e.x != r || e.y != q) break;
 #pragma unroll
         for (int v = 0; v < V; ++v)
             if (jb + v == e.z) ez[v] = __fsub_rn(ez[v], resid_s[e.w]);
@@ -326,9 +354,8 @@ template <int V>
 __device__ __forceinline__ float adj_e_col(const GridDev& g, const AdjRow<V>& B, float huR, int r, int q, int be,
                                            const float* resid_s, int& cur, int end, const PsiShot& rd, bool active) {
     float ez = B.ezR;
-    while (cur < end) {
+    while (ev_seek(g.injh_ev, cur, end, r, q)) {
         const Ev e = __ldg(g.injh_ev + cur);
-        if (e.x != r || e.y != q) break;
         if (active) ez = __fsub_rn(ez, resid_s[e.w]);
         ++cur;
     }
@@ -393,71 +420,73 @@ __global__ void __launch_bounds__(32 * MARCH_WARPS) k_adjoint_march(const GridDe
         }
         float ecol = adj_e_col<V>(g, B, huR, T.i0, q, T.be, resid_s, hc, he, rd, lane == 31);
 
-        for (int i = T.i0; i < T.i1; ++i) {
-            const int r = i + 1;
-            if (r + 1 < nx && r + 1 <= T.i1)
-                adj_row_load<V>(g, Bnn, ezR, hxR, hyR, f1, f0, r + 1, jb, lane, T.b0, T.be, act, r + 1 < T.i1);
-            // ---- E of row r (the next chunk's row when r == i1: auxiliaries not stored)
-            float ezr[V], ecol_r = 0.f;
-#pragma unroll
-            for (int v = 0; v < V; ++v) ezr[v] = 0.f;
-            if (r < nx) {
-                float hxl = __shfl_up_sync(FULL, Bn.hx[V - 1], 1);
-                if (lane == 0) hxl = Bn.hxL;
-                const bool core_r = bcore && core_row(g, r);
-                if (r < T.i1)
-                    adj_e_march<V, true>(g, Bn, B.hy, hxl, r, q, jb, core_r, resid_s, ic, ie, rd, wr, ezr);
-                else
-                    adj_e_march<V, false>(g, Bn, B.hy, hxl, r, q, jb, core_r, resid_s, ic, ie, rd, rd, ezr);
-                if (r < T.i1) ecol_r = adj_e_col<V>(g, Bn, B.hyR, r, q, T.be, resid_s, hc, he, rd, lane == 31);
-            }
-            // ---- H of row i from E_new of rows i and i+1, imaging
-            float right = __shfl_down_sync(FULL, ezc[0], 1);
-            if (lane == 31) right = ecol;
-            float hx[V], hy[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                hx[v] = B.hx[v];
-                hy[v] = B.hy[v];
-            }
-            const bool core = bcore_band && core_row(g, i);
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;
-                    hx[v] = __fsub_rn(hx[v], __fmul_rn(B.ch[v], __fsub_rn(er, ezc[v])));
-                    hy[v] = __fadd_rn(hy[v], __fmul_rn(B.ch[v], __fsub_rn(ezr[v], ezc[v])));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;
-                    if (jb + v < ny)
-                        h_update<true, true, true>(g, i, jb + v, hx[v], hy[v], __fsub_rn(er, ezc[v]),
-                                                   __fsub_rn(ezr[v], ezc[v]), B.ch[v], rd, wr);
-                }
-            }
-            {
-                float* ae = acc + ((i - T.i0) * 32 + lane) * V;
-                float* as = ae + rows * 32 * V;
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    ae[v] = __fadd_rn(ae[v], __fmul_rn(__fsub_rn(B.f1[v], B.f0[v]), ezc[v]));
-                    as[v] = __fadd_rn(as[v], __fmul_rn(__fmul_rn(B.f1[v], ezc[v]), g.dt));
-                }
-            }
-            if (act) {
-                const long long o = so + (long long)i * P + jb;
-                st_state<V>(g, g.ez[wp] + o, ezc);
-                st_state<V>(g, g.hx[wp] + o, hx);
-                st_state<V>(g, g.hy[wp] + o, hy);
-            }
-#pragma unroll
-            for (int v = 0; v < V; ++v) ezc[v] = ezr[v];
-            ecol = ecol_r;
-            B = Bn;
-            Bn = Bnn;
+#define FG_ADJ_ITER(CUR, NXT, LD)                                                                              \
+    {                                                                                                          \
+        const int r = i + 1;                                                                                   \
+        if (r + 1 < nx && r + 1 <= T.i1)                                                                       \
+            adj_row_load<V>(g, LD, ezR, hxR, hyR, f1, f0, r + 1, jb, lane, T.b0, T.be, act, r + 1 < T.i1);     \
+        float ezr[V], ecol_r = 0.f;                                                                            \
+        _Pragma("unroll") for (int v = 0; v < V; ++v) ezr[v] = 0.f;                                            \
+        if (r < nx) {                                                                                          \
+            float hxl = __shfl_up_sync(FULL, NXT.hx[V - 1], 1);                                                \
+            if (lane == 0) hxl = NXT.hxL;                                                                      \
+            const bool core_r = bcore && core_row(g, r);                                                       \
+            if (r < T.i1) {                                                                                    \
+                adj_e_march<V, true>(g, NXT, CUR.hy, hxl, r, q, jb, core_r, resid_s, ic, ie, rd, wr, ezr);     \
+                ecol_r = adj_e_col<V>(g, NXT, CUR.hyR, r, q, T.be, resid_s, hc, he, rd, lane == 31);           \
+            } else {                                                                                           \
+                adj_e_march<V, false>(g, NXT, CUR.hy, hxl, r, q, jb, core_r, resid_s, ic, ie, rd, rd, ezr);    \
+            }                                                                                                  \
+        }                                                                                                      \
+        float right = __shfl_down_sync(FULL, ezc[0], 1);                                                       \
+        if (lane == 31) right = ecol;                                                                          \
+        float hx[V], hy[V];                                                                                    \
+        _Pragma("unroll") for (int v = 0; v < V; ++v) {                                                        \
+            hx[v] = CUR.hx[v];                                                                                 \
+            hy[v] = CUR.hy[v];                                                                                 \
+        }                                                                                                      \
+        if (bcore_band && core_row(g, i)) {                                                                    \
+            _Pragma("unroll") for (int v = 0; v < V; ++v) {                                                    \
+                const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;                                       \
+                hx[v] = __fsub_rn(hx[v], __fmul_rn(CUR.ch[v], __fsub_rn(er, ezc[v])));                         \
+                hy[v] = __fadd_rn(hy[v], __fmul_rn(CUR.ch[v], __fsub_rn(ezr[v], ezc[v])));                     \
+            }                                                                                                  \
+        } else {                                                                                               \
+            _Pragma("unroll") for (int v = 0; v < V; ++v) {                                                    \
+                const float er = (v + 1 < V) ? ezc[(v + 1) % V] : right;                                       \
+                if (jb + v < ny)                                                                               \
+                    h_update<true, true, true>(g, i, jb + v, hx[v], hy[v], __fsub_rn(er, ezc[v]),              \
+                                               __fsub_rn(ezr[v], ezc[v]), CUR.ch[v], rd, wr);                  \
+            }                                                                                                  \
+        }                                                                                                      \
+        {                                                                                                      \
+            float* ae = acc + ((i - T.i0) * 32 + lane) * V;                                                    \
+            float* as = ae + rows * 32 * V;                                                                    \
+            _Pragma("unroll") for (int v = 0; v < V; ++v) {                                                    \
+                ae[v] = __fadd_rn(ae[v], __fmul_rn(__fsub_rn(CUR.f1[v], CUR.f0[v]), ezc[v]));                  \
+                as[v] = __fadd_rn(as[v], __fmul_rn(__fmul_rn(CUR.f1[v], ezc[v]), g.dt));                       \
+            }                                                                                                  \
+        }                                                                                                      \
+        if (act) {                                                                                             \
+            const long long o = so + (long long)i * P + jb;                                                    \
+            st_state<V>(g, g.ez[wp] + o, ezc);                                                                 \
+            st_state<V>(g, g.hx[wp] + o, hx);                                                                  \
+            st_state<V>(g, g.hy[wp] + o, hy);                                                                  \
+        }                                                                                                      \
+        _Pragma("unroll") for (int v = 0; v < V; ++v) ezc[v] = ezr[v];                                         \
+        ecol = ecol_r;                                                                                         \
+    }
+
+        // rotating row operands: iteration i uses (row i, row i+1) and loads row i+2
+        for (int i = T.i0; i < T.i1;) {
+            FG_ADJ_ITER(B, Bn, Bnn)
+            if (++i >= T.i1) break;
+            FG_ADJ_ITER(Bn, Bnn, B)
+            if (++i >= T.i1) break;
+            FG_ADJ_ITER(Bnn, B, Bn)
+            ++i;
         }
+#undef FG_ADJ_ITER
     }
     // group sums into the fp64 accumulators
     double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
