@@ -1,0 +1,529 @@
+"""Benchmark of the TMz FDTD hot path: one forward solve plus one
+reference-mode gradient solve per step, in Gcell-steps/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload config2] [--shots S] [--nt NT] [--tuning JSON]
+
+Workload (default): the batched multi-shot gradient case -- a 400x300
+physical model padded by 20 CPML cells per side (compute grid 440x340),
+dx = 0.025 m, 64 shots, nt = 4000, 200 MHz Ricker, 100 receivers, layered
+eps_r/sigma model generated from a fixed seed (synthetic data, no dataset).
+The full Ez history (nt x 64 x 440 x 340 float32, 153 GB) stays resident in
+HBM between the forward and the adjoint.
+
+A step is compute()'s forward (traces + history) followed by the
+reference-mode adjoint (imaging sums, L2-normalised): the path
+GPRFWI.forward / GPRFWI.backward of the reference (src/compute.py:877-942)
+with tv=False.  Gcell-steps/s fwd+adjoint = nx * ny * shots * nt / step time:
+one unit per cell-step solved forward and back (the throughput definition
+of the reference's epoch timings, cells x shots x steps / epoch time).
+
+  value      device-resident inputs, CUDA events on the solve stream
+  e2e        through the public compute() API: er/se/mr and the residual
+             copied from pinned host memory, traces and both gradients
+             copied back, every step
+  roofline   the dominant kernel (the adjoint step kernel): algorithmic bytes
+             per launch / its mean launch time, against the measured HBM
+             copy bandwidth
+  cpu_baseline  the CPU oracle (a C++/OpenMP restatement of the reference's
+             update equations) on a bounded sample of the same workload
+
+--impl reference prints the reference arm: the reference's update
+equations on the host cores (the reference has no CPU code of its own; its
+kernels are CUDA only), through the same CPU restatement, on a bounded sample.
+
+Under torchrun (N > 1) every rank solves its own 64-shot batch (weak
+scaling) and the unnormalised imaging sums are summed across ranks with one
+NCCL all-reduce before the normalisation, as a multi-GPU gradient needs.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+PKG = "fast-gpr-fwi_b200"
+
+METRIC = "Gcell-steps/s fwd+adjoint"
+UNIT = "Gcell-steps/s"
+
+# DRAM bytes per shot-cell-step of the step kernels measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, see profiles/); None until
+# a capture of the current kernels exists.
+NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": None, "adjoint": None}
+
+
+def _fg():
+    return importlib.import_module(PKG)
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--shots", type=int, default=None)
+    ap.add_argument("--nt", type=int, default=None)
+    ap.add_argument("--tuning", default=None, help="JSON dict of fg_tuning fields")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample length")
+    return ap.parse_args()
+
+
+def workload(args):
+    fg = _fg()
+    gen = fg.workloads.CONFIGS[args.workload]
+    kw = {}
+    if args.workload == "config2":
+        if args.shots:
+            kw["shots"] = args.shots
+        if args.nt:
+            kw["nt"] = args.nt
+    wl = gen(**kw)
+    if args.workload != "config2":
+        if args.shots:
+            wl.shots = args.shots
+        if args.nt:
+            wl.nt = args.nt
+    return wl
+
+
+# ---------------------------------------------------------------------------
+# byte model (algorithmic bytes; FP32 TMz)
+# ---------------------------------------------------------------------------
+
+def strip_cells(nx, ny, th):
+    """Cells inside at least one CPML slab (x strips + y strips)."""
+    if th <= 0:
+        return 0
+    return 2 * th * ny + 2 * th * nx
+
+
+def algorithmic_bytes(nx, ny, shots, th):
+    """Per launch of the forward / adjoint step kernel.
+
+    forward: Ez/Hx/Hy read + write (24 B per shot-cell), Ca/Cb (8 B per cell,
+    shared by the shots), two CPML auxiliaries read + write per strip cell
+    (16 B per shot-strip-cell), the Ez history write (4 B per shot-cell).
+    adjoint: the same plus the history read instead of its write, and the
+    two imaging accumulators read + write (16 B per cell).
+    """
+    N = nx * ny
+    P = strip_cells(nx, ny, th)
+    fwd = 24 * shots * N + 8 * N + 16 * shots * P + 4 * shots * N
+    adj = 24 * shots * N + 8 * N + 16 * shots * P + 4 * shots * N + 16 * N
+    return fwd, adj
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    return rank, local, world
+
+
+def barrier(world):
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(x: float, world: int, dev) -> float:
+    if world <= 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank, local, world):
+    fg = _fg()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wl = workload(args)
+    tuning = json.loads(args.tuning) if args.tuning else None
+    kw = wl.kwargs(dev, tv=False)
+    er_d = torch.tensor(wl.er, device=dev)
+    se_d = torch.tensor(wl.se, device=dev)
+    mr_d = torch.tensor(wl.mr, device=dev)
+    setup = fg.grid.build_setup(dev, kw["dx"], kw["ny"], kw["nx"], kw["nz"], kw["time_windows"], kw["source"],
+                                kw["source_location"], kw["source_step"], kw["receiver_location"],
+                                kw["receiver_step"], kw["pmlthick"], kw["source_apmlitudes"], kw["step"],
+                                torch.clamp(kw["er"], min=1), kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"], None,
+                                None, kw["Fixedreceiver"], None, None)
+    nx, ny, S, nt = setup.nx, setup.ny, setup.shots, setup.nt
+    solve = fg.Solve(dev, setup, tuning=tuning, tv=False)
+    plan = solve.plan
+    nrx = plan.nrx
+    stream = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    resid = torch.randn((S, nt, nrx), device=dev, generator=gen, dtype=torch.float32) * 1e-3
+    traces = torch.empty((S, nt, nrx), dtype=torch.float32, device=dev)
+    hist = torch.empty((nt, S, nx, plan.hist_pitch), dtype=torch.float32, device=dev)
+    ge = torch.empty((nx, ny), dtype=torch.float32, device=dev)
+    gs = torch.empty((nx, ny), dtype=torch.float32, device=dev)
+
+    def one_step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        plan.forward(er_d, se_d, mr_d, traces, hist)
+        if ev is not None:
+            ev[1].record(stream)
+        if world > 1:
+            plan.adjoint_reference(er_d, se_d, mr_d, hist, resid, ge, gs, normalize=False)
+            torch.distributed.all_reduce(ge)
+            torch.distributed.all_reduce(gs)
+            ge.div_(torch.linalg.vector_norm(ge))
+            gs.div_(torch.linalg.vector_norm(gs))
+        else:
+            plan.adjoint_reference(er_d, se_d, mr_d, hist, resid, ge, gs, normalize=True)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize(dev)
+    plan.device_check()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        one_step(evs[k])
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clk = clocks.stop()
+    ms_total = t0.elapsed_time(t1)
+    fwd_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    adj_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    plan.device_check()
+    ms_total = max_over_ranks(ms_total, world, dev)
+    ms_step = ms_total / args.steps
+    cell_steps = nx * ny * S * nt
+    value = world * cell_steps / (ms_step * 1e-3) / 1e9
+
+    # roofline of the dominant kernel (adjoint step kernel, nt-1 launches per adjoint)
+    fwd_b, adj_b = algorithmic_bytes(nx, ny, S, setup.th)
+    peak, peak_kind = measured_peaks()
+    fwd_launch_ms = float(np.median(fwd_ms)) / nt
+    adj_launch_ms = float(np.median(adj_ms)) / (nt - 1)
+    dom = "adjoint" if np.median(adj_ms) >= np.median(fwd_ms) else "forward"
+    bytes_launch = adj_b if dom == "adjoint" else fwd_b
+    launch_ms = adj_launch_ms if dom == "adjoint" else fwd_launch_ms
+    achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+    ncu = NCU_BYTES_PER_SHOT_CELL_STEP[dom]
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": None if ncu is None else int(ncu * S * nx * ny),
+                "kernel": "k_%s_step (%s)" % (dom, "adjoint_reference" if dom == "adjoint" else "forward"),
+                "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 5)}
+    other = {"forward": {"launch_ms": round(fwd_launch_ms, 5), "algorithmic_bytes_per_launch": int(fwd_b),
+                         "achieved_gbs": round(fwd_b / (fwd_launch_ms * 1e-3) / 1e9, 1),
+                         "phase_ms": round(float(np.median(fwd_ms)), 3)},
+             "adjoint": {"launch_ms": round(adj_launch_ms, 5), "algorithmic_bytes_per_launch": int(adj_b),
+                         "achieved_gbs": round(adj_b / (adj_launch_ms * 1e-3) / 1e9, 1),
+                         "phase_ms": round(float(np.median(adj_ms)), 3)}}
+    del hist, traces
+    torch.cuda.empty_cache()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, fg, wl, dev, rank, world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(wl, setup, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%s: %dx%d compute grid (incl. 2x%d CPML), dx=%g m, %d shots, nt=%d, "
+                                   "%d receivers, %.0f MHz Ricker, fwd + reference-mode adjoint, tv=False"
+                                   % (wl.name, nx, ny, setup.th, setup.dx, S, nt, nrx, wl.freq / 1e6),
+                       "shots_per_gpu": S, "nx": nx, "ny": ny, "nt": nt,
+                       "history_gb": round(nt * S * nx * plan.hist_pitch * 4 / 1e9, 1),
+                       "l2": "inputs larger than L2 (state %.0f MB per step, history %.0f GB)"
+                             % (6 * S * (nx + 1) * ((ny + 32) // 32 * 32) * 4 / 1e6,
+                                nt * S * nx * plan.hist_pitch * 4 / 1e9),
+                       "tuning": tuning or "default",
+                       "parallelism": "replicas: shots per GPU, one all-reduce of the imaging sums" if world > 1
+                       else "single GPU"},
+            "gpu_launches": int(args.steps * (2 * nt + 4)),
+            "roofline": roofline,
+            "kernels": other,
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, fg, wl, dev, rank, world):
+    """The same metric through compute() with host buffers, copies inside the timing."""
+    pin = lambda a: torch.tensor(np.ascontiguousarray(a)[:, :, None]).pin_memory()
+    er_h, se_h, mr_h = pin(wl.er), pin(wl.se), pin(wl.mr)
+    S, nt, nrx = wl.shots, wl.nt, wl.nrx
+    rng = np.random.default_rng(99 + rank)
+    resid_h = torch.tensor(rng.standard_normal((S, nt, nrx)).astype(np.float32) * 1e-3).pin_memory()
+    tr_h = torch.empty((S, nt, nrx), dtype=torch.float32).pin_memory()
+    ge_h = torch.empty(er_h.shape, dtype=torch.float32).pin_memory()
+    gs_h = torch.empty(se_h.shape, dtype=torch.float32).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+    tuning = json.loads(args.tuning) if args.tuning else None
+
+    def step():
+        er = er_h.to(dev, non_blocking=True).requires_grad_(True)
+        se = se_h.to(dev, non_blocking=True).requires_grad_(True)
+        mr = mr_h.to(dev, non_blocking=True)
+        g = resid_h.to(dev, non_blocking=True)
+        kw = wl.kwargs(dev, er=er, se=se, mr=mr, tv=False, tuning=tuning)
+        traces, _ = fg.compute(**kw)
+        traces.backward(g)
+        tr_h.copy_(traces.detach(), non_blocking=True)
+        ge_h.copy_(er.grad, non_blocking=True)
+        gs_h.copy_(se.grad, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = max_over_ranks(t0.elapsed_time(t1), world, dev) / args.steps
+    torch.cuda.empty_cache()
+    cells = wl.nx * wl.ny * S * nt
+    h2d = 3 * er_h.numel() * 4 + resid_h.numel() * 4
+    d2h = tr_h.numel() * 4 + ge_h.numel() * 4 + gs_h.numel() * 4
+    return {"value": round(world * cells / (ms * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_step": round(ms, 3),
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "api": "compute(..., tv=False) + traces.backward(resid)"}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle: test infrastructure, used here only as the timed baseline)
+# ---------------------------------------------------------------------------
+
+def _cpu_problem(wl, setup, shots, nt):
+    """Oracle problem for a sample of the workload: the first `shots` shots,
+    the first `nt` steps, float32 coefficients restated on the host."""
+    from oracle import oracle as orc
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers
+    coef = helpers.coefficients_f32(np.maximum(wl.er, 1), np.maximum(wl.se, 0), wl.mr, setup.dt32, setup.dx)
+    pml = setup.profile.packed() if setup.profile is not None else np.zeros((8, 0), np.float32)
+    src = orc.positions2(setup.src.cpu().numpy()[:shots], wl.nx, wl.ny)
+    rx = orc.positions2(setup.rx.cpu().numpy()[:shots], wl.nx, wl.ny)
+    return orc.Problem(wl.nx, wl.ny, setup.th, shots, nt, setup.dx, setup.dt32, coef["uE0"], coef["uE1"],
+                       coef["uE4"], coef["uH1"], coef["uH4"], coef["uE0a"], pml, src,
+                       np.ascontiguousarray(setup.srcw[:, :nt]), rx)
+
+
+def _cpu_sample_run(prob):
+    from oracle import oracle as orc
+    rng = np.random.default_rng(5)
+    resid = rng.standard_normal((prob.shots, prob.nt, prob.rx.shape[1])).astype(np.float32)
+    t0 = time.perf_counter()
+    _, hist = orc.forward(prob, np.float32)
+    orc.adjoint_reference(prob, hist, resid, np.float32)
+    return time.perf_counter() - t0
+
+
+def _cpu_sample(wl, setup, seconds):
+    """Pick a sample (shots, nt) of the workload that runs about `seconds`."""
+    from oracle import oracle as orc
+    threads = orc.set_threads(os.cpu_count() or 1)
+    shots = min(4, wl.shots)
+    nt_cal = min(40, wl.nt)
+    t_cal = _cpu_sample_run(_cpu_problem(wl, setup, shots, nt_cal))
+    per_step = t_cal / nt_cal
+    nt = int(max(nt_cal, min(wl.nt, seconds / max(per_step, 1e-9))))
+    # history memory of the sample: keep it under ~4 GB
+    nt = int(min(nt, 4e9 / (shots * wl.nx * wl.ny * 4)))
+    return shots, nt, threads
+
+
+def cpu_baseline(wl, setup, seconds):
+    shots, nt, threads = _cpu_sample(wl, setup, seconds)
+    t = _cpu_sample_run(_cpu_problem(wl, setup, shots, nt))
+    cells = wl.nx * wl.ny * shots * nt
+    return {"value": round(cells / t / 1e9, 4), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%s grid %dx%d, first %d shots, first %d of %d steps, fwd + reference adjoint, "
+                      "FP32 C++/OpenMP oracle, %.1f s" % (wl.name, wl.nx, wl.ny, shots, nt, wl.nt, t),
+            "cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's update equations on the host cores."""
+    if rank != 0:
+        return
+    fg = _fg()
+    wl = workload(args)
+    kw = wl.kwargs("cpu", tv=False)
+    setup = fg.grid.build_setup("cpu", kw["dx"], kw["ny"], kw["nx"], kw["nz"], kw["time_windows"], kw["source"],
+                                kw["source_location"], kw["source_step"], kw["receiver_location"],
+                                kw["receiver_step"], kw["pmlthick"], kw["source_apmlitudes"], kw["step"],
+                                torch.clamp(kw["er"], min=1), kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"], None,
+                                None, kw["Fixedreceiver"], None, None)
+    seconds = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
+    shots, nt, threads = _cpu_sample(wl, setup, seconds)
+    prob = _cpu_problem(wl, setup, shots, nt)
+    for _ in range(args.warmup):
+        _cpu_sample_run(prob)
+    times = [_cpu_sample_run(prob) for _ in range(args.steps)]
+    t = float(np.sum(times)) / args.steps
+    cells = wl.nx * wl.ny * shots * nt
+    value = cells / t / 1e9
+    sample = ("%s grid %dx%d, first %d shots, first %d of %d steps per step, fwd + reference adjoint, "
+              "FP32 C++/OpenMP restatement of the reference kernels" % (wl.name, wl.nx, wl.ny, shots, nt, wl.nt))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "%s: %dx%d compute grid, %d shots, nt=%d (bounded CPU sample: %d shots x %d steps)"
+                               % (wl.name, wl.nx, wl.ny, wl.shots, wl.nt, shots, nt)},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample, "cpu": _cpu_model()},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, rank, world)
+        return
+    rank, local, world = dist_init(args.gpus)
+    try:
+        run_ours(args, rank, local, world)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
