@@ -28,6 +28,7 @@ FG_ERR_TIMEOUT = 4
 EXPORTS = (
     "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_pitch", "fg_plan_workspace_bytes", "fg_plan_bind",
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
+    "fg_forward_static",
 )
 
 
@@ -99,6 +100,8 @@ def lib() -> ctypes.CDLL:
     L.fg_forward.restype = ctypes.c_int
     L.fg_adjoint_reference.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp]
     L.fg_adjoint_reference.restype = ctypes.c_int
+    L.fg_forward_static.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.fg_forward_static.restype = ctypes.c_int
     L.fg_plan_check.argtypes = [vp, vp]
     L.fg_plan_check.restype = ctypes.c_int
     L.fg_last_error.argtypes = []

@@ -429,6 +429,31 @@ int reset_state(fg_plan* p, cudaStream_t st) {
     return FG_OK;
 }
 
+// Device scratch of fg_forward_static: one array per GPU that loads the
+// library, held until the process exits.  Host code must not pass the
+// symbol itself to a kernel (on the host it names a host-side shadow); the
+// device address comes from cudaGetSymbolAddress, looked up once per device.
+static __device__ __align__(256) unsigned char g_static_scratch[FG_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_ptr[kMaxDevices] = {};
+
+int static_scratch(void** out) {
+    int dev = 0;
+    FG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(FG_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+        g_static_ptr[dev] = ptr;
+    }
+    *out = g_static_ptr[dev];
+    return FG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -644,6 +669,26 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     fg::k_grad_scale<<<blocks, 256, 0, st>>>(sums, nrm, (long long)n, normalize, grad_eps, grad_sig);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
+}
+
+int fg_forward_static(fg_plan* p, const float* er, const float* se, const float* mr, float* traces, float* hist,
+                      void* stream) {
+    if (!p) return fail(FG_ERR_INVALID, "fg_forward_static: NULL plan");
+    if (p->total > (size_t)FG_STATIC_SCRATCH_BYTES)
+        return fail(FG_ERR_WORKSPACE, "fg_forward_static: the plan needs " + std::to_string(p->total) +
+                                          " bytes of scratch, more than the static " +
+                                          std::to_string((long long)FG_STATIC_SCRATCH_BYTES));
+    void* scratch = nullptr;
+    int rc = static_scratch(&scratch);
+    if (rc) return rc;
+    char* saved = p->ws;
+    const int64_t saved_bytes = p->ws_bytes;
+    rc = fg_plan_bind(p, scratch, (int64_t)FG_STATIC_SCRATCH_BYTES, stream);
+    if (rc == FG_OK) rc = fg_forward(p, er, se, mr, traces, hist, stream);
+    p->ws = saved;
+    p->ws_bytes = saved_bytes;
+    if (saved) fill_grid(p);
+    return rc;
 }
 
 }  // extern "C"

@@ -117,6 +117,38 @@ int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const 
                          const float* hist, const float* resid, float* grad_eps, float* grad_sig,
                          int32_t normalize, double* norms, void* stream);
 
+/* Forward solve that allocates no device memory: no counterpart in the
+ * reference (whose launchers take buffers allocated by torch).
+ *
+ * For callers that cannot call cudaMalloc: cudaMalloc and cudaFree may
+ * synchronise the whole device, which a host loop driving other streams in
+ * real time cannot afford, and some host applications hand all device memory
+ * to their own pool up front, leaving nothing for a library to allocate.
+ * Such a caller still allocates the inputs and outputs (er, se, mr, traces,
+ * hist, exactly as for fg_forward) and builds the plan with fg_plan_create,
+ * which touches host memory only; this call then runs fg_forward with the
+ * plan's device scratch placed in one array of FG_STATIC_SCRATCH_BYTES that
+ * the library holds in device memory of every GPU that loads it, until the
+ * process exits.  The plan's own workspace binding (fg_plan_bind), if any,
+ * is left as it was.
+ *
+ *   - A plan whose fg_plan_workspace_bytes exceeds FG_STATIC_SCRATCH_BYTES
+ *     is rejected with FG_ERR_WORKSPACE before any device work.
+ *   - The first call on a device looks up the array's device address (with
+ *     that device current) and keeps it; make that first call before any
+ *     stream capture.
+ *   - The call waits for `stream` once, after uploading the plan's tables
+ *     (as fg_plan_bind does), then queues the solve asynchronously.
+ *   - Every call on a device shares the one array and the array keeps what
+ *     the last call left in it; each call clears the field state it needs.
+ *     Calls whose work overlaps on the GPU (other streams, other threads)
+ *     race on the array: serialise them.
+ *   - Device-side error words of the checked build land in the array, not in
+ *     the plan's workspace, so fg_plan_check does not see them. */
+#define FG_STATIC_SCRATCH_BYTES (32LL * 1024 * 1024)
+int fg_forward_static(fg_plan* plan, const float* er, const float* se, const float* mr,
+                      float* traces, float* hist, void* stream);
+
 /* Wait for the plan's work on `stream`, then read and clear the device-side
  * error word its kernels set (an out-of-range access caught by the checked
  * build, or a bounded wait that gave up).  Returns FG_OK, FG_ERR_TIMEOUT or
