@@ -257,7 +257,7 @@ def run_ours(args, rank, local, world):
     gen.manual_seed(1234 + rank)
     resid = torch.randn((S, nt, nrx), device=dev, generator=gen, dtype=torch.float32) * 1e-3
     traces = torch.empty((S, nt, nrx), dtype=torch.float32, device=dev)
-    hist = torch.empty((nt, S, nx, plan.hist_pitch), dtype=torch.float32, device=dev)
+    hist = plan.new_hist()
     ge = torch.empty((nx, ny), dtype=torch.float32, device=dev)
     gs = torch.empty((nx, ny), dtype=torch.float32, device=dev)
 
@@ -319,7 +319,7 @@ def run_ours(args, rank, local, world):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None if ncu is None else int(ncu * S * nx * ny),
-                "kernel": "k_%s_step (%s)" % (dom, "adjoint_reference" if dom == "adjoint" else "forward"),
+                "kernel": "fg::k_adj (reference adjoint step)" if dom == "adjoint" else "fg::k_fwd (forward step)",
                 "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 5)}
     other = {"forward": {"launch_ms": round(fwd_launch_ms, 5), "algorithmic_bytes_per_launch": int(fwd_b),
                          "achieved_gbs": round(fwd_b / (fwd_launch_ms * 1e-3) / 1e9, 1),
@@ -347,10 +347,9 @@ def run_ours(args, rank, local, world):
                                    "%d receivers, %.0f MHz Ricker, fwd + reference-mode adjoint, tv=False"
                                    % (wl.name, nx, ny, setup.th, setup.dx, S, nt, nrx, wl.freq / 1e6),
                        "shots_per_gpu": S, "nx": nx, "ny": ny, "nt": nt,
-                       "history_gb": round(nt * S * nx * plan.hist_pitch * 4 / 1e9, 1),
-                       "l2": "inputs larger than L2 (state %.0f MB per step, history %.0f GB)"
-                             % (6 * S * (nx + 1) * ((ny + 32) // 32 * 32) * 4 / 1e6,
-                                nt * S * nx * plan.hist_pitch * 4 / 1e9),
+                       "history_gb": round(plan.hist_floats * 4 / 1e9, 1),
+                       "l2": "inputs larger than L2 (state %.0f MB read + written per step, history %.0f GB)"
+                             % (plan.workspace.numel() / 1e6, plan.hist_floats * 4 / 1e9),
                        "tuning": tuning or "default",
                        "parallelism": "replicas: shots per GPU, one all-reduce of the imaging sums" if world > 1
                        else "single GPU"},

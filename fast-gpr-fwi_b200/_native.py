@@ -26,7 +26,7 @@ FG_ERR_TIMEOUT = 4
 
 # Every entry point include/fastgpr.h declares (checked by the tests).
 EXPORTS = (
-    "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_pitch", "fg_plan_workspace_bytes", "fg_plan_bind",
+    "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_shape", "fg_plan_workspace_bytes", "fg_plan_bind",
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
     "fg_forward_static",
 )
@@ -45,11 +45,11 @@ class FgProblem(ctypes.Structure):
 
 class FgTuning(ctypes.Structure):
     _fields_ = [
-        ("kernel", ctypes.c_int32), ("cols_per_thread", ctypes.c_int32), ("shots_per_tile", ctypes.c_int32),
-        ("rows_per_tile", ctypes.c_int32), ("warps_per_tile", ctypes.c_int32), ("stages", ctypes.c_int32),
+        ("lanes", ctypes.c_int32), ("cells_per_thread", ctypes.c_int32), ("rows_per_tile", ctypes.c_int32),
+        ("warps_per_block", ctypes.c_int32), ("stages", ctypes.c_int32), ("kernel", ctypes.c_int32),
     ]
 
-    KEYS = ("kernel", "cols_per_thread", "shots_per_tile", "rows_per_tile", "warps_per_tile", "stages")
+    KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel")
 
 
 class FastGprError(RuntimeError):
@@ -88,8 +88,8 @@ def lib() -> ctypes.CDLL:
     L.fg_plan_create.restype = ctypes.c_int
     L.fg_plan_destroy.argtypes = [vp]
     L.fg_plan_destroy.restype = ctypes.c_int
-    L.fg_plan_hist_pitch.argtypes = [vp]
-    L.fg_plan_hist_pitch.restype = i32
+    L.fg_plan_hist_shape.argtypes = [vp, ctypes.POINTER(i64)]
+    L.fg_plan_hist_shape.restype = ctypes.c_int
     L.fg_plan_workspace_bytes.argtypes = [vp]
     L.fg_plan_workspace_bytes.restype = i64
     L.fg_plan_bind.argtypes = [vp, vp, i64, vp]
@@ -156,7 +156,10 @@ class Plan:
         check(L.fg_plan_create(ctypes.byref(prob), ctypes.byref(tune) if tune is not None else None,
                                ctypes.byref(handle)))
         self._h = handle
-        self.hist_pitch = int(L.fg_plan_hist_pitch(handle))
+        shape = (ctypes.c_int64 * 5)()
+        check(L.fg_plan_hist_shape(handle, shape))
+        self.hist_shape = tuple(int(v) for v in shape)   # (nt, groups, nx, pitch, slots)
+        self.hist_floats = int(np.prod(self.hist_shape))
         nbytes = int(L.fg_plan_workspace_bytes(handle))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         check(L.fg_plan_bind(handle, self.workspace.data_ptr(), nbytes, stream_handle(self.device)))
@@ -170,6 +173,16 @@ class Plan:
         if h is not None and _lib is not None:
             _lib.fg_plan_destroy(h)
             self._h = None
+
+    def new_hist(self) -> torch.Tensor:
+        """An uninitialised Ez history buffer for this plan (flat float32)."""
+        return torch.empty(self.hist_floats, dtype=torch.float32, device=self.device)
+
+    def hist_view(self, hist: torch.Tensor) -> torch.Tensor:
+        """History as (nt, shots, nx, ny) (a copy when shots share cells)."""
+        nt, groups, nx, pitch, slots = self.hist_shape
+        h = hist.view(nt, groups, nx, pitch, slots).permute(0, 1, 4, 2, 3).reshape(nt, groups * slots, nx, pitch)
+        return h[:, :self.shots, :, :self.ny]
 
     def device_check(self):
         """Synchronise and raise if a kernel recorded a device-side error."""

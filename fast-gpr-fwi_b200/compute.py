@@ -70,10 +70,7 @@ class Solve:
         s = self.setup
         er32, se32, mr32 = self.materials(er, se, mr)
         traces = torch.empty((s.shots, s.nt, self.plan.nrx), dtype=torch.float32, device=self.device)
-        hist = None
-        if keep_history:
-            hist = torch.empty((s.nt, s.shots, s.nx, self.plan.hist_pitch), dtype=torch.float32,
-                               device=self.device)
+        hist = self.plan.new_hist() if keep_history else None
         self.plan.forward(er32, se32, mr32, traces, hist)
         return traces, hist
 

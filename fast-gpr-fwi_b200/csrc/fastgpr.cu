@@ -7,14 +7,15 @@
 #include <string>
 #include <vector>
 
-#include "../../include/fastgpr.h"
-#include "fdtd_kernels.cuh"
-#include "fdtd_tma.cuh"
-#include "fdtd_tile.cuh"
-#include "fdtd_march.cuh"
+#include <cudaTypedefs.h>
 
+#include "../../include/fastgpr.h"
+#include "fdtd_common.cuh"
+#include "fdtd_lanes.cuh"
+#include "fdtd_tile.cuh"
+
+using fg::Dev;
 using fg::Ev;
-using fg::GridDev;
 
 namespace {
 
@@ -29,9 +30,9 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail(FG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define FG_CUDA(call)                                   \
-    do {                                                \
-        cudaError_t e_ = (call);                        \
+#define FG_CUDA(call)                                       \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
@@ -45,20 +46,28 @@ struct fg_plan {
     float dx, dt;
     std::vector<int32_t> src, rx;
     std::vector<float> srcw, pml;
-    // tiling
-    int kernel, V, G, TI, NW, D;
-    int P, TY, Ph, nb, nc, ngroups, ntiles, bw;
-    std::vector<int> chunk_row;
-    std::vector<Ev> src_ev, rx_ev, inj_ev, injh_ev;
-    std::vector<int> src_off, rx_off, inj_off, injh_off;
+    // launch shape
+    int kernel;         // 0 = tensor-map tiles, 1 = lane march
+    bool shot;          // shot lanes (CS = 32) or column lanes (CS = 1)
+    int W, TI, WPB, D;  // cells per thread, rows per tile, warps per block, ring stages (0 = direct loads)
+    // tensor maps of the tile kernels (encoded when a workspace is bound)
+    CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
+    int CS, SL;         // floats per cell in a group plane, shots per group
+    int P, TY, Ph, BW, nb, nc, ngroups, ntiles;
+    std::vector<int> chunk_row, order;
+    std::vector<int4> tiles;   // (b0, i0, group, id) per position of `order`
+    std::vector<Ev> src_ev, rx_ev, inj_ev;
+    std::vector<int> src_off, rx_off, inj_off;
     // workspace layout (byte offsets)
-    size_t o_coef, o_state, o_psi, o_chunk, o_srcev, o_rxev, o_injev, o_injhev, o_offs, o_srcw, o_pml, o_gacc,
+    size_t o_coef, o_state, o_psi, o_chunk, o_order, o_tiles, o_ctr, o_srcev, o_rxev, o_injev, o_offs, o_srcw, o_pml, o_gacc,
         o_sums, o_partial, o_norms, o_err, total;
+    // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
+    int fwd_blocks = 0, adj_blocks = 0;
     long long plane, pxs, pys;
     size_t state_bytes, psi_bytes;
     char* ws = nullptr;
     int64_t ws_bytes = 0;
-    GridDev g;
+    Dev g;
 };
 
 namespace {
@@ -74,24 +83,56 @@ int classify(const fg_plan* p, int i, int j, int k) {
 }
 
 void build_tiles(fg_plan* p) {
-    p->P = (int)align_up((size_t)p->ny + 1, 32);
+    p->SL = p->shot ? 32 : 1;
+    p->CS = p->shot ? 32 : 1;
+    p->BW = p->shot ? p->W : 32 * p->W;
+    p->nb = (p->ny + p->BW - 1) / p->BW;
+    // PADC leading zero columns, then columns up to nb*BW + 3 (halo column and
+    // the 16-byte-aligned stage segments of the last band); rows of 16 bytes
+    p->P = (int)align_up((size_t)p->nb * p->BW + 2 * fg::PADC, 4);
     p->TY = (int)align_up((size_t)std::max(p->th, 1), 4);
-    p->Ph = (int)align_up((size_t)p->ny, 4);
-    p->bw = p->kernel == 0 ? p->NW * 32 * p->V : 32 * p->V;   // register march and tiles: one warp wide
-    p->nb = (p->ny + p->bw - 1) / p->bw;
+    p->Ph = (int)align_up((size_t)p->ny, 8);
     p->nc = std::max(1, (p->nx + p->TI - 1) / p->TI);
-    p->ngroups = (p->S + p->G - 1) / p->G;
+    p->ngroups = (p->S + p->SL - 1) / p->SL;
     p->ntiles = p->ngroups * p->nc * p->nb;
     p->chunk_row.resize(p->nc + 1);
-    for (int c = 0; c <= p->nc; ++c) p->chunk_row[c] = (int)((long long)c * p->nx / p->nc);
+    // tiles: chunks of exactly TI rows (the last one shorter); march: balanced chunks
+    for (int c = 0; c <= p->nc; ++c)
+        p->chunk_row[c] = p->kernel == 0 ? std::min(c * p->TI, p->nx) : (int)((long long)c * p->nx / p->nc);
+    // fetch order: tiles touching a CPML slab (more work per cell) first,
+    // each class in (group, chunk, band) order
+    {
+        const int th = p->th;
+        auto heavy = [&](int t) {
+            if (th == 0) return false;
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc;
+            const int i0 = p->chunk_row[chunk], i1 = p->chunk_row[chunk + 1];
+            const int b0 = band * p->BW, b1 = b0 + p->BW;
+            const bool xs = i0 <= th || i1 - 1 >= p->nx - th - 1;
+            const bool ys = b0 <= th + 1 || b1 - 1 >= p->ny - th - 1;
+            return xs || ys;
+        };
+        p->order.clear();
+        for (int t = 0; t < p->ntiles; ++t)
+            if (heavy(t)) p->order.push_back(t);
+        for (int t = 0; t < p->ntiles; ++t)
+            if (!heavy(t)) p->order.push_back(t);
+        p->tiles.resize(p->ntiles);
+        for (int q = 0; q < p->ntiles; ++q) {
+            const int t = p->order[q];
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc, grp = t / (p->nb * p->nc);
+            p->tiles[q] = make_int4(band * p->BW, p->chunk_row[chunk], grp, t);
+        }
+    }
 
-    const int bw = p->bw;
+    const int bw = p->BW;
     auto tile_events = [&](std::vector<Ev>& out, std::vector<int>& off, auto&& gen) {
         out.clear();
         off.assign(p->ntiles + 1, 0);
+        std::vector<Ev> evs;
         for (int t = 0; t < p->ntiles; ++t) {
             const int band = t % p->nb, rest = t / p->nb, chunk = rest % p->nc, grp = rest / p->nc;
-            std::vector<Ev> evs;
+            evs.clear();
             gen(evs, grp, p->chunk_row[chunk], p->chunk_row[chunk + 1], band * bw, band * bw + bw);
             std::stable_sort(evs.begin(), evs.end(), [](const Ev& a, const Ev& b) {
                 if (a.x != b.x) return a.x < b.x;
@@ -107,15 +148,23 @@ void build_tiles(fg_plan* p) {
     std::vector<char> live(p->nsrc, 0);
     for (int n = 0; n < p->nsrc; ++n)
         for (int t = 0; t < p->nt; ++t)
-            if (p->srcw[(size_t)n * p->nt + t] != 0.f) { live[n] = 1; break; }
-
+            if (p->srcw[(size_t)n * p->nt + t] != 0.f) {
+                live[n] = 1;
+                break;
+            }
     auto pos = [&](const std::vector<int32_t>& tab, int count, int s, int n, int c) {
         return tab[((size_t)s * count + n) * 3 + c];
     };
-    tile_events(p->src_ev, p->src_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for (int q = 0; q < p->G; ++q) {
-            const int s = grp * p->G + q;
+    // the shots of a group: slot q is shot grp*SL + q
+    auto for_group = [&](int grp, auto&& fn) {
+        for (int q = 0; q < p->SL; ++q) {
+            const int s = grp * p->SL + q;
             if (s >= p->S) break;
+            fn(s, q);
+        }
+    };
+    tile_events(p->src_ev, p->src_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
+        for_group(grp, [&](int s, int q) {
             for (int n = 0; n < p->nsrc; ++n) {
                 if (!live[n]) continue;
                 const int i = pos(p->src, p->nsrc, s, n, 0), j = pos(p->src, p->nsrc, s, n, 1),
@@ -123,45 +172,29 @@ void build_tiles(fg_plan* p) {
                 if (classify(p, i, j, k) != 1) continue;
                 if (i >= i0 && i < i1 && j >= b0 && j < be) evs.push_back(make_int4(i, q, j, n));
             }
-        }
+        });
     });
     tile_events(p->rx_ev, p->rx_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for (int q = 0; q < p->G; ++q) {
-            const int s = grp * p->G + q;
-            if (s >= p->S) break;
+        for_group(grp, [&](int s, int q) {
             for (int r = 0; r < p->nrx; ++r) {
                 const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1),
                           k = pos(p->rx, p->nrx, s, r, 2);
                 if (classify(p, i, j, k) != 1) continue;
                 if (i >= i0 && i < i1 && j >= b0 && j < be) evs.push_back(make_int4(i, q, j, r));
             }
-        }
+        });
     });
-    // adjoint injections: rows [i0, i1] (row i1 is recomputed as a halo row)
+    // adjoint injections: rows [i0, i1] and columns [b0, be] (row i1 and
+    // column be are recomputed as halo cells)
     tile_events(p->inj_ev, p->inj_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for (int q = 0; q < p->G; ++q) {
-            const int s = grp * p->G + q;
-            if (s >= p->S) break;
+        for_group(grp, [&](int s, int q) {
             for (int r = 0; r < p->nrx; ++r) {
                 const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1),
                           k = pos(p->rx, p->nrx, s, r, 2);
                 if (classify(p, i, j, k) != 1) continue;
-                if (i >= i0 && i <= i1 && j >= b0 && j < be) evs.push_back(make_int4(i, q, j, r));
+                if (i >= i0 && i <= i1 && j >= b0 && j <= be) evs.push_back(make_int4(i, q, j, r));
             }
-        }
-    });
-    // adjoint injections on the halo column be, rows [i0, i1)
-    tile_events(p->injh_ev, p->injh_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int, int be) {
-        for (int q = 0; q < p->G; ++q) {
-            const int s = grp * p->G + q;
-            if (s >= p->S) break;
-            for (int r = 0; r < p->nrx; ++r) {
-                const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1),
-                          k = pos(p->rx, p->nrx, s, r, 2);
-                if (classify(p, i, j, k) != 1) continue;
-                if (i >= i0 && i < i1 && j == be) evs.push_back(make_int4(i, q, j, r));
-            }
-        }
+        });
     });
 }
 
@@ -173,20 +206,23 @@ void layout(fg_plan* p) {
         o = align_up(o + std::max<size_t>(bytes, 1), A);
         return at;
     };
-    p->plane = (long long)(p->nx + 1) * p->P;
-    p->pxs = 2LL * p->th * p->P;
-    p->pys = 2LL * (p->nx + 1) * p->TY;
-    p->o_coef = take(5 * (size_t)p->plane * sizeof(float));
-    p->state_bytes = 6 * (size_t)p->S * p->plane * sizeof(float);
-    p->psi_bytes = 4 * (size_t)p->S * (p->pxs + p->pys) * sizeof(float);
+    const long long cplane = (long long)(p->nx + 1) * p->P;
+    p->plane = cplane * p->CS;
+    p->pxs = 2LL * p->th * p->P * p->CS;
+    p->pys = 2LL * (p->nx + 1) * p->TY * p->CS;
+    p->o_coef = take(5 * (size_t)cplane * sizeof(float));
+    p->state_bytes = 6 * (size_t)p->ngroups * p->plane * sizeof(float);
+    p->psi_bytes = 4 * (size_t)p->ngroups * (p->pxs + p->pys) * sizeof(float);
     p->o_state = take(p->state_bytes);
     p->o_psi = take(p->psi_bytes);
     p->o_chunk = take((p->nc + 1) * sizeof(int));
+    p->o_order = take((size_t)p->ntiles * sizeof(int));
+    p->o_tiles = take((size_t)p->ntiles * sizeof(int4));
+    p->o_ctr = take(2 * sizeof(int));
     p->o_srcev = take(p->src_ev.size() * sizeof(Ev));
     p->o_rxev = take(p->rx_ev.size() * sizeof(Ev));
     p->o_injev = take(p->inj_ev.size() * sizeof(Ev));
-    p->o_injhev = take(p->injh_ev.size() * sizeof(Ev));
-    p->o_offs = take(4 * (size_t)(p->ntiles + 1) * sizeof(int));
+    p->o_offs = take(3 * (size_t)(p->ntiles + 1) * sizeof(int));
     p->o_srcw = take((size_t)p->nsrc * p->nt * sizeof(float));
     p->o_pml = take(8 * (size_t)p->th * sizeof(float));
     const size_t n = (size_t)p->nx * p->ny;
@@ -199,35 +235,38 @@ void layout(fg_plan* p) {
 }
 
 void fill_grid(fg_plan* p) {
-    GridDev& g = p->g;
+    Dev& g = p->g;
     std::memset(&g, 0, sizeof(g));
     char* w = p->ws;
     g.nx = p->nx; g.ny = p->ny; g.P = p->P; g.th = p->th; g.TY = p->TY;
-    g.S = p->S; g.nt = p->nt; g.nrx = p->nrx; g.Ph = p->Ph;
+    g.S = p->S; g.nt = p->nt; g.nrx = p->nrx; g.Ph = p->Ph; g.ngroups = p->ngroups;
     g.d = p->dx; g.dt = p->dt;
     g.plane = p->plane; g.pxs = p->pxs; g.pys = p->pys;
+    const long long cplane = (long long)(p->nx + 1) * p->P;
     float* coef = (float*)(w + p->o_coef);
-    g.ca = coef; g.cb = coef + p->plane; g.cd = coef + 2 * p->plane; g.ch = coef + 3 * p->plane;
-    g.ci = coef + 4 * p->plane;
+    g.ca = coef; g.cb = coef + cplane; g.cd = coef + 2 * cplane; g.ch = coef + 3 * cplane;
+    g.ci = coef + 4 * cplane;
     g.pml = (const float*)(w + p->o_pml);
     float* st = (float*)(w + p->o_state);
-    const long long sp = (long long)p->S * p->plane;
+    const long long sp = (long long)p->ngroups * p->plane;
     g.ez[0] = st; g.ez[1] = st + sp; g.hx[0] = st + 2 * sp; g.hx[1] = st + 3 * sp;
     g.hy[0] = st + 4 * sp; g.hy[1] = st + 5 * sp;
     float* ps = (float*)(w + p->o_psi);
-    const long long xs = (long long)p->S * p->pxs, ys = (long long)p->S * p->pys;
+    const long long xs = (long long)p->ngroups * p->pxs, ys = (long long)p->ngroups * p->pys;
     g.pex[0] = ps; g.pex[1] = ps + xs; g.phx[0] = ps + 2 * xs; g.phx[1] = ps + 3 * xs;
     float* py = ps + 4 * xs;
     g.pey[0] = py; g.pey[1] = py + ys; g.phy[0] = py + 2 * ys; g.phy[1] = py + 3 * ys;
-    g.nb = p->nb; g.nc = p->nc; g.G = p->G; g.ngroups = p->ngroups; g.ntiles = p->ntiles;
+    g.nb = p->nb; g.nc = p->nc; g.ntiles = p->ntiles;
     g.chunk_row = (const int*)(w + p->o_chunk);
+    g.order = (const int*)(w + p->o_order);
+    g.tiles = (const int4*)(w + p->o_tiles);
+    g.tile_ctr = (int*)(w + p->o_ctr);
+    g.fast_cpml = 2 * p->th < p->nx && 2 * p->th < p->ny;
     g.src_ev = (const Ev*)(w + p->o_srcev);
     g.rx_ev = (const Ev*)(w + p->o_rxev);
     g.inj_ev = (const Ev*)(w + p->o_injev);
-    g.injh_ev = (const Ev*)(w + p->o_injhev);
     const int* offs = (const int*)(w + p->o_offs);
     g.src_off = offs; g.rx_off = offs + (p->ntiles + 1); g.inj_off = offs + 2 * (p->ntiles + 1);
-    g.injh_off = offs + 3 * (p->ntiles + 1);
     g.srcw = (const float*)(w + p->o_srcw);
     g.gacc = (double*)(w + p->o_gacc);
     g.ws_lo = w;
@@ -235,198 +274,269 @@ void fill_grid(fg_plan* p) {
     g.err = (int*)(w + p->o_err);
 }
 
-template <int V, int G>
-void launch_forward(const GridDev& g, int t, cudaStream_t st) {
-    const int blocks = (g.ntiles + 3) / 4;
-    fg::k_forward_step<V, G><<<blocks, 128, 0, st>>>(g, t);
-}
-template <int V, int G>
-void launch_adjoint(const GridDev& g, int it, int rp, cudaStream_t st) {
-    const int blocks = (g.ntiles + 3) / 4;
-    fg::k_adjoint_step<V, G><<<blocks, 128, 0, st>>>(g, it, rp);
+using FwdFn = cudaError_t (*)(const Dev&, int, int, int, int*, cudaStream_t);
+using AdjFn = cudaError_t (*)(const Dev&, int, int, int, int, int*, cudaStream_t);
+
+template <int W, bool SHOT>
+size_t ring_smem(int wpb, int D, bool adjoint) {
+    using RG = fg::RingGeom<W, SHOT>;
+    return fg::ring_bar_bytes(wpb, D) + (size_t)wpb * D * (adjoint ? RG::ADJ : RG::FWD) * sizeof(float);
 }
 
-template <int V, int G>
-cudaError_t launch_forward_tma(const GridDev& g, int t, int nw, int D, cudaStream_t st) {
-    const size_t smem = fg::ring_smem_bytes(D, 5 + 6 * G, fg::ring_slot_width(nw * 32 * V, g.TY), g.th);
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(fg::k_forward_tma<V, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    });
-    if (attr != cudaSuccess) return attr;
-    fg::k_forward_tma<V, G><<<g.ntiles, (nw + 1) * 32, smem, st>>>(g, t, D);
-    return cudaSuccess;
+template <class K>
+cudaError_t allow_smem(K kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
-template <int V, int G>
-cudaError_t launch_adjoint_tma(const GridDev& g, int it, int rp, int nw, int D, cudaStream_t st) {
-    const size_t smem = fg::ring_smem_bytes(D, 5 + 8 * G, fg::ring_slot_width(nw * 32 * V, g.TY), g.th);
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(fg::k_adjoint_tma<V, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    });
-    if (attr != cudaSuccess) return attr;
-    fg::k_adjoint_tma<V, G><<<g.ntiles, (nw + 1) * 32, smem, st>>>(g, it, rp, D);
-    return cudaSuccess;
-}
-template <int V>
-cudaError_t launch_forward_tile(const GridDev& g, int t, int TH, int G, cudaStream_t st) {
-    fg::k_forward_tile<V><<<g.ntiles, 32 * TH, fg::tile_fwd_smem(TH, V), st>>>(g, t, G);
-    return cudaSuccess;
-}
-template <int V>
-cudaError_t launch_adjoint_tile(const GridDev& g, int it, int rp, int TH, int G, cudaStream_t st) {
-    fg::k_adjoint_tile<V><<<g.ntiles, 32 * TH, fg::tile_adj_smem(TH, V), st>>>(g, it, rp, G);
-    return cudaSuccess;
-}
-template <int V>
-cudaError_t launch_forward_march(const GridDev& g, int t, int TI, int G, cudaStream_t st) {
-    (void)TI;
-    const int blocks = (g.ntiles + fg::MARCH_WARPS - 1) / fg::MARCH_WARPS;
-    fg::k_forward_march<V><<<blocks, 32 * fg::MARCH_WARPS, 0, st>>>(g, t, G);
-    return cudaSuccess;
-}
-template <int V>
-cudaError_t launch_adjoint_march(const GridDev& g, int it, int rp, int TI, int G, cudaStream_t st) {
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(fg::k_adjoint_march<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    });
-    if (attr != cudaSuccess) return attr;
-    const int blocks = (g.ntiles + fg::MARCH_WARPS - 1) / fg::MARCH_WARPS;
-    fg::k_adjoint_march<V><<<blocks, 32 * fg::MARCH_WARPS, fg::march_adj_smem(TI, V), st>>>(g, it, rp, G, TI);
+
+// Blocks of a persistent launch: as many as are resident on the device at
+// once, at most one warp per tile.
+template <class K>
+cudaError_t persistent_blocks(K kernel, int wpb, size_t smem, int ntiles, int* blocks) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * wpb, smem);
+    if (e != cudaSuccess) return e;
+    const int need = (ntiles + wpb - 1) / wpb;
+    *blocks = std::max(1, std::min(need, std::max(per_sm, 1) * sms));
     return cudaSuccess;
 }
 
-using FwdTileFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
-using AdjTileFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
-FwdTileFn pick_fwd_march(int V) {
-    switch (V) {
-        case 1: return launch_forward_march<1>;
-        case 2: return launch_forward_march<2>;
-        case 4: return launch_forward_march<4>;
+template <int W, bool SHOT, bool RING>
+cudaError_t launch_fwd_k(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
+    const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, false) : 0);
+    auto kernel = fg::k_fwd<W, SHOT, RING>;
+    if (*blocks == 0) {
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
+        if (e != cudaSuccess) return e;
     }
-    return nullptr;
+    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, t, D);
+    return cudaSuccess;
 }
-AdjTileFn pick_adj_march(int V);
-FwdTileFn pick_fwd_tile(int V) {
-    switch (V) {
-        case 1: return launch_forward_tile<1>;
-        case 2: return launch_forward_tile<2>;
-        case 4: return launch_forward_tile<4>;
+template <int W, bool SHOT, bool RING>
+cudaError_t launch_adj_k(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
+    const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, true) : 0);
+    auto kernel = fg::k_adj<W, SHOT, RING>;
+    if (*blocks == 0) {
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
+        if (e != cudaSuccess) return e;
     }
-    return nullptr;
+    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, it, rp, D);
+    return cudaSuccess;
 }
-AdjTileFn pick_adj_march(int V) {
-    switch (V) {
-        case 1: return launch_adjoint_march<1>;
-        case 2: return launch_adjoint_march<2>;
-        case 4: return launch_adjoint_march<4>;
-    }
-    return nullptr;
+template <int W, bool SHOT>
+cudaError_t launch_fwd(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
+    return D == 0 ? launch_fwd_k<W, SHOT, false>(g, t, wpb, D, blocks, st)
+                  : launch_fwd_k<W, SHOT, true>(g, t, wpb, D, blocks, st);
 }
-AdjTileFn pick_adj_tile(int V) {
-    switch (V) {
-        case 1: return launch_adjoint_tile<1>;
-        case 2: return launch_adjoint_tile<2>;
-        case 4: return launch_adjoint_tile<4>;
-    }
-    return nullptr;
-}
-
-using FwdTmaFn = cudaError_t (*)(const GridDev&, int, int, int, cudaStream_t);
-using AdjTmaFn = cudaError_t (*)(const GridDev&, int, int, int, int, cudaStream_t);
-template <int V>
-FwdTmaFn pick_fwd_tma_g(int G) {
-    switch (G) {
-        case 1: return launch_forward_tma<V, 1>;
-        case 2: return launch_forward_tma<V, 2>;
-        case 4: return launch_forward_tma<V, 4>;
-    }
-    return nullptr;
-}
-FwdTmaFn pick_fwd_tma(int V, int G) {
-    switch (V) {
-        case 1: return pick_fwd_tma_g<1>(G);
-        case 2: return pick_fwd_tma_g<2>(G);
-        case 4: return pick_fwd_tma_g<4>(G);
-    }
-    return nullptr;
-}
-template <int V>
-AdjTmaFn pick_adj_tma_g(int G) {
-    switch (G) {
-        case 1: return launch_adjoint_tma<V, 1>;
-        case 2: return launch_adjoint_tma<V, 2>;
-        case 4: return launch_adjoint_tma<V, 4>;
-    }
-    return nullptr;
-}
-AdjTmaFn pick_adj_tma(int V, int G) {
-    switch (V) {
-        case 1: return pick_adj_tma_g<1>(G);
-        case 2: return pick_adj_tma_g<2>(G);
-        case 4: return pick_adj_tma_g<4>(G);
-    }
-    return nullptr;
+template <int W, bool SHOT>
+cudaError_t launch_adj(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
+    return D == 0 ? launch_adj_k<W, SHOT, false>(g, it, rp, wpb, D, blocks, st)
+                  : launch_adj_k<W, SHOT, true>(g, it, rp, wpb, D, blocks, st);
 }
 
-using FwdFn = void (*)(const GridDev&, int, cudaStream_t);
-using AdjFn = void (*)(const GridDev&, int, int, cudaStream_t);
+template <bool SHOT>
+FwdFn pick_fwd_w(int W) {
+    switch (W) {
+        case 2: return launch_fwd<2, SHOT>;
+        case 4: return launch_fwd<4, SHOT>;
+        case 8: return launch_fwd<8, SHOT>;
+    }
+    return nullptr;
+}
+FwdFn pick_fwd(bool shot, int W) { return shot ? pick_fwd_w<true>(W) : pick_fwd_w<false>(W); }
+template <bool SHOT>
+AdjFn pick_adj_w(int W) {
+    switch (W) {
+        case 2: return launch_adj<2, SHOT>;
+        case 4: return launch_adj<4, SHOT>;
+        case 8: return launch_adj<8, SHOT>;
+    }
+    return nullptr;
+}
+AdjFn pick_adj(bool shot, int W) { return shot ? pick_adj_w<true>(W) : pick_adj_w<false>(W); }
 
-template <int V>
-FwdFn pick_fwd_g(int G) {
-    switch (G) {
-        case 1: return launch_forward<V, 1>;
-        case 2: return launch_forward<V, 2>;
-        case 4: return launch_forward<V, 4>;
-        case 8: return launch_forward<V, 8>;
+// Shared memory of the larger (adjoint) ring, or 0 for direct loads.
+size_t plan_ring_smem(const fg_plan* p) {
+    if (p->D == 0) return 0;
+    switch ((p->shot ? 10 : 0) + p->W) {
+        case 12: return ring_smem<2, true>(p->WPB, p->D, true);
+        case 14: return ring_smem<4, true>(p->WPB, p->D, true);
+        case 18: return ring_smem<8, true>(p->WPB, p->D, true);
+        case 2: return ring_smem<2, false>(p->WPB, p->D, true);
+        case 4: return ring_smem<4, false>(p->WPB, p->D, true);
+        case 8: return ring_smem<8, false>(p->WPB, p->D, true);
     }
-    return nullptr;
-}
-FwdFn pick_fwd(int V, int G) {
-    switch (V) {
-        case 1: return pick_fwd_g<1>(G);
-        case 2: return pick_fwd_g<2>(G);
-        case 4: return pick_fwd_g<4>(G);
-    }
-    return nullptr;
-}
-template <int V>
-AdjFn pick_adj_g(int G) {
-    switch (G) {
-        case 1: return launch_adjoint<V, 1>;
-        case 2: return launch_adjoint<V, 2>;
-        case 4: return launch_adjoint<V, 4>;
-        case 8: return launch_adjoint<V, 8>;
-    }
-    return nullptr;
-}
-AdjFn pick_adj(int V, int G) {
-    switch (V) {
-        case 1: return pick_adj_g<1>(G);
-        case 2: return pick_adj_g<2>(G);
-        case 4: return pick_adj_g<4>(G);
-    }
-    return nullptr;
+    return 0;
 }
 
 int coefficients(const float* er, const float* se, const float* mr, int nx, int ny, float dt, float dx, int adjoint,
-                 float* out, int P, cudaStream_t st) {
+                 float* out, int P, int col0, cudaStream_t st) {
     const long long n = (long long)(nx + 1) * P;
     const int threads = 256;
     const long long blocks = (n + threads - 1) / threads;
-    fg::k_coefficients<<<(unsigned)blocks, threads, 0, st>>>(er, se, mr, nx, ny, dt, dx, adjoint, out, P);
+    fg::k_coefficients<<<(unsigned)blocks, threads, 0, st>>>(er, se, mr, nx, ny, dt, dx, adjoint, out, P, col0);
     FG_CUDA(cudaGetLastError());
     return FG_OK;
 }
 
+// Zero fields, auxiliaries and the two tile counters before a solve.
 int reset_state(fg_plan* p, cudaStream_t st) {
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_state, 0, p->state_bytes, st));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_psi, 0, p->psi_bytes, st));
+    FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 2 * sizeof(int), st));
     return FG_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    });
+    return fn;
+}
+
+// A float32 tensor map over `base`: dims[0] fastest, strides in bytes of
+// dims 1.., box in elements; out-of-range elements of a box read as zero.
+int encode_map(CUtensorMap* m, const void* base, int rank, const uint64_t* dims, const uint64_t* strides,
+               const uint32_t* box) {
+    auto fn = tensor_map_encoder();
+    if (!fn) return fail(FG_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    cuuint64_t d[5], st[4];
+    cuuint32_t b[5], es[5];
+    for (int k = 0; k < rank; ++k) {
+        d[k] = dims[k];
+        b[k] = box[k];
+        es[k] = 1;
+        if (k + 1 < rank) st[k] = strides[k];
+    }
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, const_cast<void*>(base), d, st, b, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(FG_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return FG_OK;
+}
+
+// State box of `cells` columns and `rows` rows over all six field buffers
+// (Ez, Hx, Hy x parity), one group.
+int encode_state_map(const fg_plan* p, CUtensorMap* m, int cells, int rows) {
+    const void* base = p->ws + p->o_state;
+    const uint64_t f4 = sizeof(float);
+    if (p->shot) {
+        const uint64_t dims[5] = {32, (uint64_t)p->P, (uint64_t)p->nx + 1, (uint64_t)p->ngroups, 6};
+        const uint64_t st[4] = {32 * f4, (uint64_t)p->P * 32 * f4, (uint64_t)p->plane * f4,
+                                (uint64_t)p->ngroups * p->plane * f4};
+        const uint32_t box[5] = {32, (uint32_t)cells, (uint32_t)rows, 1, 1};
+        return encode_map(m, base, 5, dims, st, box);
+    }
+    const uint64_t dims[4] = {(uint64_t)p->P, (uint64_t)p->nx + 1, (uint64_t)p->ngroups, 6};
+    const uint64_t st[3] = {(uint64_t)p->P * f4, (uint64_t)p->plane * f4, (uint64_t)p->ngroups * p->plane * f4};
+    const uint32_t box[4] = {(uint32_t)cells, (uint32_t)rows, 1, 1};
+    return encode_map(m, base, 4, dims, st, box);
+}
+
+int encode_tile_maps(fg_plan* p) {
+    const int R = p->TI, W = p->W;
+    const int BW = p->BW, NW = BW + 8;
+    const bool sh = p->shot;
+    int rc = FG_OK;
+    if ((rc = encode_state_map(p, &p->tm_fez, sh ? W + 2 : NW, R + 2))) return rc;
+    if ((rc = encode_state_map(p, &p->tm_fhx, sh ? W + 1 : NW, R))) return rc;
+    if ((rc = encode_state_map(p, &p->tm_fhy, sh ? W : NW, R + 1))) return rc;
+    if ((rc = encode_state_map(p, &p->tm_aez, sh ? W + 1 : NW, R + 1))) return rc;
+    if ((rc = encode_state_map(p, &p->tm_ahx, sh ? W + 2 : NW, R + 1))) return rc;
+    if ((rc = encode_state_map(p, &p->tm_ahy, sh ? W + 1 : NW, R + 2))) return rc;
+    const uint64_t f4 = sizeof(float);
+    const uint64_t dims[3] = {(uint64_t)p->P, (uint64_t)p->nx + 1, 5};
+    const uint64_t st[2] = {(uint64_t)p->P * f4, (uint64_t)(p->nx + 1) * p->P * f4};
+    const uint32_t box[3] = {(uint32_t)(BW + 8), (uint32_t)R + 1, 5};
+    return encode_map(&p->tm_co, p->ws + p->o_coef, 3, dims, st, box);
+}
+
+// Box over the Ez history: W (shot lanes, all 32 slots) or BW (column lanes)
+// columns of R rows of one (step, group).
+int encode_hist_map(const fg_plan* p, CUtensorMap* m, const float* hist) {
+    const uint64_t f4 = sizeof(float);
+    const uint64_t steps = (uint64_t)p->nt * p->ngroups;
+    if (p->shot) {
+        const uint64_t dims[4] = {32, (uint64_t)p->Ph, (uint64_t)p->nx, steps};
+        const uint64_t st[3] = {32 * f4, (uint64_t)p->Ph * 32 * f4, (uint64_t)p->nx * p->Ph * 32 * f4};
+        const uint32_t box[4] = {32, (uint32_t)p->W, (uint32_t)p->TI, 1};
+        return encode_map(m, hist, 4, dims, st, box);
+    }
+    const uint64_t dims[3] = {(uint64_t)p->Ph, (uint64_t)p->nx, steps};
+    const uint64_t st[2] = {(uint64_t)p->Ph * f4, (uint64_t)p->nx * p->Ph * f4};
+    const uint32_t box[3] = {(uint32_t)p->BW, (uint32_t)p->TI, 1};
+    return encode_map(m, hist, 3, dims, st, box);
+}
+
+// Persistent pipeline launches: TI consumer warps + 1 producer warp per CTA,
+// as many CTAs as are resident on the device (at most one per tile).
+template <class K>
+cudaError_t pipe_blocks(K kernel, int threads, size_t smem, int ntiles, int* blocks) {
+    if (*blocks) return cudaSuccess;
+    cudaError_t e = allow_smem(kernel, smem);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (e != cudaSuccess) return e;
+    *blocks = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
+    return cudaSuccess;
+}
+template <int W, bool SHOT>
+cudaError_t launch_fwd_tile(fg_plan* p, const Dev& g, int t, cudaStream_t st) {
+    const fg::TileSmem<W, SHOT> L(p->TI, false);
+    const fg::PipeSmem M(p->th, p->D, L.total);
+    auto kernel = fg::k_fwd_pipe<W, SHOT>;
+    const int threads = 32 * (p->TI + 1);
+    const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->fwd_blocks);
+    if (e != cudaSuccess) return e;
+    kernel<<<p->fwd_blocks, threads, M.total, st>>>(g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t, p->D);
+    return cudaSuccess;
+}
+template <int W, bool SHOT>
+cudaError_t launch_adj_tile(fg_plan* p, const Dev& g, const CUtensorMap& tmh, int it, int rp, cudaStream_t st) {
+    const fg::TileSmem<W, SHOT> L(p->TI, true);
+    const fg::PipeSmem M(p->th, p->D, L.total);
+    auto kernel = fg::k_adj_pipe<W, SHOT>;
+    const int threads = 32 * (p->TI + 1);
+    const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->adj_blocks);
+    if (e != cudaSuccess) return e;
+    kernel<<<p->adj_blocks, threads, M.total, st>>>(g, p->tm_aez, p->tm_ahx, p->tm_ahy, p->tm_co, tmh, it, rp,
+                                                     p->D);
+    return cudaSuccess;
+}
+using FwdTileFn = cudaError_t (*)(fg_plan*, const Dev&, int, cudaStream_t);
+using AdjTileFn = cudaError_t (*)(fg_plan*, const Dev&, const CUtensorMap&, int, int, cudaStream_t);
+FwdTileFn pick_fwd_tile(bool shot, int W) {
+    if (shot) return W == 4 ? launch_fwd_tile<4, true> : W == 8 ? launch_fwd_tile<8, true> : nullptr;
+    return W == 2 ? launch_fwd_tile<2, false> : W == 4 ? launch_fwd_tile<4, false> : nullptr;
+}
+AdjTileFn pick_adj_tile(bool shot, int W) {
+    if (shot) return W == 4 ? launch_adj_tile<4, true> : W == 8 ? launch_adj_tile<8, true> : nullptr;
+    return W == 2 ? launch_adj_tile<2, false> : W == 4 ? launch_adj_tile<4, false> : nullptr;
+}
+// Shared memory of the larger (adjoint) pipeline CTA.
+size_t plan_tile_smem(const fg_plan* p) {
+    size_t stage = 0;
+    switch ((p->shot ? 10 : 0) + p->W) {
+        case 14: stage = fg::TileSmem<4, true>(p->TI, true).total; break;
+        case 18: stage = fg::TileSmem<8, true>(p->TI, true).total; break;
+        case 2: stage = fg::TileSmem<2, false>(p->TI, true).total; break;
+        case 4: stage = fg::TileSmem<4, false>(p->TI, true).total; break;
+    }
+    return fg::PipeSmem(p->th, p->D, stage).total;
 }
 
 // Device scratch of fg_forward_static: one array per GPU that loads the
@@ -500,44 +610,56 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             delete p;
             return fail(FG_ERR_INVALID, "receiver position outside the grid");
         }
-    p->kernel = tune ? tune->kernel : 3;
-    p->V = tune && tune->cols_per_thread ? tune->cols_per_thread : (p->kernel >= 2 ? 2 : 1);
-    p->G = tune && tune->shots_per_tile ? tune->shots_per_tile
-                                        : (p->kernel >= 2 ? std::min(q.shots, 4) : (q.shots >= 2 ? 2 : 1));
-    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : (p->kernel == 2 ? 8 : 16);
-    p->NW = tune && tune->warps_per_tile ? tune->warps_per_tile : 0;
-    p->D = tune && tune->stages ? tune->stages : 4;
-    if (p->kernel == 0 && p->NW == 0) {
-        // default: one band covering the row when it fits in 16 warps
-        p->NW = std::min(16, std::max(1, (q.ny + 32 * p->V - 1) / (32 * p->V)));
-    }
-    const bool ok_common = (p->V == 1 || p->V == 2 || p->V == 4) && p->TI >= 2;
-    const bool ok_k0 = p->kernel == 0 && (p->G == 1 || p->G == 2 || p->G == 4) && p->NW >= 1 && p->NW <= 16 &&
-                       p->D >= 3 && p->D <= 8;
-    const bool ok_k1 = p->kernel == 1 && (p->G == 1 || p->G == 2 || p->G == 4 || p->G == 8);
-    const bool ok_k2 = p->kernel == 2 && p->G >= 1 && p->G <= 64 && p->TI <= 16;
-    const bool ok_k3 = p->kernel == 3 && p->G >= 1 && p->G <= 64 &&
-                       fg::march_adj_smem(p->TI, p->V) <= 227 * 1024;
-    if (!ok_common || !(ok_k0 || ok_k1 || ok_k2 || ok_k3)) {
+    const int lanes = tune ? tune->lanes : 0;
+    if (lanes < 0 || lanes > 2) {
         delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning");
+        return fail(FG_ERR_INVALID, "unsupported tuning: lanes must be 0, 1 or 2");
     }
-    // The row-streaming tiles keep one x-slab auxiliary row per stage; with
-    // 2*th >= nx a row lies in both x-slabs and the register march is used.
-    if (p->kernel == 0 && 2 * q.th >= q.nx) {
-        p->kernel = 1;
-        if (p->G > 8) p->G = 8;
+    p->shot = lanes == 1 || (lanes == 0 && q.shots >= 8);
+    // defaults: the fastest measured shapes on the 440 x 340 benchmark grid --
+    // lane march (4 cells x 4 rows) for shot lanes, tile pipeline (2 cells x 4
+    // rows) for column lanes
+    const bool tuned_kernel = tune && (tune->kernel || tune->stages || tune->rows_per_tile || tune->cells_per_thread);
+    p->kernel = tuned_kernel ? tune->kernel : (p->shot ? 1 : 0);
+    if (p->kernel < 0 || p->kernel > 1) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: kernel must be 0 (tiles) or 1 (lane march)");
     }
+    p->W = tune && tune->cells_per_thread ? tune->cells_per_thread : (p->shot ? 4 : 2);
+    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 4;
     if (p->kernel == 0) {
-        const int TY = (int)align_up((size_t)std::max(q.th, 1), 4);
-        const size_t smem = fg::ring_smem_bytes(p->D, 5 + 8 * p->G, fg::ring_slot_width(p->NW * 32 * p->V, TY), q.th);
-        if (smem > 227 * 1024) {
+        const bool okw = p->shot ? (p->W == 4 || p->W == 8) : (p->W == 2 || p->W == 4);
+        const int st = tune ? tune->stages : 0;
+        if (!okw || !(p->TI == 2 || p->TI == 4 || p->TI == 8) || st < 0 || st == 1 || st > fg::MAX_STAGES) {
             delete p;
-            return fail(FG_ERR_INVALID, "tuning needs more than 227 KB of shared memory");
+            return fail(FG_ERR_INVALID, "unsupported tuning: tiles take cells_per_thread 4/8 (shot lanes) or 2/4 "
+                                        "(column lanes), rows_per_tile 2/4/8 and stages 0 or 2..4");
         }
+    }
+    p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : 4;
+    p->D = tune ? tune->stages : 0;
+    if (p->kernel == 0 && p->D == 0) p->D = 3;   // pipeline stages of the tile kernels
+    if (!(p->W == 2 || p->W == 4 || p->W == 8) || p->TI < 1 || !(p->WPB == 1 || p->WPB == 2 || p->WPB == 4) ||
+        p->D < 0 || p->D == 1 || p->D > 8) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: cells_per_thread 2/4/8, rows_per_tile >= 1, "
+                                    "warps_per_block 1/2/4, stages 0 or 2..8");
+    }
+    // shot-lane stages copy coefficient rows from column j0-4: 16-byte aligned only for W >= 4
+    if (p->D > 0 && p->shot && p->W < 4) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: shot lanes with stages need cells_per_thread 4 or 8");
+    }
+    if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: the ring needs more than 227 KB of shared memory");
     }
     build_tiles(p);
     layout(p);
+    if (p->kernel == 0 && plan_tile_smem(p) > 227 * 1024) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: a tile needs more than 227 KB of shared memory");
+    }
     *out = p;
     return FG_OK;
 }
@@ -549,7 +671,15 @@ int fg_plan_destroy(fg_plan* plan) {
 
 int64_t fg_plan_workspace_bytes(const fg_plan* plan) { return plan ? (int64_t)plan->total : -1; }
 
-int32_t fg_plan_hist_pitch(const fg_plan* plan) { return plan ? plan->Ph : -1; }
+int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
+    if (!p || !shape) return fail(FG_ERR_INVALID, "fg_plan_hist_shape: NULL argument");
+    shape[0] = p->nt;
+    shape[1] = p->ngroups;
+    shape[2] = p->nx;
+    shape[3] = p->Ph;
+    shape[4] = p->CS;
+    return FG_OK;
+}
 
 int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     if (!p) return fail(FG_ERR_INVALID, "fg_plan_bind: NULL plan");
@@ -564,19 +694,23 @@ int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
         return cudaMemcpyAsync(p->ws + off, src, n, cudaMemcpyHostToDevice, st);
     };
     FG_CUDA(up(p->o_chunk, p->chunk_row.data(), p->chunk_row.size() * sizeof(int)));
+    FG_CUDA(up(p->o_order, p->order.data(), p->order.size() * sizeof(int)));
+    FG_CUDA(up(p->o_tiles, p->tiles.data(), p->tiles.size() * sizeof(int4)));
     FG_CUDA(up(p->o_srcev, p->src_ev.data(), p->src_ev.size() * sizeof(Ev)));
     FG_CUDA(up(p->o_rxev, p->rx_ev.data(), p->rx_ev.size() * sizeof(Ev)));
     FG_CUDA(up(p->o_injev, p->inj_ev.data(), p->inj_ev.size() * sizeof(Ev)));
-    FG_CUDA(up(p->o_injhev, p->injh_ev.data(), p->injh_ev.size() * sizeof(Ev)));
     std::vector<int> offs;
     offs.insert(offs.end(), p->src_off.begin(), p->src_off.end());
     offs.insert(offs.end(), p->rx_off.begin(), p->rx_off.end());
     offs.insert(offs.end(), p->inj_off.begin(), p->inj_off.end());
-    offs.insert(offs.end(), p->injh_off.begin(), p->injh_off.end());
     FG_CUDA(up(p->o_offs, offs.data(), offs.size() * sizeof(int)));
     FG_CUDA(up(p->o_srcw, p->srcw.data(), p->srcw.size() * sizeof(float)));
     FG_CUDA(up(p->o_pml, p->pml.data(), p->pml.size() * sizeof(float)));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_err, 0, sizeof(int) * 4, st));
+    if (p->kernel == 0) {
+        const int rc = encode_tile_maps(p);
+        if (rc) return rc;
+    }
     // the host tables must stay valid until the copies have been consumed
     FG_CUDA(cudaStreamSynchronize(st));
     return FG_OK;
@@ -586,41 +720,32 @@ int fg_coefficients(const float* er, const float* se, const float* mr, int32_t n
                     int32_t adjoint, float* out, int32_t pitch, void* stream) {
     if (!er || !se || !mr || !out) return fail(FG_ERR_INVALID, "fg_coefficients: NULL argument");
     if (nx < 1 || ny < 1 || pitch < ny + 1) return fail(FG_ERR_INVALID, "fg_coefficients: bad shape");
-    return coefficients(er, se, mr, nx, ny, dt, dx, adjoint, out, pitch, (cudaStream_t)stream);
+    return coefficients(er, se, mr, nx, ny, dt, dx, adjoint, out, pitch, 0, (cudaStream_t)stream);
 }
 
 int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, float* traces, float* hist,
                void* stream) {
     if (!p || !er || !se || !mr || (!traces && p->nrx > 0)) return fail(FG_ERR_INVALID, "fg_forward: NULL argument");
     if (!p->ws) return fail(FG_ERR_WORKSPACE, "fg_forward: plan has no workspace");
+    FwdFn fn = pick_fwd(p->shot, p->W);
+    FwdTileFn tfn = pick_fwd_tile(p->shot, p->W);
+    if ((p->kernel == 1 && !fn) || (p->kernel == 0 && !tfn)) return fail(FG_ERR_INVALID, "no kernel for this tuning");
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P, st);
+    int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st);
     if (rc) return rc;
     if ((rc = reset_state(p, st))) return rc;
     if (p->nrx > 0) FG_CUDA(cudaMemsetAsync(traces, 0, (size_t)p->S * p->nt * p->nrx * sizeof(float), st));
-    GridDev g = p->g;
+    Dev g = p->g;
     g.traces = traces;
     g.hist = hist;
     if (hist) {
         g.out_lo = (const char*)hist;
-        g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
+        g.out_hi = (const char*)(hist + (size_t)p->nt * p->ngroups * p->nx * p->Ph * p->CS);
     }
-    if (p->kernel == 3) {
-        FwdTileFn fn = pick_fwd_march(p->V);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->TI, p->G, st));
-    } else if (p->kernel == 2) {
-        FwdTileFn fn = pick_fwd_tile(p->V);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->TI, p->G, st));
-    } else if (p->kernel == 0) {
-        FwdTmaFn fn = pick_fwd_tma(p->V, p->G);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->NW, p->D, st));
+    if (p->kernel == 0) {
+        for (int t = 0; t < p->nt; ++t) FG_CUDA(tfn(p, g, t, st));
     } else {
-        FwdFn fn = pick_fwd(p->V, p->G);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int t = 0; t < p->nt; ++t) fn(g, t, st);
+        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
     }
     FG_CUDA(cudaGetLastError());
     return FG_OK;
@@ -632,33 +757,38 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     if (!p || !er || !se || !mr || !hist || (!resid && p->nrx > 0))
         return fail(FG_ERR_INVALID, "fg_adjoint_reference: NULL argument");
     if (!p->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_reference: plan has no workspace");
+    AdjFn fn = pick_adj(p->shot, p->W);
+    AdjTileFn tfn = pick_adj_tile(p->shot, p->W);
+    if ((p->kernel == 1 && !fn) || (p->kernel == 0 && !tfn)) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+    CUtensorMap tmh;
+    if (p->kernel == 0) {
+        const int rc = encode_hist_map(p, &tmh, hist);
+        if (rc) return rc;
+    }
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 1, (float*)(p->ws + p->o_coef), p->P, st);
+    int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 1, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st);
     if (rc) return rc;
     if ((rc = reset_state(p, st))) return rc;
     const size_t n = (size_t)p->nx * p->ny;
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_gacc, 0, (size_t)p->ngroups * 2 * n * sizeof(double), st));
-    GridDev g = p->g;
+    Dev g = p->g;
     g.hist = const_cast<float*>(hist);
     g.out_lo = (const char*)hist;
-    g.out_hi = (const char*)(hist + (size_t)p->nt * p->S * p->nx * p->Ph);
+    g.out_hi = (const char*)(hist + (size_t)p->nt * p->ngroups * p->nx * p->Ph * p->CS);
     g.resid = resid;
-    if (p->kernel == 3) {
-        AdjTileFn fn = pick_adj_march(p->V);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->TI, p->G, st));
-    } else if (p->kernel == 2) {
-        AdjTileFn fn = pick_adj_tile(p->V);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->TI, p->G, st));
-    } else if (p->kernel == 0) {
-        AdjTmaFn fn = pick_adj_tma(p->V, p->G);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->NW, p->D, st));
+    if (p->kernel == 0) {
+        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(tfn(p, g, tmh, it, (p->nt - 1 - it) & 1, st));
     } else {
-        AdjFn fn = pick_adj(p->V, p->G);
-        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-        for (int it = p->nt - 1; it >= 1; --it) fn(g, it, (p->nt - 1 - it) & 1, st);
+        for (int it = p->nt - 1; it >= 1; --it)
+            FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->WPB, p->D, &p->adj_blocks, st));
+    }
+    if (p->nt >= 2) {
+        // the adjoint Ez after the last step (it = 1) is in the buffer that launch wrote
+        const float* ez_final = g.ez[((p->nt - 2) & 1) ^ 1];
+        const long long cells = (long long)p->ngroups * p->nx * p->ny;
+        const int tb = (int)((cells + 255) / 256);
+        if (p->shot) fg::k_imaging_tail<32><<<tb, 256, 0, st>>>(g, ez_final);
+        else fg::k_imaging_tail<1><<<tb, 256, 0, st>>>(g, ez_final);
     }
     double* sums = (double*)(p->ws + p->o_sums);
     double* partial = (double*)(p->ws + p->o_partial);
@@ -687,7 +817,14 @@ int fg_forward_static(fg_plan* p, const float* er, const float* se, const float*
     if (rc == FG_OK) rc = fg_forward(p, er, se, mr, traces, hist, stream);
     p->ws = saved;
     p->ws_bytes = saved_bytes;
-    if (saved) fill_grid(p);
+    if (saved) {
+        fill_grid(p);
+        // the tile kernels' tensor maps address the workspace too
+        if (p->kernel == 0) {
+            const int mrc = encode_tile_maps(p);
+            if (rc == FG_OK) rc = mrc;
+        }
+    }
     return rc;
 }
 

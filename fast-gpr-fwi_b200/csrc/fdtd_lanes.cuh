@@ -1,0 +1,950 @@
+// Lane-march time-step kernels: one launch per time step, persistent warps
+// that fetch tiles from a counter, no synchronisation between warps.
+//
+// Tile = (shot group, row chunk [i0, i1), column band).  Each thread owns W
+// consecutive columns j0 .. j0+W-1 of one shot and marches down the rows of
+// the chunk, carrying the previous row's values in registers, so every cell's
+// Ez/Hx/Hy is read once and written once per step.  The one-cell halo a
+// thread needs from outside its columns (column j0-1 / j0+W, row i0-1 / i1)
+// is recomputed from the previous step's state, which lives in the other
+// buffer of a ping-pong pair, so tiles never wait on each other.
+//
+//   shot lanes   (SHOT = true):  lane l is shot slot l of the group (CS = 32);
+//                all lanes of a warp touch the same cells, so each access is
+//                one 128-byte line, coefficients are warp-uniform and every
+//                boundary branch is uniform across the warp.
+//   column lanes (SHOT = false): one shot per group (CS = 1); lane l owns
+//                columns b0 + l*W .. b0 + l*W + W-1.
+//
+// Scheduling: the grid holds as many warps as fit on the GPU; each warp takes
+// the next tile position from a per-launch counter (CPML-heavy tiles come
+// first in the order table), so the slow boundary tiles start early and the
+// light interior tiles fill in behind them.
+//
+// Operand delivery (RING):
+//   false  each row's operands are loaded from global memory into registers
+//          when the row is computed;
+//   true   lane 0 of each warp streams the warp's row segments -- contiguous
+//          runs of whole cells (all 32 shots of a cell are adjacent) -- into
+//          a D-stage shared-memory ring with cp.async.bulk, D rows ahead and
+//          across tile boundaries, completing on one mbarrier per stage.
+//          Bytes in flight then cost no registers.  Waits are bounded: a
+//          stage that does not complete within 2 s sets the device error
+//          word, the warp waits (bounded) for its copies in flight and
+//          leaves, and later launches of the solve return at once.
+//
+// Forward step t (src/compute.py:574-712), per row i: Hx (columns j0-1 ..
+// j0+W-1) and Hy from the old Ez, then Ez from the new H, the CPML
+// corrections of each, the source injection, the stores, the Ez history and
+// the receiver samples (trace[t+1] = Ez after step t, which is what the
+// reference's store_outputs reads at the start of step t+1).
+//
+// Reference-mode adjoint step (src/compute.py:1048-1172): residual injection
+// at the receivers, E (Ucgeta's uE0) from the old H, then H from the new E,
+// then the imaging sums with the stored forward Ez.  The march computes E one
+// row ahead of H; the imaging products of a warp's 32 shots are summed by a
+// reduce-scatter over the lanes and added to the group's fp64 accumulator.
+#pragma once
+
+#include "fdtd_common.cuh"
+
+namespace fg {
+
+__device__ __forceinline__ long long coef_at(const Dev& g, int i, int j) { return (long long)i * g.P + j + PADC; }
+
+// ---------------------------------------------------------------------------
+// mbarrier / bulk-copy primitives (no multicast anywhere)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bulk global -> shared copy completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ uint64_t globaltimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Arm `bar` for the copies `each` enumerates and issue them.  `each(f)` calls
+// f(dst, src, bytes) for every copy of the stage; the byte count is summed in
+// a first pass, so the barrier always expects exactly what is issued (the
+// checked build drops -- and records -- a copy whose source is out of range).
+template <class Each>
+__device__ __forceinline__ void issue_stage(const Dev& g, uint64_t* bar, Each&& each) {
+    uint32_t total = 0;
+    each([&](void*, const void* s, uint32_t b) {
+        if (b && FG_OK_PTR(g, s, (int)b)) total += b;
+    });
+    mbar_expect_tx(bar, total);
+    each([&](void* d, const void* s, uint32_t b) {
+        if (b && FG_OK_PTR(g, s, (int)b)) bulk_g2s(d, s, b, bar);
+    });
+}
+
+constexpr int ERR_WAIT_STAGE = 201;                          // device error word: a stage never completed
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // 2 s; a stage normally lands in microseconds
+
+// Bounded wait of one thread for phase `parity` of `bar`.
+__device__ __forceinline__ bool wait_stage(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) return false;
+        __nanosleep(20);
+    }
+    return true;
+}
+
+// Geometry of a warp's ring stage.
+template <int W, bool SHOT>
+struct RingGeom {
+    static constexpr int CS = SHOT ? 32 : 1;
+    static constexpr int BW = SHOT ? W : 32 * W;        // columns of a band
+    static constexpr int NS = SHOT ? W + 2 : BW + 8;    // cells of a state segment
+    static constexpr int NH = BW;                       // cells of a history segment
+    static constexpr int NCF = SHOT ? W + 8 : BW + 8;   // floats of a coefficient segment
+    static constexpr int FWD = 3 * NS * CS + 3 * NCF;   // floats of a forward stage
+    static constexpr int ADJ = 3 * NS * CS + NH * CS + 3 * NCF;   // floats of an adjoint stage
+};
+
+// Dynamic shared memory: the CPML profile, then (RING) the barriers and the
+// stages of every warp of the block.
+__host__ __device__ inline size_t prof_bytes(int th) { return ((size_t)8 * th * 4 + 127) / 128 * 128; }
+__host__ __device__ inline size_t ring_bar_bytes(int wpb, int D) { return (((size_t)wpb * D * 8) + 127) / 128 * 128; }
+
+// Copy the CPML profile (8 x th) into shared memory; every thread of the
+// block passes the barrier.
+__device__ __forceinline__ const float* stage_profile(const Dev& g, unsigned char* smem) {
+    float* R = reinterpret_cast<float*>(smem);
+    for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) R[k] = __ldg(g.pml + k);
+    __syncthreads();
+    return R;
+}
+
+// ---------------------------------------------------------------------------
+// Tiles
+// ---------------------------------------------------------------------------
+template <bool SHOT>
+struct LaneTile {
+    int id, grp, i0, i1, b0, j0, l, s;
+    bool live;
+};
+
+template <int W, bool SHOT>
+__device__ __forceinline__ LaneTile<SHOT> decode_tile(const Dev& g, int id, int lane) {
+    LaneTile<SHOT> T;
+    T.id = id;
+    const int band = id % g.nb;
+    const int rest = id / g.nb;
+    const int chunk = rest % g.nc;
+    T.grp = rest / g.nc;
+    T.i0 = __ldg(g.chunk_row + chunk);
+    T.i1 = __ldg(g.chunk_row + chunk + 1);
+    if (SHOT) {
+        T.l = lane;
+        T.b0 = band * W;
+        T.j0 = T.b0;
+        T.s = T.grp * 32 + lane;
+        T.live = true;   // padded slots (s >= S) exist in memory and stay zero
+    } else {
+        T.l = 0;
+        T.b0 = band * 32 * W;
+        T.j0 = T.b0 + lane * W;
+        T.s = T.grp;
+        T.live = T.j0 < g.ny;
+    }
+    return T;
+}
+
+// Next tile position of this warp (lane 0 takes it, all lanes see it).
+__device__ __forceinline__ int fetch_tile(int* ctr, int lane) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(ctr, 1);
+    return __shfl_sync(FULL, p, 0);
+}
+
+// A tile as the ring producer sees it: rows [i0, i1) and the element
+// offsets of its row-0 segments, decoded once when the tile is fetched.
+struct TileQ {
+    int i0 = 0, i1 = 0;   // i1 <= i0: no tile
+    long long sbase = 0;  // state segment of row 0 within the field buffers
+    long long cbase = 0;  // coefficient segment of row 0
+    long long hbase = 0;  // history segment of row 0 (adjoint)
+    uint32_t hs = 0;      // bytes of a history segment (adjoint)
+};
+
+template <int W, bool SHOT>
+__device__ __forceinline__ TileQ tile_q(const Dev& g, int pos, int it) {
+    TileQ q;
+    if (pos >= g.ntiles) return q;
+    constexpr int CS = SHOT ? 32 : 1;
+    const LaneTile<SHOT> T = decode_tile<W, SHOT>(g, __ldg(g.order + pos), 0);
+    q.i0 = T.i0;
+    q.i1 = T.i1;
+    const int c0s = SHOT ? T.b0 - 1 : T.b0 - 4;   // 16-byte aligned segment starts
+    q.sbase = (long long)T.grp * g.plane + (long long)(c0s + PADC) * CS;
+    q.cbase = T.b0 - 4 + PADC;
+    const long long hrow = (long long)g.Ph * CS;
+    q.hbase = ((long long)it * g.ngroups + T.grp) * g.nx * hrow + (long long)T.b0 * CS;
+    // history cells of the band that exist in a history row
+    const int hcells = SHOT ? W : max(0, min(32 * W, g.Ph - T.b0));
+    q.hs = (uint32_t)hcells * CS * 4;
+    return q;
+}
+
+// Producer of a warp's ring: streams the rows of the current and the next
+// tile.  Only lane 0 runs it.  Invariant: (ptile, prow) names the next row to
+// issue, ptile = 0 for the current tile and 1 for the next one.
+struct RingProducer {
+    int ptile = 0, prow = 0;
+    uint32_t qi = 0;   // stages issued
+    int slot = 0;      // qi % D
+    TileQ q[2];        // current and next tile
+};
+
+// ---------------------------------------------------------------------------
+// Forward step
+// ---------------------------------------------------------------------------
+template <int W>
+struct FwdIn {                 // operands of row i
+    float en[W + 2];           // Ez_old(i+1, j0-1 .. j0+W)
+    float hxo[W + 1];          // Hx_old(i, j0-1 .. j0+W-1)
+    float hyo[W];              // Hy_old(i, j0 .. j0+W-1)
+    float ca[W], cb[W];        // uE0, uE1 (i, j0 ..)
+    float ch[W + 1];           // uH1 (i, j0-1 ..)
+};
+
+// Row i of the forward step from its operands; carries ezc (Ez_old of row i,
+// columns j0-1 .. j0+W) and hyu (Hy_new of row i-1) to the next row.
+template <int W, int CS>
+__device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const FwdIn<W>& B, float (&ezc)[W + 2],
+                                        float (&hyu)[W], int i, int t, int j0, int l, int slot, int s, bool bcore,
+                                        float* ezW, float* hxW, float* hyW, float* hist, long long hrow,
+                                        const PsiG& rd, const PsiG& wr, int& sc, int se, int& rc, int re) {
+    const int nx = g.nx, ny = g.ny, th = g.th;
+    float hxn[W + 1], hyn[W], ezn[W];
+    if (bcore && i >= th + 1 && i <= nx - th - 1) {
+#pragma unroll
+        for (int k = 0; k <= W; ++k) hxn[k] = __fsub_rn(B.hxo[k], __fmul_rn(B.ch[k], __fsub_rn(ezc[k + 1], ezc[k])));
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            hyn[w] = __fadd_rn(B.hyo[w], __fmul_rn(B.ch[w + 1], __fsub_rn(B.en[w + 1], ezc[w + 1])));
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            ezn[w] = __fmaf_rn(-B.cb[w], __fsub_rn(hxn[w + 1], hxn[w]),
+                               madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
+    } else if (g.fast_cpml) {
+        float dzx[W + 1], dzy[W], dhy[W], dhx[W];
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            hxn[k] = B.hxo[k];
+            dzx[k] = __fsub_rn(ezc[k + 1], ezc[k]);
+        }
+        hx_cells<W + 1, CS>(g, R, i, j0 - 1, l, hxn, dzx, B.ch, 1, rd, wr);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            hyn[w] = B.hyo[w];
+            dzy[w] = __fsub_rn(B.en[w + 1], ezc[w + 1]);
+        }
+        hy_cells<W, CS, true>(g, R, i, j0, l, hyn, dzy, B.ch + 1, rd, wr);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            ezn[w] = ezc[w + 1];
+            dhy[w] = __fsub_rn(hyn[w], hyu[w]);
+            dhx[w] = __fsub_rn(hxn[w + 1], hxn[w]);
+        }
+        e_cells<W, CS>(g, R, i, j0, l, ezn, dhy, dhx, B.ca, B.cb, W, true, rd, wr);
+    } else {
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            const int j = j0 - 1 + k;
+            hxn[k] = B.hxo[k];
+            if (j >= 0 && j < ny) {
+                const float dz = __fsub_rn(ezc[k + 1], ezc[k]);
+                if (k == 0) hxn[k] = hx_cell<CS, false>(g, R, i, j, l, B.hxo[k], dz, B.ch[k], rd, rd);
+                else hxn[k] = hx_cell<CS, true>(g, R, i, j, l, B.hxo[k], dz, B.ch[k], rd, wr);
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const int j = j0 + w;
+            hyn[w] = B.hyo[w];
+            if (j < ny)
+                hyn[w] = hy_cell<CS, true>(g, R, i, j, l, B.hyo[w], __fsub_rn(B.en[w + 1], ezc[w + 1]), B.ch[w + 1],
+                                           rd, wr);
+        }
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const int j = j0 + w;
+            ezn[w] = ezc[w + 1];
+            if (j < ny)
+                ezn[w] = e_cell<CS, true>(g, R, i, j, l, ezc[w + 1], __fsub_rn(hyn[w], hyu[w]),
+                                          __fsub_rn(hxn[w + 1], hxn[w]), B.ca[w], B.cb[w], rd, wr);
+        }
+    }
+    // Hertzian dipole (sourcereceiver.cu:84), in list order
+    for (; sc < se; ++sc) {
+        const Ev e = __ldg(g.src_ev + sc);
+        if (e.x != i) break;
+        if (e.y != slot) continue;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (j0 + w == e.z) {
+                const float cd = ldro(g, g.cd + coef_at(g, i, e.z));
+                ezn[w] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezn[w]);
+            }
+    }
+    const long long o = ((long long)i * g.P + j0 + PADC) * CS + l;
+    st_cells<W, CS>(g, ezW + o, ezn);
+    st_cells<W, CS>(g, hxW + o, hxn + 1);
+    st_cells<W, CS>(g, hyW + o, hyn);
+    if (hist && j0 < g.Ph) st_cells<W, CS, true>(g, hist + (long long)i * hrow, ezn);
+    for (; rc < re; ++rc) {
+        const Ev e = __ldg(g.rx_ev + rc);
+        if (e.x != i) break;
+        if (e.y != slot || t + 1 >= g.nt) continue;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (j0 + w == e.z) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezn[w];
+    }
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) ezc[k] = B.en[k];
+#pragma unroll
+    for (int w = 0; w < W; ++w) hyu[w] = hyn[w];
+}
+
+// Stage of forward row i of tile Q: Ez_old of row i+1, Hx_old and Hy_old of
+// row i, and the uE0 / uE1 / uH1 coefficient rows.
+template <int W, bool SHOT>
+__device__ __forceinline__ void issue_fwd(const Dev& g, uint64_t* bar, float* st, const TileQ& Q, int i, int rp) {
+    using RG = RingGeom<W, SHOT>;
+    constexpr int CS = RG::CS;
+    constexpr uint32_t zs = (uint32_t)(SHOT ? (W + 2) : RG::NS) * CS * 4;
+    constexpr uint32_t xs = (uint32_t)(SHOT ? (W + 1) : RG::NS) * CS * 4;
+    constexpr uint32_t ys = (uint32_t)(SHOT ? W : RG::NS) * CS * 4;
+    constexpr uint32_t cs = (uint32_t)RG::NCF * 4;
+    constexpr int yo = SHOT ? CS : 0;   // Hy starts one cell later in shot-lane stages
+    const long long rowS = (long long)g.P * CS;
+    const long long so = Q.sbase + (long long)i * rowS;
+    const long long co = Q.cbase + (long long)i * g.P;
+    float* cst = st + 3 * RG::NS * CS;
+    issue_stage(g, bar, [&](auto&& f) {
+        f(st, g.ez[rp] + so + rowS, zs);
+        f(st + RG::NS * CS, g.hx[rp] + so, xs);
+        f(st + 2 * RG::NS * CS + yo, g.hy[rp] + so + yo, ys);
+        f(cst, g.ca + co, cs);
+        f(cst + RG::NCF, g.cb + co, cs);
+        f(cst + 2 * RG::NCF, g.ch + co, cs);
+    });
+}
+
+template <int W, bool SHOT, bool RING>
+__global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int D) {
+    constexpr int CS = SHOT ? 32 : 1;
+    using RG = RingGeom<W, SHOT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* R = stage_profile(g, smem);
+    // a stage of an earlier launch never landed: leave at once
+    if (RING && *(volatile int*)g.err != 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[(t + 1) & 1] = 0;   // the next launch's counter
+    int* ctr = g.tile_ctr + (t & 1);
+    const int lane = threadIdx.x & 31;
+    const int P = g.P, ny = g.ny, th = g.th, nt_ = g.ntiles;
+    const int rp = t & 1, wp = rp ^ 1;
+    const long long hrow = (long long)g.Ph * CS;
+
+    uint64_t* bars = nullptr;
+    float* ring = nullptr;
+    if (RING) {
+        const int wib = threadIdx.x >> 5;
+        unsigned char* base = smem + prof_bytes(th);
+        bars = reinterpret_cast<uint64_t*>(base) + (size_t)wib * D;
+        ring = reinterpret_cast<float*>(base + ring_bar_bytes(blockDim.x >> 5, D)) + (size_t)wib * D * RG::FWD;
+        if (lane == 0) {
+            for (int d = 0; d < D; ++d) mbar_init(bars + d, 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+    }
+    int cur = fetch_tile(ctr, lane);
+    int nxt = cur < nt_ ? fetch_tile(ctr, lane) : nt_;
+    RingProducer pr;
+    uint32_t qc = 0;   // stages consumed
+    int cslot = 0;     // qc % D
+    uint32_t cpar = 0; // (qc / D) & 1
+    if (RING && lane == 0) {
+        pr.q[0] = tile_q<W, SHOT>(g, cur, 0);
+        pr.q[1] = tile_q<W, SHOT>(g, nxt, 0);
+    }
+    auto produce = [&]() {
+        while ((int)(pr.qi - qc) < D && pr.ptile <= 1) {
+            const TileQ& Q = pr.q[pr.ptile];
+            if (Q.i1 <= Q.i0) break;
+            issue_fwd<W, SHOT>(g, bars + pr.slot, ring + (size_t)pr.slot * RG::FWD, Q, Q.i0 + pr.prow, rp);
+            ++pr.qi;
+            if (++pr.slot == D) pr.slot = 0;
+            if (++pr.prow >= Q.i1 - Q.i0) {
+                ++pr.ptile;
+                pr.prow = 0;
+            }
+        }
+    };
+#define FG_CELL(i, j) (((long long)(i) * P + (j) + PADC) * CS + l)
+
+    while (cur < nt_) {
+        const LaneTile<SHOT> T = decode_tile<W, SHOT>(g, __ldg(g.order + cur), lane);
+        if (RING && lane == 0) produce();
+        const int l = T.l, j0 = T.j0, slot = SHOT ? l : 0;
+        const long long go = (long long)T.grp * g.plane;
+        const float* ezR = g.ez[rp] + go;
+        const float* hyR = g.hy[rp] + go;
+        const float* hxR = g.hx[rp] + go;
+        float* ezW = g.ez[wp] + go;
+        float* hxW = g.hx[wp] + go;
+        float* hyW = g.hy[wp] + go;
+        const PsiG rd = psi_group(g, rp, T.grp), wr = psi_group(g, wp, T.grp);
+        // H at columns j0-1 .. j0+W-1 and E at j0 .. j0+W-1 are all interior cells
+        const bool bcore = j0 >= th + 1 && j0 + W <= ny - th;
+        int sc = __ldg(g.src_off + T.id);
+        const int se = __ldg(g.src_off + T.id + 1);
+        int rc = __ldg(g.rx_off + T.id);
+        const int re = __ldg(g.rx_off + T.id + 1);
+        float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + T.grp) * g.nx) * hrow + (long long)j0 * CS + l
+                             : nullptr;
+        // Ez_old of row i0, columns j0-1 .. j0+W, and the new Hy of the row
+        // above the chunk (its auxiliaries are only read)
+        float ezc[W + 2], hyu[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) hyu[w] = 0.f;
+        if (T.live) {
+            ezc[0] = ldro(g, ezR + FG_CELL(T.i0, j0 - 1));
+            ld_cells<W, CS>(g, ezc + 1, ezR + FG_CELL(T.i0, j0));
+            ezc[W + 1] = ldro(g, ezR + FG_CELL(T.i0, j0 + W));
+            if (T.i0 >= 1) {
+                const int ih = T.i0 - 1;
+                float ea[W], ha[W], ca[W], dz[W];
+                ld_cells<W, CS>(g, ea, ezR + FG_CELL(ih, j0));
+                ld_cells<W, CS>(g, ha, hyR + FG_CELL(ih, j0));
+                ld_coef<W>(g, ca, g.ch + coef_at(g, ih, j0));
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    hyu[w] = ha[w];
+                    dz[w] = __fsub_rn(ezc[w + 1], ea[w]);
+                }
+                if (g.fast_cpml) {
+                    hy_cells<W, CS, false>(g, R, ih, j0, l, hyu, dz, ca, rd, rd);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < W; ++w)
+                        if (j0 + w < ny) hyu[w] = hy_cell<CS, false>(g, R, ih, j0 + w, l, ha[w], dz[w], ca[w], rd, rd);
+                }
+            }
+        }
+        const int nrow = T.i1 - T.i0;
+        for (int n = 0; n < nrow; ++n) {
+            const int i = T.i0 + n;
+            FwdIn<W> B;
+            if (RING) {
+                const bool ok = wait_stage(bars + cslot, cpar);
+                if (!__all_sync(FULL, ok)) {
+                    // a stage never landed: record it, wait (bounded) for this
+                    // warp's copies still in flight, and leave
+                    if (lane == 0) {
+                        atomicCAS(g.err, 0, ERR_WAIT_STAGE);
+                        for (uint32_t m = qc; m < pr.qi; ++m) wait_stage(bars + m % D, (m / D) & 1u);
+                    }
+                    __syncwarp();
+                    return;
+                }
+                const float* st = ring + (size_t)cslot * RG::FWD;
+                const float* cst = st + 3 * RG::NS * CS;
+                // this lane's first cell (column j0-1) within the stage segments
+                const int cz = SHOT ? l : (lane * W + 3);
+                const int cc = SHOT ? 3 : (lane * W + 3);
+#pragma unroll
+                for (int k = 0; k < W + 2; ++k) B.en[k] = st[cz + k * CS];
+#pragma unroll
+                for (int k = 0; k <= W; ++k) B.hxo[k] = st[RG::NS * CS + cz + k * CS];
+#pragma unroll
+                for (int w = 0; w < W; ++w) B.hyo[w] = st[2 * RG::NS * CS + cz + (w + 1) * CS];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    B.ca[w] = cst[cc + 1 + w];
+                    B.cb[w] = cst[RG::NCF + cc + 1 + w];
+                }
+#pragma unroll
+                for (int k = 0; k <= W; ++k) B.ch[k] = cst[2 * RG::NCF + cc + k];
+                __syncwarp();
+                ++qc;
+                if (++cslot == D) {
+                    cslot = 0;
+                    cpar ^= 1u;
+                }
+                if (lane == 0) {
+                    fence_proxy_async();
+                    produce();
+                }
+            } else if (T.live) {
+                const long long crow = coef_at(g, i, j0);
+                B.en[0] = ldro(g, ezR + FG_CELL(i + 1, j0 - 1));
+                ld_cells<W, CS>(g, B.en + 1, ezR + FG_CELL(i + 1, j0));
+                B.en[W + 1] = ldro(g, ezR + FG_CELL(i + 1, j0 + W));
+                B.hxo[0] = ldro(g, hxR + FG_CELL(i, j0 - 1));
+                ld_cells<W, CS>(g, B.hxo + 1, hxR + FG_CELL(i, j0));
+                ld_cells<W, CS>(g, B.hyo, hyR + FG_CELL(i, j0));
+                ld_coef<W>(g, B.ca, g.ca + crow);
+                ld_coef<W>(g, B.cb, g.cb + crow);
+                B.ch[0] = ldro(g, g.ch + crow - 1);
+                ld_coef<W>(g, B.ch + 1, g.ch + crow);
+            }
+            if (T.live)
+                fwd_row<W, CS>(g, R, B, ezc, hyu, i, t, j0, l, slot, T.s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr,
+                               sc, se, rc, re);
+        }
+        cur = nxt;
+        nxt = cur < nt_ ? fetch_tile(ctr, lane) : nt_;
+        if (RING && lane == 0) {
+            --pr.ptile;
+            pr.q[0] = pr.q[1];
+            pr.q[1] = tile_q<W, SHOT>(g, nxt, 0);
+        }
+    }
+#undef FG_CELL
+}
+
+// ---------------------------------------------------------------------------
+// Reference-mode adjoint step
+// ---------------------------------------------------------------------------
+template <int W>
+struct AdjEIn {                // operands of the E update of row r
+    float ez[W + 1];           // Ez_old(r, j0 .. j0+W)
+    float hxo[W + 2];          // Hx_old(r, j0-1 .. j0+W)
+    float hyo[W + 1];          // Hy_old(r, j0 .. j0+W)
+    float ca[W + 1], cb[W + 1];
+};
+
+template <int W, int CS>
+__device__ __forceinline__ void adj_e_load(const Dev& g, AdjEIn<W>& A, int r, int j0, int l, const float* ezR,
+                                           const float* hxR, const float* hyR) {
+    const long long rb = (long long)r * g.P + j0 + PADC;
+    ld_cells<W, CS>(g, A.ez, ezR + rb * CS + l);
+    A.ez[W] = ldro(g, ezR + (rb + W) * CS + l);
+    A.hxo[0] = ldro(g, hxR + (rb - 1) * CS + l);
+    ld_cells<W, CS>(g, A.hxo + 1, hxR + rb * CS + l);
+    A.hxo[W + 1] = ldro(g, hxR + (rb + W) * CS + l);
+    ld_cells<W, CS>(g, A.hyo, hyR + rb * CS + l);
+    A.hyo[W] = ldro(g, hyR + (rb + W) * CS + l);
+    ld_coef<W + 1>(g, A.ca, g.ca + rb);
+    ld_coef<W + 1>(g, A.cb, g.cb + rb);
+}
+
+// New E of row r, columns j0 .. j0+W (column j0+W is the halo), from the old
+// state: residuals injected first (list order), then the E update with the
+// old H (hyu = Hy_old of row r-1).  Auxiliaries are stored for the thread's
+// own cells when `own` (row r inside the chunk); the halo column and the halo
+// row below the chunk only read theirs.
+template <int W, int CS>
+__device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, AdjEIn<W>& A, int r, int j0, int l, int slot,
+                                          bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
+                                          const float* resid_s, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
+    // back_source (back.cu:34): Ez -= residual, no scaling
+    for (; ic < ie; ++ic) {
+        const Ev e = __ldg(g.inj_ev + ic);
+        if (e.x != r) break;
+        if (e.y != slot) continue;
+#pragma unroll
+        for (int k = 0; k <= W; ++k)
+            if (j0 + k == e.z) A.ez[k] = __fsub_rn(A.ez[k], __ldg(resid_s + e.w));
+    }
+    if (core) {
+#pragma unroll
+        for (int k = 0; k <= W; ++k)
+            out[k] = __fmaf_rn(-A.cb[k], __fsub_rn(A.hxo[k + 1], A.hxo[k]),
+                               madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
+    } else if (g.fast_cpml) {
+        float dhy[W + 1], dhx[W + 1];
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            out[k] = A.ez[k];
+            dhy[k] = __fsub_rn(A.hyo[k], hyu[k]);
+            dhx[k] = __fsub_rn(A.hxo[k + 1], A.hxo[k]);
+        }
+        e_cells<W + 1, CS>(g, R, r, j0, l, out, dhy, dhx, A.ca, A.cb, W, own, rd, wr);
+    } else {
+        const int ny = g.ny;
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            const int j = j0 + k;
+            out[k] = A.ez[k];
+            if (j < ny) {
+                const float dhy = __fsub_rn(A.hyo[k], hyu[k]);
+                const float dhx = __fsub_rn(A.hxo[k + 1], A.hxo[k]);
+                if (k < W && own)
+                    out[k] = e_cell<CS, true>(g, R, r, j, l, A.ez[k], dhy, dhx, A.ca[k], A.cb[k], rd, wr);
+                else out[k] = e_cell<CS, false>(g, R, r, j, l, A.ez[k], dhy, dhx, A.ca[k], A.cb[k], rd, rd);
+            }
+        }
+    }
+}
+
+// Sum v[0..M) over the 32 lanes of a warp by recursive halving.  Returns, in
+// every lane, the sum of element (lane >> s) & (M-1) with s = 5 - log2(M);
+// lanes whose low s bits are zero hold the M distinct sums.  Fixed
+// association order (deterministic).
+template <int M>
+__device__ __forceinline__ float lane_reduce_scatter(float (&v)[M], int lane) {
+    static_assert(M == 4 || M == 8 || M == 16, "2W elements");
+#pragma unroll
+    for (int len = M, m = 16; len > 1; len >>= 1, m >>= 1) {
+        const bool upper = (lane & m) != 0;
+#pragma unroll
+        for (int k = 0; k < len / 2; ++k) {
+            const float send = upper ? v[k] : v[k + len / 2];
+            const float keep = upper ? v[k + len / 2] : v[k];
+            v[k] = __fadd_rn(keep, __shfl_xor_sync(FULL, send, m));
+        }
+    }
+    constexpr int s = M == 4 ? 3 : (M == 8 ? 2 : 1);
+    float x = v[0];
+#pragma unroll
+    for (int m = (1 << s) >> 1; m >= 1; m >>= 1) x = __fadd_rn(x, __shfl_xor_sync(FULL, x, m));
+    return x;
+}
+
+// Stage of adjoint iteration i of tile Q: E operands of row r = i+1 (Ez_old,
+// Hx_old, Hy_old, uE0, uE1; none when r is the frame row), uH1 of row i and
+// the forward Ez of step it at row i.
+template <int W, bool SHOT>
+__device__ __forceinline__ void issue_adj(const Dev& g, uint64_t* bar, float* st, const TileQ& Q, int i, int rp) {
+    using RG = RingGeom<W, SHOT>;
+    constexpr int CS = RG::CS;
+    // shot-lane stages hold exactly the cells used: Ez, Hy from j0, Hx from j0-1
+    constexpr uint32_t zs = (uint32_t)(SHOT ? (W + 1) : RG::NS) * CS * 4;
+    constexpr uint32_t xs = (uint32_t)(SHOT ? (W + 2) : RG::NS) * CS * 4;
+    constexpr uint32_t cs = (uint32_t)RG::NCF * 4;
+    constexpr int zo = SHOT ? CS : 0;
+    const int r = i + 1;
+    const bool erow = r < g.nx;
+    const long long rowS = (long long)g.P * CS;
+    const long long so = Q.sbase + (long long)r * rowS;
+    const long long co = Q.cbase + (long long)r * g.P;
+    const float* h1 = g.hist + Q.hbase + (long long)i * g.Ph * CS;
+    float* hst = st + 3 * RG::NS * CS;
+    float* cst = hst + RG::NH * CS;
+    issue_stage(g, bar, [&](auto&& f) {
+        if (erow) {
+            f(st + zo, g.ez[rp] + so + zo, zs);
+            f(st + RG::NS * CS, g.hx[rp] + so, xs);
+            f(st + 2 * RG::NS * CS + zo, g.hy[rp] + so + zo, zs);
+            f(cst, g.ca + co, cs);
+            f(cst + RG::NCF, g.cb + co, cs);
+        }
+        f(cst + 2 * RG::NCF, g.ch + Q.cbase + (long long)i * g.P, cs);
+        f(hst, h1, Q.hs);
+    });
+}
+
+template <int W, bool SHOT, bool RING>
+__global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const int rp, const int D) {
+    constexpr int CS = SHOT ? 32 : 1;
+    using RG = RingGeom<W, SHOT>;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* R = stage_profile(g, smem);
+    if (RING && *(volatile int*)g.err != 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[rp ^ 1] = 0;   // the next launch's counter
+    int* ctr = g.tile_ctr + rp;
+    const int lane = threadIdx.x & 31;
+    const int P = g.P, nx = g.nx, ny = g.ny, th = g.th, nt_ = g.ntiles;
+    const int wp = rp ^ 1;
+    const long long hrow = (long long)g.Ph * CS;
+
+    uint64_t* bars = nullptr;
+    float* ring = nullptr;
+    if (RING) {
+        const int wib = threadIdx.x >> 5;
+        unsigned char* base = smem + prof_bytes(th);
+        bars = reinterpret_cast<uint64_t*>(base) + (size_t)wib * D;
+        ring = reinterpret_cast<float*>(base + ring_bar_bytes(blockDim.x >> 5, D)) + (size_t)wib * D * RG::ADJ;
+        if (lane == 0) {
+            for (int d = 0; d < D; ++d) mbar_init(bars + d, 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+    }
+    int cur = fetch_tile(ctr, lane);
+    int nxt = cur < nt_ ? fetch_tile(ctr, lane) : nt_;
+    RingProducer pr;
+    uint32_t qc = 0;
+    int cslot = 0;
+    uint32_t cpar = 0;
+    if (RING && lane == 0) {
+        pr.q[0] = tile_q<W, SHOT>(g, cur, it);
+        pr.q[1] = tile_q<W, SHOT>(g, nxt, it);
+    }
+    auto produce = [&]() {
+        while ((int)(pr.qi - qc) < D && pr.ptile <= 1) {
+            const TileQ& Q = pr.q[pr.ptile];
+            if (Q.i1 <= Q.i0) break;
+            issue_adj<W, SHOT>(g, bars + pr.slot, ring + (size_t)pr.slot * RG::ADJ, Q, Q.i0 + pr.prow, rp);
+            ++pr.qi;
+            if (++pr.slot == D) pr.slot = 0;
+            if (++pr.prow >= Q.i1 - Q.i0) {
+                ++pr.ptile;
+                pr.prow = 0;
+            }
+        }
+    };
+
+    while (cur < nt_) {
+        const LaneTile<SHOT> T = decode_tile<W, SHOT>(g, __ldg(g.order + cur), lane);
+        if (RING && lane == 0) produce();
+        const int l = T.l, j0 = T.j0, slot = SHOT ? l : 0;
+        // column lanes without cells only take part in the warp's stage protocol
+        const bool work = SHOT || T.live;
+        const long long go = (long long)T.grp * g.plane;
+        const float* ezR = g.ez[rp] + go;
+        const float* hxR = g.hx[rp] + go;
+        const float* hyR = g.hy[rp] + go;
+        float* ezW = g.ez[wp] + go;
+        float* hxW = g.hx[wp] + go;
+        float* hyW = g.hy[wp] + go;
+        const PsiG rd = psi_group(g, rp, T.grp), wr = psi_group(g, wp, T.grp);
+        // E at columns j0 .. j0+W (incl. the halo) and H at j0 .. j0+W-1 are interior cells
+        const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
+        int ic = __ldg(g.inj_off + T.id);
+        const int ie = __ldg(g.inj_off + T.id + 1);
+        const float* resid_s = g.resid + ((long long)T.s * g.nt + it) * g.nrx;
+        const float* f1g = g.hist + ((long long)it * g.ngroups + T.grp) * nx * hrow + (long long)j0 * CS + l;
+        double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
+        double* gas = gae + (long long)nx * ny;
+        const bool hist_ok = j0 < g.Ph;
+
+        // new E of row i0 (own), with the old H of rows i0-1 and i0; eoc keeps
+        // the old Ez of the row (before the residual injection)
+        float ezc[W + 1], hxc[W + 2], hyc[W + 1], eoc[W];
+        if (work) {
+            float hyu[W + 1];
+#pragma unroll
+            for (int k = 0; k <= W; ++k) hyu[k] = 0.f;
+            if (T.i0 >= 1) {
+                const long long rb = (long long)(T.i0 - 1) * P + j0 + PADC;
+                ld_cells<W, CS>(g, hyu, hyR + rb * CS + l);
+                hyu[W] = ldro(g, hyR + (rb + W) * CS + l);
+            }
+            AdjEIn<W> A;
+            adj_e_load<W, CS>(g, A, T.i0, j0, l, ezR, hxR, hyR);
+#pragma unroll
+            for (int w = 0; w < W; ++w) eoc[w] = A.ez[w];
+            adj_e_row<W, CS>(g, R, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
+                             ezc, resid_s, ic, ie, rd, wr);
+#pragma unroll
+            for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
+#pragma unroll
+            for (int k = 0; k <= W; ++k) hyc[k] = A.hyo[k];
+        }
+
+        const int nrow = T.i1 - T.i0;
+        for (int n = 0; n < nrow; ++n) {
+            const int i = T.i0 + n, r = i + 1;
+            AdjEIn<W> A;
+            float ch[W], f1[W];
+            if (RING) {
+                const bool ok = wait_stage(bars + cslot, cpar);
+                if (!__all_sync(FULL, ok)) {
+                    if (lane == 0) {
+                        atomicCAS(g.err, 0, ERR_WAIT_STAGE);
+                        for (uint32_t m = qc; m < pr.qi; ++m) wait_stage(bars + m % D, (m / D) & 1u);
+                    }
+                    __syncwarp();
+                    return;
+                }
+                const float* st = ring + (size_t)cslot * RG::ADJ;
+                const float* hst = st + 3 * RG::NS * CS;
+                const float* cst = hst + RG::NH * CS;
+                const int cz = SHOT ? l : (lane * W + 3);   // column j0-1
+                const int cc = SHOT ? 3 : (lane * W + 3);
+                if (r < nx) {
+#pragma unroll
+                    for (int k = 0; k <= W; ++k) {
+                        A.ez[k] = st[cz + (k + 1) * CS];
+                        A.hyo[k] = st[2 * RG::NS * CS + cz + (k + 1) * CS];
+                        A.ca[k] = cst[cc + 1 + k];
+                        A.cb[k] = cst[RG::NCF + cc + 1 + k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < W + 2; ++k) A.hxo[k] = st[RG::NS * CS + cz + k * CS];
+                }
+                const int hz = SHOT ? l : lane * W;   // column j0 within the history segment
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    ch[w] = cst[2 * RG::NCF + cc + 1 + w];
+                    f1[w] = hist_ok ? hst[hz + w * CS] : 0.f;
+                }
+                __syncwarp();
+                ++qc;
+                if (++cslot == D) {
+                    cslot = 0;
+                    cpar ^= 1u;
+                }
+                if (lane == 0) {
+                    fence_proxy_async();
+                    produce();
+                }
+                if (!work) continue;
+            } else {
+                if (!work) continue;
+                if (r < nx) adj_e_load<W, CS>(g, A, r, j0, l, ezR, hxR, hyR);
+                ld_coef<W>(g, ch, g.ch + coef_at(g, i, j0));
+                if (hist_ok) {
+                    ld_cells<W, CS>(g, f1, f1g + (long long)i * hrow);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < W; ++w) f1[w] = 0.f;
+                }
+            }
+            // new E of row r (own if inside the chunk, else the halo row below)
+            float ezr[W + 1], eor[W];
+            if (r < nx) {
+#pragma unroll
+                for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
+                adj_e_row<W, CS>(g, R, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < T.i1, hyc, ezr,
+                                 resid_s, ic, ie, rd, wr);
+            } else {
+#pragma unroll
+                for (int w = 0; w < W; ++w) eor[w] = 0.f;
+#pragma unroll
+                for (int k = 0; k <= W; ++k) ezr[k] = A.hyo[k] = 0.f;
+#pragma unroll
+                for (int k = 0; k < W + 2; ++k) A.hxo[k] = 0.f;
+            }
+            // H of row i from the new E
+            float hx[W], hy[W];
+            if (bcore && i >= th + 1 && i <= nx - th - 1) {
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    hx[w] = __fsub_rn(hxc[w + 1], __fmul_rn(ch[w], __fsub_rn(ezc[w + 1], ezc[w])));
+                    hy[w] = __fadd_rn(hyc[w], __fmul_rn(ch[w], __fsub_rn(ezr[w], ezc[w])));
+                }
+            } else if (g.fast_cpml) {
+                float dzx[W], dzy[W];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    hx[w] = hxc[w + 1];
+                    hy[w] = hyc[w];
+                    dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
+                    dzy[w] = __fsub_rn(ezr[w], ezc[w]);
+                }
+                hx_cells<W, CS>(g, R, i, j0, l, hx, dzx, ch, 0, rd, wr);
+                hy_cells<W, CS, true>(g, R, i, j0, l, hy, dzy, ch, rd, wr);
+            } else {
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    const int j = j0 + w;
+                    hx[w] = hxc[w + 1];
+                    hy[w] = hyc[w];
+                    if (j < ny) {
+                        hx[w] = hx_cell<CS, true>(g, R, i, j, l, hxc[w + 1], __fsub_rn(ezc[w + 1], ezc[w]), ch[w], rd,
+                                                  wr);
+                        hy[w] = hy_cell<CS, true>(g, R, i, j, l, hyc[w], __fsub_rn(ezr[w], ezc[w]), ch[w], rd, wr);
+                    }
+                }
+            }
+            // imaging (compute.py:1167-1172).  sum_t (Ez_f[t] - Ez_f[t-1]) lambda_t is
+            // summed by parts as sum_t Ez_f[t] (lambda_t - lambda_{t+1}) - Ez_f[0] lambda_1:
+            // lambda_{t+1} is this step's old Ez, so the history is read once
+            // per step; k_imaging_tail subtracts the last term.  The sigma sum is
+            // sum_t Ez_f[t] lambda_t dt.
+            float v[2 * W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                v[w] = __fmul_rn(f1[w], __fsub_rn(ezc[w], eoc[w]));
+                v[W + w] = __fmul_rn(__fmul_rn(f1[w], ezc[w]), g.dt);
+            }
+            const long long go2 = (long long)i * ny + j0;
+            if (SHOT) {
+                constexpr int s = (2 * W) == 4 ? 3 : ((2 * W) == 8 ? 2 : 1);
+                const float x = lane_reduce_scatter<2 * W>(v, lane);
+                if ((lane & ((1 << s) - 1)) == 0) {
+                    const int e = lane >> s;   // element index 0 .. 2W-1
+                    const int w = e < W ? e : e - W;
+                    if (j0 + w < ny) {
+                        double* a = (e < W ? gae : gas) + go2 + w;
+                        if (FG_OK_PTR(g, a, 8)) *a += (double)x;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int w = 0; w < W; ++w)
+                    if (j0 + w < ny) {
+                        if (FG_OK_PTR(g, gae + go2 + w, 8)) gae[go2 + w] += (double)v[w];
+                        if (FG_OK_PTR(g, gas + go2 + w, 8)) gas[go2 + w] += (double)v[W + w];
+                    }
+            }
+            const long long o = ((long long)i * P + j0 + PADC) * CS + l;
+            st_cells<W, CS>(g, ezW + o, ezc);
+            st_cells<W, CS>(g, hxW + o, hx);
+            st_cells<W, CS>(g, hyW + o, hy);
+#pragma unroll
+            for (int k = 0; k <= W; ++k) {
+                ezc[k] = ezr[k];
+                hyc[k] = A.hyo[k];
+            }
+#pragma unroll
+            for (int w = 0; w < W; ++w) eoc[w] = eor[w];
+#pragma unroll
+            for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
+        }
+        cur = nxt;
+        nxt = cur < nt_ ? fetch_tile(ctr, lane) : nt_;
+        if (RING && lane == 0) {
+            --pr.ptile;
+            pr.q[0] = pr.q[1];
+            pr.q[1] = tile_q<W, SHOT>(g, nxt, it);
+        }
+    }
+}
+
+// The last term of the summation by parts: g_eps -= sum_s Ez_f[0] lambda_1,
+// with lambda_1 the adjoint Ez after the last step (it = 1).  One thread per
+// (group, cell); the products are those of the per-step imaging (float32),
+// summed over the group's shots in slot order.
+template <int CS>
+__global__ void k_imaging_tail(const Dev g, const float* __restrict__ ez_final) {
+    const long long n = (long long)g.nx * g.ny;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)g.ngroups * n) return;
+    const int grp = (int)(idx / n);
+    const long long c = idx % n;
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const float* f0 = g.hist + (((long long)grp * g.nx + i) * g.Ph + j) * CS;
+    const float* lam = ez_final + (long long)grp * g.plane + ((long long)i * g.P + j + PADC) * CS;
+    float acc = 0.f;
+#pragma unroll 8
+    for (int l = 0; l < CS; ++l) acc = __fadd_rn(acc, __fmul_rn(__ldg(f0 + l), __ldg(lam + l)));
+    double* a = g.gacc + (long long)grp * 2 * n + c;
+    *a -= (double)acc;
+}
+
+}  // namespace fg

@@ -1,466 +1,637 @@
-// Tiled time-step kernels: one CTA per (shot group, row chunk, column band)
-// tile of TH rows x 32V columns, one warp per row.  Each CTA stages the old
-// state of its tile plus a one-cell halo in shared memory, computes the
-// first-half update (H in the forward, E in the adjoint) on the tile and the
-// halo cells its second half needs, synchronises, and finishes the step.
-// Everything a CTA reads comes from the previous step's buffers (ping-pong),
-// so CTAs never wait on each other within a step; latency is hidden by
-// running many small CTAs per SM.
+// Tensor-map tile pipelines: one launch per time step; persistent CTAs, each
+// with R consumer warps and one producer warp.
 //
-// The per-cell arithmetic is the device code of fdtd_device.cuh, so results
-// are bit-identical to the other kernels and to the reference.
+// Tile = (column band, row chunk [i0, i0+R), shot group).  The producer's lane
+// 0 fetches every operand of a tile -- the old Ez/Hx/Hy rows with a one-cell
+// halo, the coefficient rows, and in the adjoint the stored forward Ez rows --
+// with one cp.async.bulk.tensor copy per field (a box of 32 shots x cells x
+// rows, or cells x rows for one shot) into one of S shared-memory stages,
+// completing on the stage's "full" mbarrier; it runs up to S tiles ahead of
+// the consumers and reuses a stage once its "empty" mbarrier has one arrival
+// per consumer warp.  Rows and columns outside the field arrays are filled
+// with zeros by the copy engine, which is the reference's zero frame.  Each
+// consumer warp computes one row of the tile from the stage and writes the
+// new state (and new CPML auxiliaries) straight to global memory.  Everything
+// a CTA reads comes from the previous step's buffers (ping-pong), so CTAs
+// never wait on each other.  A CTA takes tiles blockIdx.x, blockIdx.x +
+// gridDim.x, ... of the tile table (CPML-heavy tiles first).  Every wait is
+// bounded (2 s): a stage that never lands sets the device error word, the
+// consumers agree to stop (one barrier with an AND reduction), wait (bounded)
+// for the stages that may still be landing, and leave; later launches of the
+// solve return at once.
+//
+//   shot lanes   (SHOT = true):  lane l is shot slot l of the group (CS = 32);
+//                all lanes of a warp touch the same cells, coefficients are
+//                warp-uniform and every boundary branch is uniform.
+//   column lanes (SHOT = false): one shot per group (CS = 1); lane l owns
+//                columns b0 + l*W .. b0 + l*W + W-1.
+//
+// Forward step t (src/compute.py:574-712), per row i: Hy of row i-1 (the halo
+// row, recomputed), Hx (columns j0-1 .. j0+W-1) and Hy of row i, then Ez, the
+// CPML corrections of each, the source injection, the stores, the Ez history
+// and the receiver samples (trace[t+1] = Ez after step t, which is what the
+// reference's store_outputs reads at the start of step t+1).
+//
+// Reference-mode adjoint step (src/compute.py:1048-1172): residual injection
+// at the receivers and the E update (Ucgeta's uE0) of rows i0 .. i0+R (the
+// last one is the halo row below) from the old H into shared memory, one CTA
+// barrier, then H of each row from the new E and the imaging sums with the
+// stored forward Ez; the products of a warp's 32 shots are summed by a
+// reduce-scatter over the lanes and added to the group's fp64 accumulator.
 #pragma once
 
-#include "fdtd_device.cuh"
+#include <cuda.h>
+
+#include "fdtd_common.cuh"
+#include "fdtd_lanes.cuh"
 
 namespace fg {
 
-struct TileT {
-    int band, chunk, grp, i0, i1, b0, be;
+// Box geometry of a tile, in cells (SHOT: per shot slot row of 32 floats).
+template <int W, bool SHOT>
+struct TileGeom {
+    static constexpr int CS = SHOT ? 32 : 1;
+    static constexpr int BW = SHOT ? W : 32 * W;   // columns of a band
+    // column windows (first column relative to j0 - 1 in shot lanes, b0 - 4 in column lanes)
+    static constexpr int NWIN = SHOT ? 0 : BW + 8;
+    // forward boxes: Ez rows i0-1 .. i0+R, cols j0-1 .. j0+W; Hx rows i0 .. i0+R-1, cols j0-1 ..
+    // j0+W-1; Hy rows i0-1 .. i0+R-1, cols j0 .. j0+W-1
+    static constexpr int FEZ = SHOT ? W + 2 : NWIN;
+    static constexpr int FHX = SHOT ? W + 1 : NWIN;
+    static constexpr int FHY = SHOT ? W : NWIN;
+    // adjoint boxes: Ez rows i0 .. i0+R, cols j0 .. j0+W; Hx rows i0 .. i0+R, cols j0-1 .. j0+W;
+    // Hy rows i0-1 .. i0+R, cols j0 .. j0+W; forward Ez rows i0 .. i0+R-1, cols j0 .. j0+W-1
+    static constexpr int AEZ = SHOT ? W + 1 : NWIN;
+    static constexpr int AHX = SHOT ? W + 2 : NWIN;
+    static constexpr int AHY = SHOT ? W + 1 : NWIN;
+    static constexpr int AH = BW;
+    static constexpr int NCF = BW + 8;   // coefficient columns b0-4 .. b0+BW+3
 };
 
-__device__ __forceinline__ TileT tile_t(const GridDev& g, int V) {
-    TileT t;
-    const int tile = blockIdx.x;
-    t.band = tile % g.nb;
-    const int rest = tile / g.nb;
-    t.chunk = rest % g.nc;
-    t.grp = rest / g.nc;
-    t.i0 = g.chunk_row[t.chunk];
-    t.i1 = g.chunk_row[t.chunk + 1];
-    t.b0 = t.band * 32 * V;
-    t.be = t.b0 + 32 * V;
-    return t;
+__host__ __device__ inline size_t align128(size_t x) { return (x + 127) / 128 * 128; }
+
+// Shared-memory layout of one stage (bytes), R rows; the CTA holds S stages.
+template <int W, bool SHOT>
+struct TileSmem {
+    using G = TileGeom<W, SHOT>;
+    size_t ez, hx, hy, co, hs, en, total;
+    __host__ __device__ TileSmem(int R, bool adjoint) {
+        const size_t cs = G::CS * sizeof(float);
+        size_t o = 0;
+        ez = o;
+        o = align128(o + (adjoint ? (size_t)G::AEZ * (R + 1) : (size_t)G::FEZ * (R + 2)) * cs);
+        hx = o;
+        o = align128(o + (adjoint ? (size_t)G::AHX * (R + 1) : (size_t)G::FHX * R) * cs);
+        hy = o;
+        o = align128(o + (adjoint ? (size_t)G::AHY * (R + 2) : (size_t)G::FHY * (R + 1)) * cs);
+        co = o;
+        o = align128(o + (size_t)G::NCF * (R + 1) * 5 * sizeof(float));
+        hs = o;
+        if (adjoint) o = align128(o + (size_t)G::AH * R * cs);
+        en = o;
+        if (adjoint) o = align128(o + (size_t)(SHOT ? W + 1 : G::NWIN) * (R + 1) * cs);
+        total = o;
+    }
+    // bytes the copies of one stage deliver
+    __host__ __device__ static uint32_t tx_bytes(int R, bool adjoint) {
+        const size_t cs = G::CS * sizeof(float);
+        size_t b = (size_t)G::NCF * (R + 1) * 5 * sizeof(float);
+        if (adjoint)
+            b += ((size_t)G::AEZ * (R + 1) + (size_t)G::AHX * (R + 1) + (size_t)G::AHY * (R + 2) + (size_t)G::AH * R) *
+                 cs;
+        else b += ((size_t)G::FEZ * (R + 2) + (size_t)G::FHX * R + (size_t)G::FHY * (R + 1)) * cs;
+        return (uint32_t)b;
+    }
+};
+
+// Whole-CTA layout: barriers and flags, CPML profile, S stages.
+constexpr int MAX_STAGES = 4;
+struct PipeSmem {
+    size_t full, empty, flag, prof, stages, stage_bytes, total;
+    __host__ __device__ PipeSmem(int th, int S, size_t stage) {
+        full = 0;
+        empty = 8 * MAX_STAGES;
+        flag = 16 * MAX_STAGES;
+        prof = 128;
+        stages = align128(prof + (size_t)8 * th * sizeof(float));
+        stage_bytes = stage;
+        total = stages + (size_t)S * stage;
+    }
+};
+
+// cp.async.bulk.tensor loads (tile mode, no multicast) of a box at the given
+// coordinates, completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
 }
 
-// Whether every cell a warp updates in row i is a plain interior cell: no
-// CPML slab, not on the i == 0 / j == 0 edges, all columns < ny.  Such warps
-// take the lean path (same arithmetic, no per-cell boundary tests).
-__device__ __forceinline__ bool core_warp(const GridDev& g, int i, int b0, int be) {
-    const int th = g.th;
-    return i >= th + 1 && i <= g.nx - th - 1 && b0 >= th + 1 && be <= g.ny - th;
+// A state box: field f (0 Ez, 1 Hx, 2 Hy) of parity par, first column `col`
+// (plane column, pad included) and first row `row` of group grp.
+template <bool SHOT>
+__device__ __forceinline__ void tma_state(void* dst, const CUtensorMap* tm, int col, int row, int grp, int f, int par,
+                                          uint64_t* bar) {
+    if (SHOT) tma_load_5d(dst, tm, 0, col, row, grp, 2 * f + par, bar);
+    else tma_load_4d(dst, tm, col, row, grp, 2 * f + par, bar);
 }
 
-template <int V>
-__device__ __forceinline__ void lds_v(float (&x)[V], const float* p) {
-    if constexpr (V == 4) {
-        const float4 q = *reinterpret_cast<const float4*>(p);
-        x[0] = q.x; x[1] = q.y; x[2] = q.z; x[3] = q.w;
-    } else if constexpr (V == 2) {
-        const float2 q = *reinterpret_cast<const float2*>(p);
-        x[0] = q.x; x[1] = q.y;
-    } else {
-        x[0] = *p;
+// Whether an earlier launch recorded a stage that never landed; read by
+// thread 0 and shared through shared memory, so the whole CTA takes the same
+// branch.
+__device__ __forceinline__ bool abort_launch(const Dev& g, volatile int* flag) {
+    if (threadIdx.x == 0) *flag = *(volatile int*)g.err;
+    __syncthreads();
+    return *flag != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Barrier 1 among the R consumer warps, returning the AND of `ok` over them.
+__device__ __forceinline__ bool consumers_and(bool ok, int nthreads) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)ok), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void consumers_sync(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Producer loop (lane 0 of warp R): for the CTA's k-th tile, wait until stage
+// k % S is free, arm its full barrier and issue the tile's copies.
+template <class Issue>
+__device__ __forceinline__ void produce_tiles(const Dev& g, uint64_t* full, uint64_t* empty, int S, Issue&& issue) {
+    int s = 0;
+    int k = 0;
+    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
+        // the u-th reuse of a stage (u = k / S >= 1) waits for completion u-1
+        // of its empty barrier
+        if (k >= S && !wait_stage(empty + s, (uint32_t)(k / S + 1) & 1u)) return;   // consumers stopped
+        issue(p, s, full + s);
+        if (++s == S) s = 0;
     }
 }
-template <int V>
-__device__ __forceinline__ void sts_v(float* p, const float (&x)[V]) {
-    if constexpr (V == 4) {
-        *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
-    } else if constexpr (V == 2) {
-        *reinterpret_cast<float2*>(p) = make_float2(x[0], x[1]);
-    } else {
-        *p = x[0];
+
+// Consumer side: wait for the k-th tile's stage; on a stage that never lands,
+// all consumers agree, wait (bounded) for the stages that may still be in
+// flight and report false.
+__device__ __forceinline__ bool consume_wait(const Dev& g, uint64_t* full, int s, uint32_t par, int k, int S,
+                                             int nthreads) {
+    const bool ok = wait_stage(full + s, par);
+    if (consumers_and(ok, nthreads)) return true;
+    if (threadIdx.x == 0) atomicCAS(g.err, 0, ERR_WAIT_STAGE);
+    // stages of tiles k .. k+S-1 may have been issued
+    int ss = s;
+    uint32_t pp = par;
+    for (int m = 0; m < S; ++m) {
+        if (blockIdx.x + (k + m) * gridDim.x >= g.ntiles) break;
+        wait_stage(full + ss, pp);
+        if (++ss == S) {
+            ss = 0;
+            pp ^= 1u;
+        }
     }
+    return false;
 }
 
 // ---------------------------------------------------------------------------
-// Forward step.  Shared memory (floats), own cells of a row at offset 4 so
-// that vector accesses are aligned:
-//   ez_s  [TH+2][SE]   Ez_old rows i0-1 .. i0+TH; col 3 = b0-1, 4.. = b0.., 4+32V = be
-//   hx_s  [TH  ][SE]   Hx_new rows i0 .. i0+TH-1; col 3 = b0-1, 4.. = b0..
-//   hy_s  [TH+1][SY]   Hy_new rows i0-1 .. i0+TH-1; col 0.. = b0..        (SY = 32V)
+// Forward step
 // ---------------------------------------------------------------------------
-__host__ __device__ inline size_t tile_fwd_smem(int TH, int V) {
-    return sizeof(float) * ((size_t)(2 * TH + 2) * (32 * V + 8) + (size_t)(TH + 1) * 32 * V);
+template <int W, bool SHOT>
+__device__ __forceinline__ void fwd_tile_issue(const Dev& g, const CUtensorMap* tm_ez, const CUtensorMap* tm_hx,
+                                               const CUtensorMap* tm_hy, const CUtensorMap* tm_co, unsigned char* st,
+                                               const TileSmem<W, SHOT>& L, int R, int4 T, int rp, uint64_t* bar) {
+    const int b0 = T.x, i0 = T.y, grp = T.z;
+    mbar_expect_tx(bar, TileSmem<W, SHOT>::tx_bytes(R, false));
+    const int cs = (SHOT ? b0 - 1 : b0 - 4) + PADC;   // first state column
+    tma_state<SHOT>(st + L.ez, tm_ez, cs, i0 - 1, grp, 0, rp, bar);
+    tma_state<SHOT>(st + L.hx, tm_hx, cs, i0, grp, 1, rp, bar);
+    tma_state<SHOT>(st + L.hy, tm_hy, SHOT ? cs + 1 : cs, i0 - 1, grp, 2, rp, bar);
+    tma_load_3d(st + L.co, tm_co, b0 - 4 + PADC, i0 - 1, 0, bar);
 }
 
-template <int V>
-__global__ void __launch_bounds__(512, 2) k_forward_tile(const GridDev g, const int t, const int G) {
-    extern __shared__ __align__(16) float sm[];
-    const int TH = blockDim.x >> 5;
-    const int lane = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const TileT T = tile_t(g, V);
-    const int SE = 32 * V + 8, SY = 32 * V;
-    float* ez_s = sm;
-    float* hx_s = ez_s + (TH + 2) * SE;
-    float* hy_s = hx_s + TH * SE;
-    const int ny = g.ny, P = g.P;
+// Row i0 + w of tile T from its stage.
+template <int W, bool SHOT>
+__device__ __forceinline__ void fwd_tile_row(const Dev& g, const float* Rp, const unsigned char* st,
+                                             const TileSmem<W, SHOT>& L, int R, int w, int4 T, int t) {
+    using G = TileGeom<W, SHOT>;
+    constexpr int CS = G::CS;
+    const float* sEZ = reinterpret_cast<const float*>(st + L.ez);
+    const float* sHX = reinterpret_cast<const float*>(st + L.hx);
+    const float* sHY = reinterpret_cast<const float*>(st + L.hy);
+    const float* sCO = reinterpret_cast<const float*>(st + L.co);
+    const int b0 = T.x, i0 = T.y, grp = T.z, tile = T.w;
     const int rp = t & 1, wp = rp ^ 1;
-    const int i = T.i0 + ty;
-    const bool row_ok = i < T.i1;
-    const int rows = T.i1 - T.i0;
-    const int cs = lane * V;          // column of this thread's first cell within the band
-    const int jb = T.b0 + cs;
-    const bool act = jb < P;
-    const bool core = core_warp(g, i, T.b0, T.be);
-    const long long hplane = (long long)g.nx * g.Ph;
-    const int sc0 = g.src_off[blockIdx.x], se = g.src_off[blockIdx.x + 1];
-    const int rc0 = g.rx_off[blockIdx.x], re = g.rx_off[blockIdx.x + 1];
-
-    float ca[V], cb[V], ch[V];
+    const int lane = threadIdx.x & 31;
+    const int i = i0 + w;
+    const int nx = g.nx, ny = g.ny, th = g.th;
+    const int l = SHOT ? lane : 0;
+    const int j0 = SHOT ? b0 : b0 + lane * W;
+    if (i >= nx || (!SHOT && j0 >= ny)) return;
+    const int slot = SHOT ? lane : 0;
+    const int s = SHOT ? grp * 32 + lane : grp;
+    const long long go = (long long)grp * g.plane;
+    const PsiG rd = psi_group(g, rp, grp), wr = psi_group(g, wp, grp);
+    // column index of j0-1 within the boxes: Ez and Hx start at j0-1 (shot
+    // lanes) or b0-4 (column lanes); Hy one column later in shot lanes
+    const int cz = SHOT ? 0 : lane * W + 3;
+    const int cy = SHOT ? -1 : lane * W + 3;
+    const int cc = SHOT ? 3 : lane * W + 3;   // coefficient column of j0-1
+#define EZS(r, k) sEZ[((r) * G::FEZ + cz + (k)) * CS + l]
+#define HXS(r, k) sHX[((r) * G::FHX + cz + (k)) * CS + l]
+#define HYS(r, k) sHY[((r) * G::FHY + cy + (k)) * CS + l]
+#define COS(p, r, k) sCO[((p) * (R + 1) + (r)) * G::NCF + cc + (k)]
+    // box rows: Ez, Hy, coefficients start at i0-1 (index w+1 = row i); Hx at i0 (index w = row i)
+    FwdIn<W> B;
+    float ezc[W + 2], hyu[W];
 #pragma unroll
-    for (int v = 0; v < V; ++v) { ca[v] = 0.f; cb[v] = 0.f; ch[v] = 0.f; }
-    const long long io = (long long)i * P + jb;   // this thread's cell offset within a plane
-    if (row_ok && act) {
-        ld_coef<V>(g, ca, g.ca + io);
-        ld_coef<V>(g, cb, g.cb + io);
-        ld_coef<V>(g, ch, g.ch + io);
+    for (int k = 0; k < W + 2; ++k) {
+        ezc[k] = EZS(w + 1, k);
+        B.en[k] = EZS(w + 2, k);
     }
-    float* er_s = ez_s + (1 + ty) * SE + 4;      // this warp's row of Ez_old, own cells
-    float* hxr_s = hx_s + ty * SE + 4;
+#pragma unroll
+    for (int k = 0; k <= W; ++k) {
+        B.hxo[k] = HXS(w, k);
+        B.ch[k] = COS(3, w + 1, k);
+    }
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        B.hyo[q] = HYS(w + 1, q + 1);
+        B.ca[q] = COS(0, w + 1, q + 1);
+        B.cb[q] = COS(1, w + 1, q + 1);
+    }
+    // new Hy of row i-1 (its auxiliaries are only read)
+#pragma unroll
+    for (int q = 0; q < W; ++q) hyu[q] = 0.f;
+    if (i >= 1) {
+        float ha[W], dz[W], chu[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            ha[q] = HYS(w, q + 1);
+            chu[q] = COS(3, w, q + 1);
+            dz[q] = __fsub_rn(ezc[q + 1], EZS(w, q + 1));
+            hyu[q] = ha[q];
+        }
+        const bool xcore = i - 1 >= th && i - 1 <= nx - th - 1;
+        if (xcore && j0 >= 1 && j0 + W <= ny) {
+#pragma unroll
+            for (int q = 0; q < W; ++q) hyu[q] = __fadd_rn(ha[q], __fmul_rn(chu[q], dz[q]));
+        } else if (g.fast_cpml) {
+            hy_cells<W, CS, false>(g, Rp, i - 1, j0, l, hyu, dz, chu, rd, rd);
+        } else {
+#pragma unroll
+            for (int q = 0; q < W; ++q)
+                if (j0 + q < ny) hyu[q] = hy_cell<CS, false>(g, Rp, i - 1, j0 + q, l, ha[q], dz[q], chu[q], rd, rd);
+        }
+    }
+#undef EZS
+#undef HXS
+#undef HYS
+#undef COS
+    const bool bcore = j0 >= th + 1 && j0 + W <= ny - th;
+    int sc = __ldg(g.src_off + tile);
+    const int se = __ldg(g.src_off + tile + 1);
+    int rc = __ldg(g.rx_off + tile);
+    const int re = __ldg(g.rx_off + tile + 1);
+    // skip the events of the rows above this warp's row
+    while (sc < se && __ldg(g.src_ev + sc).x < i) ++sc;
+    while (rc < re && __ldg(g.rx_ev + rc).x < i) ++rc;
+    const long long hrow = (long long)g.Ph * CS;
+    float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + grp) * nx) * hrow + (long long)j0 * CS + l : nullptr;
+    fwd_row<W, CS>(g, Rp, B, ezc, hyu, i, t, j0, l, slot, s, bcore, g.ez[wp] + go, g.hx[wp] + go, g.hy[wp] + go,
+                   hist, hrow, rd, wr, sc, se, rc, re);
+}
 
-    for (int q = 0; q < G; ++q) {
-        const int s = T.grp * G + q;
-        if (s >= g.S) break;
-        const long long so = (long long)s * g.plane;
-        const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-        // ---- stage Ez_old (tile + halo) and the old H values this thread updates
-        float hx[V], hy[V], ezo[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) { hx[v] = 0.f; hy[v] = 0.f; ezo[v] = 0.f; }
-        if (row_ok) {
-            if (act) {
-                ld_state<V>(g, ezo, g.ez[rp] + so + io);
-                ld_state<V>(g, hx, g.hx[rp] + so + io);
-                ld_state<V>(g, hy, g.hy[rp] + so + io);
-            }
-            sts_v<V>(er_s + cs, ezo);
-            if (lane == 0) er_s[-1] = T.b0 > 0 ? ld1(g, g.ez[rp] + so + io - 1) : 0.f;
-            if (lane == 31) er_s[32 * V] = T.be < P ? ld1(g, g.ez[rp] + so + io + V) : 0.f;
+template <int W, bool SHOT>
+__global__ void __launch_bounds__(288) k_fwd_pipe(const Dev g, const __grid_constant__ CUtensorMap tm_ez,
+                                                  const __grid_constant__ CUtensorMap tm_hx,
+                                                  const __grid_constant__ CUtensorMap tm_hy,
+                                                  const __grid_constant__ CUtensorMap tm_co, const int t,
+                                                  const int S) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int R = (blockDim.x >> 5) - 1;   // consumer warps; warp R produces
+    const TileSmem<W, SHOT> L(R, false);
+    const PipeSmem M(g.th, S, L.total);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + M.full);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
+    float* Rp = reinterpret_cast<float*>(smem + M.prof);
+    if (abort_launch(g, reinterpret_cast<volatile int*>(smem + M.flag))) return;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, R);
         }
-        if (ty == 0) {
-            // row above the tile (for the halo Hy) and row below (Ez[i1], the frame when i1 == nx)
-            float a[V], b[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) { a[v] = 0.f; b[v] = 0.f; }
-            if (act && T.i0 >= 1) ld_state<V>(g, a, g.ez[rp] + so + io - P);
-            if (act) ld_state<V>(g, b, g.ez[rp] + so + io + (long long)rows * P);
-            sts_v<V>(ez_s + 4 + cs, a);
-            sts_v<V>(ez_s + (rows + 1) * SE + 4 + cs, b);
+        fence_mbar_init();
+    }
+    for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) Rp[k] = __ldg(g.pml + k);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rp = t & 1;
+    if (warp == R) {
+        if (lane == 0)
+            produce_tiles(g, full, empty, S, [&](int p, int s, uint64_t* bar) {
+                fwd_tile_issue<W, SHOT>(g, &tm_ez, &tm_hx, &tm_hy, &tm_co, smem + M.stages + (size_t)s * L.total, L, R,
+                                        __ldg(g.tiles + p), rp, bar);
+            });
+        return;
+    }
+    int s = 0;
+    uint32_t par = 0;
+    int k = 0;
+    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
+        if (!consume_wait(g, full, s, par, k, S, 32 * R)) return;
+        fwd_tile_row<W, SHOT>(g, Rp, smem + M.stages + (size_t)s * L.total, L, R, warp, __ldg(g.tiles + p), t);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + s);
+        if (++s == S) {
+            s = 0;
+            par ^= 1u;
         }
-        __syncthreads();
-        // ---- H of the tile, the halo column b0-1 (Hx) and the halo row i0-1 (Hy)
-        if (row_ok) {
-            float e0[V], e1[V];
-            lds_v<V>(e0, er_s + cs);
-            lds_v<V>(e1, er_s + SE + cs);
-            const float eR = er_s[cs + V];
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float right = (v + 1 < V) ? e0[(v + 1) % V] : eR;
-                    hx[v] = __fsub_rn(hx[v], __fmul_rn(ch[v], __fsub_rn(right, e0[v])));
-                    hy[v] = __fadd_rn(hy[v], __fmul_rn(ch[v], __fsub_rn(e1[v], e0[v])));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int j = jb + v;
-                    const float right = (v + 1 < V) ? e0[(v + 1) % V] : eR;
-                    if (j < ny)
-                        h_update<true, true, true>(g, i, j, hx[v], hy[v], __fsub_rn(right, e0[v]),
-                                                   __fsub_rn(e1[v], e0[v]), ch[v], rd, wr);
-                }
-            }
-            sts_v<V>(hxr_s + cs, hx);
-            sts_v<V>(hy_s + (1 + ty) * SY + cs, hy);
-            if (lane == 0) {
-                float hl = 0.f, hy_unused = 0.f;
-                if (T.b0 > 0) {
-                    const int j = T.b0 - 1;
-                    hl = ld1(g, g.hx[rp] + so + io - 1);
-                    h_update<false, true, false>(g, i, j, hl, hy_unused, __fsub_rn(e0[0], er_s[-1]), 0.f,
-                                                 ldc1(g, g.ch + io - 1), rd, rd);
-                }
-                hxr_s[-1] = hl;
-            }
-        }
-        if (ty == 0) {
-            const int ih = T.i0 - 1;
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const int j = jb + v, c = cs + v;
-                float h = 0.f, hx_unused = 0.f;
-                if (ih >= 0 && j < ny) {
-                    h = ld1(g, g.hy[rp] + so + io - P + v);
-                    h_update<false, false, true>(g, ih, j, hx_unused, h, 0.f,
-                                                 __fsub_rn(ez_s[SE + 4 + c], ez_s[4 + c]), ldc1(g, g.ch + io - P + v),
-                                                 rd, rd);
-                }
-                hy_s[c] = h;
-            }
-        }
-        __syncthreads();
-        // ---- E of the tile, sources, stores, history, receivers
-        if (row_ok) {
-            float hyu[V], hxl[V];
-            lds_v<V>(hyu, hy_s + ty * SY + cs);
-            hxl[0] = hxr_s[cs - 1];
-#pragma unroll
-            for (int v = 1; v < V; ++v) hxl[v] = hx[v - 1];
-            float ezw[V];
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float dhy = __fsub_rn(hy[v], hyu[v]);
-                    const float dhx = __fsub_rn(hx[v], hxl[v]);
-                    ezw[v] = __fmaf_rn(-cb[v], dhx, madd2(ca[v], ezo[v], cb[v], dhy));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int j = jb + v;
-                    ezw[v] = ezo[v];
-                    if (j < ny)
-                        ezw[v] = e_update<true>(g, i, j, ezo[v], __fsub_rn(hy[v], hyu[v]), __fsub_rn(hx[v], hxl[v]),
-                                                ca[v], cb[v], rd, wr);
-                }
-            }
-            for (int k = sc0; k < se; ++k) {
-                const Ev e = __ldg(g.src_ev + k);
-                if (e.x != i || e.y != q) continue;
-#pragma unroll
-                for (int v = 0; v < V; ++v)
-                    if (jb + v == e.z) {
-                        const float cd = ldc1(g, g.cd + io + v);
-                        ezw[v] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezw[v]);
-                    }
-            }
-            if (act) {
-                st_state<V>(g, g.ez[wp] + so + io, ezw);
-                st_state<V>(g, g.hx[wp] + so + io, hx);
-                st_state<V>(g, g.hy[wp] + so + io, hy);
-            }
-            if (g.hist && jb < g.Ph)
-                st_state<V>(g, g.hist + ((long long)t * g.S + s) * hplane + (long long)i * g.Ph + jb, ezw);
-            if (t + 1 < g.nt) {
-                for (int k = rc0; k < re; ++k) {
-                    const Ev e = __ldg(g.rx_ev + k);
-                    if (e.x != i || e.y != q) continue;
-#pragma unroll
-                    for (int v = 0; v < V; ++v)
-                        if (jb + v == e.z) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezw[v];
-                }
-            }
-        }
-        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------
-// Reference-mode adjoint step.  Shared memory (floats), own cells at offset 4:
-//   hy_s  [TH+2][SE]   Hy_old rows i0-1 .. i1; col 4.. = b0.., 4+32V = be
-//   hx_s  [TH+1][SE]   Hx_old rows i0 .. i1;   col 3 = b0-1, 4.. = b0.., 4+32V = be
-//   en_s  [TH+1][SE]   E_new  rows i0 .. i1;   col 4.. = b0.., 4+32V = be
+// Reference-mode adjoint step
 // ---------------------------------------------------------------------------
-__host__ __device__ inline size_t tile_adj_smem(int TH, int V) {
-    return sizeof(float) * ((size_t)(3 * TH + 4) * (32 * V + 8));
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_tile_issue(const Dev& g, const CUtensorMap* tm_ez, const CUtensorMap* tm_hx,
+                                               const CUtensorMap* tm_hy, const CUtensorMap* tm_co,
+                                               const CUtensorMap* tm_h, unsigned char* st,
+                                               const TileSmem<W, SHOT>& L, int R, int4 T, int rp, int it,
+                                               uint64_t* bar) {
+    const int b0 = T.x, i0 = T.y, grp = T.z;
+    mbar_expect_tx(bar, TileSmem<W, SHOT>::tx_bytes(R, true));
+    const int cs = (SHOT ? b0 - 1 : b0 - 4) + PADC;
+    tma_state<SHOT>(st + L.ez, tm_ez, SHOT ? cs + 1 : cs, i0, grp, 0, rp, bar);
+    tma_state<SHOT>(st + L.hx, tm_hx, cs, i0, grp, 1, rp, bar);
+    tma_state<SHOT>(st + L.hy, tm_hy, SHOT ? cs + 1 : cs, i0 - 1, grp, 2, rp, bar);
+    tma_load_3d(st + L.co, tm_co, b0 - 4 + PADC, i0, 0, bar);
+    if (SHOT) tma_load_4d(st + L.hs, tm_h, 0, b0, i0, it * g.ngroups + grp, bar);
+    else tma_load_3d(st + L.hs, tm_h, b0, i0, it * g.ngroups + grp, bar);
 }
 
-// Adjoint E of cell (r, j) of shot s (with the residuals injected there, in
-// list order) from the staged old H values; STORE writes the auxiliaries.
-template <bool STORE>
-__device__ __forceinline__ float adj_e_tile(const GridDev& g, int r, int j, int q, float ez, float hy_c, float hy_u,
-                                            float hx_c, float hx_l, float ca, float cb, const Ev* ev, int k0, int k1,
-                                            const float* resid_s, const PsiShot& rd, const PsiShot& wr) {
-    for (int k = k0; k < k1; ++k) {
-        const Ev e = __ldg(ev + k);
-        if (e.x == r && e.y == q && e.z == j) ez = __fsub_rn(ez, resid_s[e.w]);
+// Box column indices of one lane: j0 within the Ez/Hy/new-E boxes, j0-1 within
+// the Hx box, j0-1 within the coefficient box.
+template <int W, bool SHOT>
+struct AdjCols {
+    int c0, cx, cc;
+    __device__ __forceinline__ AdjCols(int lane) {
+        c0 = SHOT ? 0 : lane * W + 4;
+        cx = SHOT ? 0 : lane * W + 3;
+        cc = SHOT ? 3 : lane * W + 3;
     }
-    return e_update<STORE>(g, r, j, ez, __fsub_rn(hy_c, hy_u), __fsub_rn(hx_c, hx_l), ca, cb, rd, wr);
+};
+
+// Phase 1: new E of rows i0 .. i0+R (row i0+R is the halo row below) into the
+// stage's new-E rows; warp w takes row i0+w, warp 0 also the halo row.
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsigned char* st,
+                                           const TileSmem<W, SHOT>& L, int R, int w, int4 T, int it, int rp) {
+    using G = TileGeom<W, SHOT>;
+    constexpr int CS = G::CS;
+    constexpr int NE = SHOT ? W + 1 : G::NWIN;
+    const float* sEZ = reinterpret_cast<const float*>(st + L.ez);
+    const float* sHX = reinterpret_cast<const float*>(st + L.hx);
+    const float* sHY = reinterpret_cast<const float*>(st + L.hy);
+    const float* sCO = reinterpret_cast<const float*>(st + L.co);
+    float* sEN = reinterpret_cast<float*>(st + L.en);
+    const int b0 = T.x, i0 = T.y, grp = T.z, tile = T.w;
+    const int lane = threadIdx.x & 31;
+    const int nx = g.nx, ny = g.ny, th = g.th;
+    const int l = SHOT ? lane : 0;
+    const int j0 = SHOT ? b0 : b0 + lane * W;
+    if (!SHOT && j0 >= ny) return;
+    const int slot = SHOT ? lane : 0;
+    const int s = SHOT ? grp * 32 + lane : grp;
+    const PsiG rd = psi_group(g, rp, grp), wr = psi_group(g, rp ^ 1, grp);
+    const int i1 = min(i0 + R, nx);
+    const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
+    const float* resid_s = g.resid + ((long long)s * g.nt + it) * g.nrx;
+    const AdjCols<W, SHOT> C(lane);
+#define EZS(r, k) sEZ[((r) * G::AEZ + C.c0 + (k)) * CS + l]
+#define HXS(r, k) sHX[((r) * G::AHX + C.cx + (k)) * CS + l]
+#define HYS(r, k) sHY[((r) * G::AHY + C.c0 + (k)) * CS + l]
+#define ENS(r, k) sEN[((r) * NE + C.c0 + (k)) * CS + l]
+#define COS(p, r, k) sCO[((p) * (R + 1) + (r)) * G::NCF + C.cc + (k)]
+    for (int rr = w; rr <= R; rr = (w == 0 && rr == 0) ? R : R + 1) {
+        const int r = i0 + rr;
+        if (r >= nx) {
+#pragma unroll
+            for (int k = 0; k <= W; ++k) ENS(rr, k) = 0.f;
+            continue;
+        }
+        AdjEIn<W> A;
+        float hyu[W + 1];
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            A.ez[k] = EZS(rr, k);
+            A.hyo[k] = HYS(rr + 1, k);
+            hyu[k] = HYS(rr, k);
+            A.ca[k] = COS(0, rr, k + 1);
+            A.cb[k] = COS(1, rr, k + 1);
+        }
+#pragma unroll
+        for (int k = 0; k < W + 2; ++k) A.hxo[k] = HXS(rr, k);
+        int ic = __ldg(g.inj_off + tile);
+        const int ie = __ldg(g.inj_off + tile + 1);
+        while (ic < ie && __ldg(g.inj_ev + ic).x < r) ++ic;
+        float e[W + 1];
+        adj_e_row<W, CS>(g, Rp, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_s,
+                         ic, ie, rd, wr);
+#pragma unroll
+        for (int k = 0; k <= W; ++k) ENS(rr, k) = e[k];
+    }
+#undef EZS
+#undef HXS
+#undef HYS
+#undef ENS
+#undef COS
 }
 
-template <int V>
-__global__ void __launch_bounds__(512, 2) k_adjoint_tile(const GridDev g, const int it, const int rp, const int G) {
-    extern __shared__ __align__(16) float sm[];
-    const int TH = blockDim.x >> 5;
-    const int lane = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const TileT T = tile_t(g, V);
-    const int SE = 32 * V + 8;
-    float* hy_s = sm;
-    float* hx_s = hy_s + (TH + 2) * SE;
-    float* en_s = hx_s + (TH + 1) * SE;
-    const int nx = g.nx, ny = g.ny, P = g.P;
+// Phase 2: H of row i0+w from the new E, the imaging sums, the stores.
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_tile_h(const Dev& g, const float* Rp, const unsigned char* st,
+                                           const TileSmem<W, SHOT>& L, int R, int w, int4 T, int it, int rp) {
+    using G = TileGeom<W, SHOT>;
+    constexpr int CS = G::CS;
+    constexpr int NE = SHOT ? W + 1 : G::NWIN;
+    const float* sEZ = reinterpret_cast<const float*>(st + L.ez);
+    const float* sHX = reinterpret_cast<const float*>(st + L.hx);
+    const float* sHY = reinterpret_cast<const float*>(st + L.hy);
+    const float* sCO = reinterpret_cast<const float*>(st + L.co);
+    const float* sH = reinterpret_cast<const float*>(st + L.hs);
+    const float* sEN = reinterpret_cast<const float*>(st + L.en);
+    const int b0 = T.x, i0 = T.y, grp = T.z;
+    const int lane = threadIdx.x & 31;
+    const int nx = g.nx, ny = g.ny, th = g.th;
+    const int i = i0 + w;
+    if (i >= nx) return;
+    const int l = SHOT ? lane : 0;
+    const int j0 = SHOT ? b0 : b0 + lane * W;
+    const bool live = SHOT || j0 < ny;
     const int wp = rp ^ 1;
-    const int i = T.i0 + ty;
-    const bool row_ok = i < T.i1;
-    const int rows = T.i1 - T.i0;
-    const bool last_row = ty == rows - 1;
-    const int cs = lane * V;
-    const int jb = T.b0 + cs;
-    const bool act = jb < P;
-    const int i1 = T.i1, be = T.be;
-    const long long hplane = (long long)nx * g.Ph;
-    const int ic0 = g.inj_off[blockIdx.x], ie = g.inj_off[blockIdx.x + 1];
-    const int hc0 = g.injh_off[blockIdx.x], he = g.injh_off[blockIdx.x + 1];
-    const bool core = core_warp(g, i, T.b0, T.be) && ic0 == ie;
-    const long long io = (long long)i * P + jb;
-    float* hyr_s = hy_s + (1 + ty) * SE + 4;     // Hy_old of row i, own cells
-    float* hxr_s = hx_s + ty * SE + 4;           // Hx_old of row i
-    float* enr_s = en_s + ty * SE + 4;           // E_new of row i
-
-    float ca[V], cb[V], ch[V];
+    const long long go = (long long)grp * g.plane;
+    const PsiG rd = psi_group(g, rp, grp), wr = psi_group(g, wp, grp);
+    const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
+    const AdjCols<W, SHOT> C(lane);
+#define EZS(r, k) sEZ[((r) * G::AEZ + C.c0 + (k)) * CS + l]
+#define HXS(r, k) sHX[((r) * G::AHX + C.cx + (k)) * CS + l]
+#define HYS(r, k) sHY[((r) * G::AHY + C.c0 + (k)) * CS + l]
+#define ENS(r, k) sEN[((r) * NE + C.c0 + (k)) * CS + l]
+#define COS(p, r, k) sCO[((p) * (R + 1) + (r)) * G::NCF + C.cc + (k)]
+    float ezc[W + 1], ezr[W], hx[W], hy[W], ch[W], f1[W], eo[W];
 #pragma unroll
-    for (int v = 0; v < V; ++v) { ca[v] = 0.f; cb[v] = 0.f; ch[v] = 0.f; }
-    if (row_ok && act) {
-        ld_coef<V>(g, ca, g.ca + io);
-        ld_coef<V>(g, cb, g.cb + io);
-        ld_coef<V>(g, ch, g.ch + io);
+    for (int k = 0; k <= W; ++k) ezc[k] = live ? ENS(w, k) : 0.f;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        ezr[q] = live ? ENS(w + 1, q) : 0.f;
+        hx[q] = live ? HXS(w, q + 1) : 0.f;
+        hy[q] = live ? HYS(w + 1, q) : 0.f;
+        ch[q] = live ? COS(3, w, q + 1) : 0.f;
+        eo[q] = live ? EZS(w, q) : 0.f;
+        f1[q] = live ? sH[((size_t)w * G::AH + (SHOT ? 0 : lane * W) + q) * CS + l] : 0.f;
     }
-    float acc_e[V], acc_s[V];
+#undef EZS
+#undef HXS
+#undef HYS
+#undef ENS
+#undef COS
+    if (live) {
+        if (bcore && i >= th + 1 && i <= nx - th - 1) {
 #pragma unroll
-    for (int v = 0; v < V; ++v) { acc_e[v] = 0.f; acc_s[v] = 0.f; }
-
-    for (int q = 0; q < G; ++q) {
-        const int s = T.grp * G + q;
-        if (s >= g.S) break;
-        const long long so = (long long)s * g.plane;
-        const PsiShot rd = psi_shot(g, rp, s), wr = psi_shot(g, wp, s);
-        const float* resid_s = g.resid + ((long long)s * g.nt + it) * g.nrx;
-        // ---- stage old H (tile + halo) and this thread's old Ez
-        float ezo[V], hxo[V], hyo[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) { ezo[v] = 0.f; hxo[v] = 0.f; hyo[v] = 0.f; }
-        if (row_ok) {
-            if (act) {
-                ld_state<V>(g, ezo, g.ez[rp] + so + io);
-                ld_state<V>(g, hxo, g.hx[rp] + so + io);
-                ld_state<V>(g, hyo, g.hy[rp] + so + io);
+            for (int q = 0; q < W; ++q) {
+                hx[q] = __fsub_rn(hx[q], __fmul_rn(ch[q], __fsub_rn(ezc[q + 1], ezc[q])));
+                hy[q] = __fadd_rn(hy[q], __fmul_rn(ch[q], __fsub_rn(ezr[q], ezc[q])));
             }
-            sts_v<V>(hyr_s + cs, hyo);
-            sts_v<V>(hxr_s + cs, hxo);
-            if (lane == 0) hxr_s[-1] = T.b0 > 0 ? ld1(g, g.hx[rp] + so + io - 1) : 0.f;
-            if (lane == 31) {
-                hxr_s[32 * V] = be < P ? ld1(g, g.hx[rp] + so + io + V) : 0.f;
-                hyr_s[32 * V] = be < P ? ld1(g, g.hy[rp] + so + io + V) : 0.f;
+        } else if (g.fast_cpml) {
+            float dzx[W], dzy[W];
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                dzx[q] = __fsub_rn(ezc[q + 1], ezc[q]);
+                dzy[q] = __fsub_rn(ezr[q], ezc[q]);
             }
-        }
-        if (ty == 0) {
-            // Hy row i0-1 (columns b0 .. be); Hx and Hy of the halo row i1
-            float a[V], bx[V], by[V];
+            hx_cells<W, CS>(g, Rp, i, j0, l, hx, dzx, ch, 0, rd, wr);
+            hy_cells<W, CS, true>(g, Rp, i, j0, l, hy, dzy, ch, rd, wr);
+        } else {
 #pragma unroll
-            for (int v = 0; v < V; ++v) { a[v] = 0.f; bx[v] = 0.f; by[v] = 0.f; }
-            if (act && T.i0 >= 1) ld_state<V>(g, a, g.hy[rp] + so + io - P);
-            if (act && i1 < nx) {
-                ld_state<V>(g, bx, g.hx[rp] + so + io + (long long)rows * P);
-                ld_state<V>(g, by, g.hy[rp] + so + io + (long long)rows * P);
-            }
-            sts_v<V>(hy_s + 4 + cs, a);
-            sts_v<V>(hx_s + rows * SE + 4 + cs, bx);
-            sts_v<V>(hy_s + (rows + 1) * SE + 4 + cs, by);
-            if (lane == 0) {
-                hy_s[4 + 32 * V] = (T.i0 >= 1 && be < P) ? ld1(g, g.hy[rp] + so + io - P + 32 * V) : 0.f;
-                hx_s[rows * SE + 3] = (T.b0 > 0 && i1 < nx) ? ld1(g, g.hx[rp] + so + io + (long long)rows * P - 1) : 0.f;
-            }
-        }
-        __syncthreads();
-        // ---- E_new of the tile, of the halo row i1 and of the halo column be
-        if (row_ok) {
-            float hu[V], hl[V], e[V];
-            lds_v<V>(hu, hyr_s - SE + cs);
-            hl[0] = hxr_s[cs - 1];
-#pragma unroll
-            for (int v = 1; v < V; ++v) hl[v] = hxo[v - 1];
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v)
-                    e[v] = __fmaf_rn(-cb[v], __fsub_rn(hxo[v], hl[v]),
-                                     madd2(ca[v], ezo[v], cb[v], __fsub_rn(hyo[v], hu[v])));
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int j = jb + v;
-                    e[v] = ezo[v];
-                    if (j < ny)
-                        e[v] = adj_e_tile<true>(g, i, j, q, ezo[v], hyo[v], hu[v], hxo[v], hl[v], ca[v], cb[v],
-                                                g.inj_ev, ic0, ie, resid_s, rd, wr);
+            for (int q = 0; q < W; ++q) {
+                const int j = j0 + q;
+                if (j < ny) {
+                    hx[q] = hx_cell<CS, true>(g, Rp, i, j, l, hx[q], __fsub_rn(ezc[q + 1], ezc[q]), ch[q], rd, wr);
+                    hy[q] = hy_cell<CS, true>(g, Rp, i, j, l, hy[q], __fsub_rn(ezr[q], ezc[q]), ch[q], rd, wr);
                 }
             }
-            sts_v<V>(enr_s + cs, e);
-            if (lane == 31) {
-                float eh = 0.f;
-                if (be < ny) {
-                    const long long c = io + V;
-                    const float ez = ld1(g, g.ez[rp] + so + c);
-                    eh = adj_e_tile<false>(g, i, be, q, ez, hyr_s[32 * V], hyr_s[32 * V - SE], hxr_s[32 * V],
-                                           hxr_s[32 * V - 1], ldc1(g, g.ca + c), ldc1(g, g.cb + c), g.injh_ev, hc0, he,
-                                           resid_s, rd, rd);
-                }
-                enr_s[32 * V] = eh;
-            }
         }
-        if (last_row) {
-            const float* hyb = hy_s + (rows + 1) * SE + 4;   // Hy_old row i1
-            const float* hxb = hx_s + rows * SE + 4;         // Hx_old row i1
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const int j = jb + v, c = cs + v;
-                float eb = 0.f;
-                if (i1 < nx && j < ny) {
-                    const long long o = io + (long long)P + v;   // (i1, j): the row after this warp's
-                    const float ez = ld1(g, g.ez[rp] + so + o);
-                    eb = adj_e_tile<false>(g, i1, j, q, ez, hyb[c], hyb[c - SE], hxb[c], hxb[c - 1],
-                                           ldc1(g, g.ca + o), ldc1(g, g.cb + o), g.inj_ev, ic0, ie, resid_s, rd, rd);
-                }
-                en_s[rows * SE + 4 + c] = eb;
-            }
-        }
-        __syncthreads();
-        // ---- H of the tile, imaging, stores
-        if (row_ok) {
-            float e0[V], e1[V], f1[V], f0[V];
-            lds_v<V>(e0, enr_s + cs);
-            lds_v<V>(e1, enr_s + SE + cs);
-            const float eR = enr_s[cs + V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) { f1[v] = 0.f; f0[v] = 0.f; }
-            if (jb < g.Ph) {
-                const float* h1 = g.hist + (((long long)it * g.S + s) * nx + i) * g.Ph + jb;
-                ld_state<V>(g, f1, h1);
-                ld_state<V>(g, f0, h1 - (long long)g.S * hplane);
-            }
-            if (core) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const float right = (v + 1 < V) ? e0[(v + 1) % V] : eR;
-                    hxo[v] = __fsub_rn(hxo[v], __fmul_rn(ch[v], __fsub_rn(right, e0[v])));
-                    hyo[v] = __fadd_rn(hyo[v], __fmul_rn(ch[v], __fsub_rn(e1[v], e0[v])));
-                    acc_e[v] = __fadd_rn(acc_e[v], __fmul_rn(__fsub_rn(f1[v], f0[v]), e0[v]));
-                    acc_s[v] = __fadd_rn(acc_s[v], __fmul_rn(__fmul_rn(f1[v], e0[v]), g.dt));
-                }
-            } else {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    const int j = jb + v;
-                    const float right = (v + 1 < V) ? e0[(v + 1) % V] : eR;
-                    if (j < ny) {
-                        h_update<true, true, true>(g, i, j, hxo[v], hyo[v], __fsub_rn(right, e0[v]),
-                                                   __fsub_rn(e1[v], e0[v]), ch[v], rd, wr);
-                        acc_e[v] = __fadd_rn(acc_e[v], __fmul_rn(__fsub_rn(f1[v], f0[v]), e0[v]));
-                        acc_s[v] = __fadd_rn(acc_s[v], __fmul_rn(__fmul_rn(f1[v], e0[v]), g.dt));
-                    }
-                }
-            }
-            if (act) {
-                st_state<V>(g, g.ez[wp] + so + io, e0);
-                st_state<V>(g, g.hx[wp] + so + io, hxo);
-                st_state<V>(g, g.hy[wp] + so + io, hyo);
-            }
-        }
-        __syncthreads();
     }
-    if (row_ok) {
-        double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
-        double* gas = gae + (long long)nx * ny;
+    // imaging (compute.py:1167-1172), summed by parts: sum_t Ez_f[t] (lambda_t -
+    // lambda_{t+1}) with lambda_{t+1} the old Ez of this step (k_imaging_tail
+    // subtracts Ez_f[0] lambda_1); sigma: sum_t Ez_f[t] lambda_t dt
+    float v[2 * W];
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int j = jb + v;
-            if (j < ny) {
-                const long long o = (long long)i * ny + j;
-                gae[o] += (double)acc_e[v];
-                gas[o] += (double)acc_s[v];
+    for (int q = 0; q < W; ++q) {
+        v[q] = __fmul_rn(f1[q], __fsub_rn(ezc[q], eo[q]));
+        v[W + q] = __fmul_rn(__fmul_rn(f1[q], ezc[q]), g.dt);
+    }
+    double* gae = g.gacc + (long long)grp * 2 * ((long long)nx * ny);
+    double* gas = gae + (long long)nx * ny;
+    const long long go2 = (long long)i * ny + j0;
+    if (SHOT) {
+        constexpr int sh = (2 * W) == 4 ? 3 : ((2 * W) == 8 ? 2 : 1);
+        const float x = lane_reduce_scatter<2 * W>(v, lane);
+        if ((lane & ((1 << sh) - 1)) == 0) {
+            const int e = lane >> sh;
+            const int q = e < W ? e : e - W;
+            if (j0 + q < ny) {
+                double* a = (e < W ? gae : gas) + go2 + q;
+                if (FG_OK_PTR(g, a, 8)) *a += (double)x;
             }
+        }
+    } else if (live) {
+#pragma unroll
+        for (int q = 0; q < W; ++q)
+            if (j0 + q < ny) {
+                if (FG_OK_PTR(g, gae + go2 + q, 8)) gae[go2 + q] += (double)v[q];
+                if (FG_OK_PTR(g, gas + go2 + q, 8)) gas[go2 + q] += (double)v[W + q];
+            }
+    }
+    if (!live) return;
+    const long long o = ((long long)i * g.P + j0 + PADC) * CS + l;
+    st_cells<W, CS>(g, g.ez[wp] + go + o, ezc);
+    st_cells<W, CS>(g, g.hx[wp] + go + o, hx);
+    st_cells<W, CS>(g, g.hy[wp] + go + o, hy);
+}
+
+template <int W, bool SHOT>
+__global__ void __launch_bounds__(288) k_adj_pipe(const Dev g, const __grid_constant__ CUtensorMap tm_ez,
+                                                  const __grid_constant__ CUtensorMap tm_hx,
+                                                  const __grid_constant__ CUtensorMap tm_hy,
+                                                  const __grid_constant__ CUtensorMap tm_co,
+                                                  const __grid_constant__ CUtensorMap tm_h, const int it,
+                                                  const int rp, const int S) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int R = (blockDim.x >> 5) - 1;
+    const TileSmem<W, SHOT> L(R, true);
+    const PipeSmem M(g.th, S, L.total);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + M.full);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
+    float* Rp = reinterpret_cast<float*>(smem + M.prof);
+    if (abort_launch(g, reinterpret_cast<volatile int*>(smem + M.flag))) return;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, R);
+        }
+        fence_mbar_init();
+    }
+    for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) Rp[k] = __ldg(g.pml + k);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == R) {
+        if (lane == 0)
+            produce_tiles(g, full, empty, S, [&](int p, int s, uint64_t* bar) {
+                adj_tile_issue<W, SHOT>(g, &tm_ez, &tm_hx, &tm_hy, &tm_co, &tm_h,
+                                        smem + M.stages + (size_t)s * L.total, L, R, __ldg(g.tiles + p), rp, it, bar);
+            });
+        return;
+    }
+    int s = 0;
+    uint32_t par = 0;
+    int k = 0;
+    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
+        if (!consume_wait(g, full, s, par, k, S, 32 * R)) return;
+        unsigned char* st = smem + M.stages + (size_t)s * L.total;
+        const int4 T = __ldg(g.tiles + p);
+        adj_tile_e<W, SHOT>(g, Rp, st, L, R, warp, T, it, rp);
+        consumers_sync(32 * R);
+        adj_tile_h<W, SHOT>(g, Rp, st, L, R, warp, T, it, rp);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + s);
+        if (++s == S) {
+            s = 0;
+            par ^= 1u;
         }
     }
 }

@@ -63,15 +63,26 @@ typedef struct fg_problem {
     const float* pml;      /* HOST (8, th) ERA ERB ERE ERF HRA HRB HRE HRF, or NULL if th == 0 */
 } fg_problem;
 
-/* Launch shape chosen by the autotuner; NULL or zero fields select defaults. */
+/* Launch shape (all zero or NULL = defaults chosen from the problem).  A tile
+ * is (shot group, row chunk, column band); each thread owns `cells_per_thread`
+ * consecutive columns of one shot. */
 typedef struct fg_tuning {
-    int32_t kernel;            /* 3 = prefetching warp march (default), 2 = staged 2-D tiles,
-                                  0 = TMA row-streaming tiles, 1 = per-warp register march */
-    int32_t cols_per_thread;   /* 1, 2 or 4 columns per thread */
-    int32_t shots_per_tile;    /* shots per tile: kernels 2, 3: 1..64; TMA tiles 1, 2, 4; register march 1, 2, 4, 8 */
-    int32_t rows_per_tile;     /* rows of one tile (>= 2; 2-D tiles <= 16, one warp per row) */
-    int32_t warps_per_tile;    /* TMA tiles: consumer warps, 1..16 */
-    int32_t stages;            /* TMA tiles: shared-memory ring depth, 3..8 */
+    int32_t lanes;             /* 0 = choose (shot lanes when shots >= 8), 1 = shot lanes: the 32
+                                  lanes of a warp are 32 shots of the same cells, 2 = column
+                                  lanes: one shot per warp, lanes own consecutive columns */
+    int32_t cells_per_thread;  /* 2, 4 or 8 (default 4 with shot lanes, 2 with column lanes) */
+    int32_t rows_per_tile;     /* rows of one tile, >= 1 (default 4) */
+    int32_t warps_per_block;   /* 1, 2 or 4 (default 4) */
+    int32_t stages;            /* lane march: 0 = operands loaded into registers row by row;
+                                  2..8 = a ring of this many rows per warp in shared memory,
+                                  filled ahead by bulk copies (shot lanes need cells_per_thread >= 4) */
+    int32_t kernel;            /* 0 = tensor-map tile pipeline: persistent CTAs of rows_per_tile
+                                  (2/4/8) consumer warps and one producer warp that fetches tiles
+                                  by cp.async.bulk.tensor into `stages` (2..4, default 3)
+                                  shared-memory stages; cells_per_thread 4/8 (shot lanes) or 2/4
+                                  (column lanes); 1 = lane march (persistent warps).  With no
+                                  kernel, stages, rows or cells given, shot lanes take the lane
+                                  march and column lanes the tile pipeline. */
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
@@ -82,9 +93,13 @@ typedef struct fg_plan fg_plan;
  * are rejected with FG_ERR_INVALID. */
 int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out);
 int fg_plan_destroy(fg_plan* plan);
-/* Row pitch (floats) of the Ez history fg_forward writes: the history is
- * (nt, shots, nx, pitch) with columns >= ny unused.  -1 on a NULL plan. */
-int32_t fg_plan_hist_pitch(const fg_plan* plan);
+/* Shape of the Ez history buffer fg_forward writes and fg_adjoint_reference
+ * reads: shape = {nt, groups, nx, pitch, slots}, float32, last index fastest.
+ * Ez after step t of shot s at cell (i, j) is element
+ * [t][s / slots][i][j][s % slots]; columns j >= ny and slots of shots >= the
+ * solve's count are padding.  The buffer holds the product of the five
+ * extents in floats. */
+int fg_plan_hist_shape(const fg_plan* plan, int64_t shape[5]);
 /* Device scratch a plan needs, in bytes (>= 0), or -1 on a NULL plan. */
 int64_t fg_plan_workspace_bytes(const fg_plan* plan);
 /* Attach a workspace (256-byte aligned device memory of at least
@@ -100,8 +115,8 @@ int fg_coefficients(const float* er, const float* se, const float* mr, int32_t n
 
 /* Forward solve (compute.py:574-712).  er, se, mr: (nx, ny) float32.
  * traces: (shots, nt, nrx) float32, Ez at each receiver at the start of each
- * step.  hist: (nt, shots, nx, fg_plan_hist_pitch) float32 Ez after each
- * step, or NULL. */
+ * step.  hist: Ez after each step in the layout of fg_plan_hist_shape, or
+ * NULL. */
 int fg_forward(fg_plan* plan, const float* er, const float* se, const float* mr,
                float* traces, float* hist, void* stream);
 

@@ -260,8 +260,18 @@ def setup(device, dx, ny, nx, nz, time_windows, source_location, source_step, re
 
 
 def _fields(G):
+    """The six field arrays (compute.py:499-518), each followed by a zeroed
+    tail.  The reference's H kernel reads Ez[i+1] and Ez[j+1] up to
+    (ny+1)(nz+1) + (nz+1) floats past the end of the last shot's buffer and
+    multiplies them by zero coefficients (src/lib/fields_updates_gpu.cu:65,75);
+    with torch's caching allocator that memory can hold NaN from an earlier
+    tensor, and NaN * 0 is NaN.  The zeroed tail gives the over-read the value
+    the reference's own runs see when it lands on zeros; the kernels and
+    their arguments are unchanged."""
     shape = (G.step, int(G.nx) + 1, int(G.ny) + 1, int(G.nz) + 1)
-    return [torch.zeros(shape, device=G.device) for _ in range(6)]  # Ex Ey Ez Hx Hy Hz
+    n = shape[0] * shape[1] * shape[2] * shape[3]
+    pad = 2 * shape[2] * shape[3] + 64
+    return [torch.zeros(n + pad, device=G.device)[:n].view(shape) for _ in range(6)]  # Ex Ey Ez Hx Hy Hz
 
 
 def _pml_call(lib, p, which, F, coef, G):

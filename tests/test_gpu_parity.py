@@ -113,18 +113,19 @@ def test_setup_matches_reference(fg, dev, refdrv):
 
 TUNINGS = [
     None,
-    {"kernel": 3, "cols_per_thread": 1, "shots_per_tile": 1, "rows_per_tile": 3},
-    {"kernel": 3, "cols_per_thread": 4, "shots_per_tile": 3, "rows_per_tile": 24},
-    {"kernel": 3, "cols_per_thread": 2, "shots_per_tile": 2, "rows_per_tile": 7},
-    {"kernel": 2, "cols_per_thread": 1, "shots_per_tile": 1, "rows_per_tile": 3},
-    {"kernel": 2, "cols_per_thread": 4, "shots_per_tile": 3, "rows_per_tile": 16},
-    {"kernel": 2, "cols_per_thread": 2, "shots_per_tile": 2, "rows_per_tile": 7},
-    {"kernel": 0, "cols_per_thread": 2, "shots_per_tile": 1, "rows_per_tile": 7, "warps_per_tile": 1, "stages": 3},
-    {"kernel": 0, "cols_per_thread": 4, "shots_per_tile": 2, "rows_per_tile": 33, "warps_per_tile": 2, "stages": 4},
-    {"kernel": 0, "cols_per_thread": 2, "shots_per_tile": 4, "rows_per_tile": 9, "warps_per_tile": 1, "stages": 5},
-    {"kernel": 0, "cols_per_thread": 1, "shots_per_tile": 2, "rows_per_tile": 5, "warps_per_tile": 3, "stages": 4},
-    {"kernel": 1, "cols_per_thread": 2, "shots_per_tile": 1, "rows_per_tile": 7},
-    {"kernel": 1, "cols_per_thread": 4, "shots_per_tile": 2, "rows_per_tile": 33},
+    # tensor-map tiles
+    {"lanes": 1, "cells_per_thread": 4, "rows_per_tile": 2},
+    {"lanes": 1, "cells_per_thread": 8, "rows_per_tile": 8, "stages": 2},
+    {"lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "stages": 4},
+    {"lanes": 2, "cells_per_thread": 2, "rows_per_tile": 8},
+    {"lanes": 2, "cells_per_thread": 4, "rows_per_tile": 2},
+    # lane march
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 2, "rows_per_tile": 3},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 7, "warps_per_block": 1},
+    {"kernel": 1, "lanes": 2, "cells_per_thread": 4, "rows_per_tile": 1},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 9, "stages": 2},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 16, "warps_per_block": 2, "stages": 4},
+    {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 6, "stages": 3},
 ]
 
 
@@ -137,7 +138,7 @@ def test_forward_bit_exact_vs_oracle(fg, orc, dev, tuning):
                                      torch.tensor(wl.mr, device=dev))
         o_tr, o_hist = orc.forward(prob, np.float32)
         np.testing.assert_array_equal(traces.cpu().numpy(), o_tr)
-        np.testing.assert_array_equal(hist[..., :wl.ny].cpu().numpy(), o_hist)
+        np.testing.assert_array_equal(solve.plan.hist_view(hist).cpu().numpy(), o_hist)
 
 
 @pytest.mark.parametrize("tuning", TUNINGS)
@@ -198,17 +199,18 @@ def test_tiling_invariance(fg, dev):
     wl = fg.workloads.small(shots=5, nt=100)
     w = torch.ones((wl.shots, wl.nt, wl.nrx), device=dev)
     base = _run_package(fg, wl, dev, w)
-    for tuning in TUNINGS[1:] + [{"kernel": 1, "cols_per_thread": 1, "shots_per_tile": 8, "rows_per_tile": 5}]:
+    for tuning in TUNINGS[1:]:
         got = _run_package(fg, wl, dev, w, tuning=tuning)
         assert torch.equal(got[0], base[0])
         for a, b in zip(got[1:], base[1:]):
             assert helpers.rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-6
 
 
-def test_shot_alone_equals_shot_in_batch(fg, dev):
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_shot_alone_equals_shot_in_batch(fg, dev, lanes):
     wl = fg.workloads.small(shots=4, nt=100)
     w = torch.ones((wl.shots, wl.nt, wl.nrx), device=dev)
-    tr, _, _ = _run_package(fg, wl, dev, w)
+    tr, _, _ = _run_package(fg, wl, dev, w, tuning={"lanes": lanes})
     setup = helpers.setup_for(wl, dev)
     for s in range(wl.shots):
         er = torch.tensor(wl.er[:, :, None], device=dev)
@@ -217,3 +219,22 @@ def test_shot_alone_equals_shot_in_batch(fg, dev):
                        customreceiver=setup.rx[s:s + 1].clone())
         tr1, _ = fg.compute(**kw)
         assert torch.equal(tr1[0], tr[s])
+
+
+def test_two_shot_groups_vs_oracle(fg, orc, dev):
+    """More shots than one warp's 32 lanes: two shot groups, the second padded."""
+    wl = fg.workloads.small(shots=37, nt=70, fixed=True)
+    wl.source_step = [0.03, 0.01, 0.0]
+    prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+    solve = fg.Solve(dev, setup, tv=False)
+    er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+    traces, hist = solve.forward(er, se, mr)
+    o_tr, o_hist = orc.forward(prob, np.float32)
+    np.testing.assert_array_equal(traces.cpu().numpy(), o_tr)
+    np.testing.assert_array_equal(solve.plan.hist_view(hist).cpu().numpy(), o_hist)
+    rng = np.random.default_rng(8)
+    resid = rng.standard_normal(traces.shape).astype(np.float32)
+    ge, gs = solve.gradient(er, se, mr, hist, torch.tensor(resid, device=dev), normalize=False)
+    oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
+    assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
+    assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
