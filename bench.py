@@ -59,10 +59,11 @@ PKG = "fast-gpr-fwi_b200"
 METRIC = "Gcell-steps/s fwd+adjoint"
 UNIT = "Gcell-steps/s"
 
-# DRAM bytes per shot-cell-step of the step kernels measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum, see profiles/); None until
-# a capture of the current kernels exists.
-NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": None, "adjoint": None}
+# DRAM bytes per shot-cell-step of the default step kernels, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch on the
+# 64-shot 440x340 grid, summarised under profiles/): forward
+# 261.3 MB, adjoint 282.5 MB per launch over 64 x 440 x 340 shot-cells.
+NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 261.3e6 / (64 * 440 * 340), "adjoint": 282.5e6 / (64 * 440 * 340)}
 
 
 def _fg():
@@ -413,16 +414,17 @@ def run_e2e(args, fg, wl, dev, rank, world):
 # CPU legs (the oracle: test infrastructure, used here only as the timed baseline)
 # ---------------------------------------------------------------------------
 
-def _cpu_problem(wl, setup, shots, nt):
-    """Oracle problem for a sample of the workload: the first `shots` shots,
+def _cpu_problem(wl, setup, shots, nt, first=0):
+    """Oracle problem for a sample of the workload: shots first..first+shots-1,
     the first `nt` steps, float32 coefficients restated on the host."""
     from oracle import oracle as orc
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import helpers
     coef = helpers.coefficients_f32(np.maximum(wl.er, 1), np.maximum(wl.se, 0), wl.mr, setup.dt32, setup.dx)
     pml = setup.profile.packed() if setup.profile is not None else np.zeros((8, 0), np.float32)
-    src = orc.positions2(setup.src.cpu().numpy()[:shots], wl.nx, wl.ny)
-    rx = orc.positions2(setup.rx.cpu().numpy()[:shots], wl.nx, wl.ny)
+    sel = slice(first, first + shots)
+    src = orc.positions2(setup.src.cpu().numpy()[sel], wl.nx, wl.ny)
+    rx = orc.positions2(setup.rx.cpu().numpy()[sel], wl.nx, wl.ny)
     return orc.Problem(wl.nx, wl.ny, setup.th, shots, nt, setup.dx, setup.dt32, coef["uE0"], coef["uE1"],
                        coef["uE4"], coef["uH1"], coef["uH4"], coef["uE0a"], pml, src,
                        np.ascontiguousarray(setup.srcw[:, :nt]), rx)
@@ -439,26 +441,38 @@ def _cpu_sample_run(prob):
 
 
 def _cpu_sample(wl, setup, seconds):
-    """Pick a sample (shots, nt) of the workload that runs about `seconds`."""
+    """Pick a sample of the workload that runs about `seconds`: `batches`
+    consecutive batches of `shots` shots, each solved over the first `nt`
+    steps (the history of one batch is kept under ~4 GB of host memory)."""
     from oracle import oracle as orc
     threads = orc.set_threads(os.cpu_count() or 1)
     shots = min(4, wl.shots)
     nt_cal = min(40, wl.nt)
+    _cpu_sample_run(_cpu_problem(wl, setup, shots, nt_cal))           # thread pool and page warm-up
+    nt_cal = min(120, wl.nt)
     t_cal = _cpu_sample_run(_cpu_problem(wl, setup, shots, nt_cal))
     per_step = t_cal / nt_cal
     nt = int(max(nt_cal, min(wl.nt, seconds / max(per_step, 1e-9))))
-    # history memory of the sample: keep it under ~4 GB
     nt = int(min(nt, 4e9 / (shots * wl.nx * wl.ny * 4)))
-    return shots, nt, threads
+    batches = int(max(1, min(wl.shots // shots, round(seconds / max(per_step * nt, 1e-9)))))
+    return shots, nt, batches, threads
+
+
+def _cpu_sample_time(wl, setup, shots, nt, batches):
+    return sum(_cpu_sample_run(_cpu_problem(wl, setup, shots, nt, b * shots)) for b in range(batches))
+
+
+def _sample_text(wl, shots, nt, batches):
+    return ("%s grid %dx%d, shots 0-%d in batches of %d, first %d of %d steps, fwd + reference adjoint"
+            % (wl.name, wl.nx, wl.ny, shots * batches - 1, shots, nt, wl.nt))
 
 
 def cpu_baseline(wl, setup, seconds):
-    shots, nt, threads = _cpu_sample(wl, setup, seconds)
-    t = _cpu_sample_run(_cpu_problem(wl, setup, shots, nt))
-    cells = wl.nx * wl.ny * shots * nt
+    shots, nt, batches, threads = _cpu_sample(wl, setup, seconds)
+    t = _cpu_sample_time(wl, setup, shots, nt, batches)
+    cells = wl.nx * wl.ny * shots * batches * nt
     return {"value": round(cells / t / 1e9, 4), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%s grid %dx%d, first %d shots, first %d of %d steps, fwd + reference adjoint, "
-                      "FP32 C++/OpenMP oracle, %.1f s" % (wl.name, wl.nx, wl.ny, shots, nt, wl.nt, t),
+            "sample": _sample_text(wl, shots, nt, batches) + ", FP32 C++/OpenMP oracle, %.1f s" % t,
             "cpu": _cpu_model()}
 
 
@@ -486,22 +500,20 @@ def run_reference(args, rank, world):
                                 torch.clamp(kw["er"], min=1), kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"], None,
                                 None, kw["Fixedreceiver"], None, None)
     seconds = max(2.0, min(args.cpu_seconds, 120.0 / max(1, args.steps + args.warmup)))
-    shots, nt, threads = _cpu_sample(wl, setup, seconds)
-    prob = _cpu_problem(wl, setup, shots, nt)
+    shots, nt, batches, threads = _cpu_sample(wl, setup, seconds)
     for _ in range(args.warmup):
-        _cpu_sample_run(prob)
-    times = [_cpu_sample_run(prob) for _ in range(args.steps)]
+        _cpu_sample_time(wl, setup, shots, nt, batches)
+    times = [_cpu_sample_time(wl, setup, shots, nt, batches) for _ in range(args.steps)]
     t = float(np.sum(times)) / args.steps
-    cells = wl.nx * wl.ny * shots * nt
+    cells = wl.nx * wl.ny * shots * batches * nt
     value = cells / t / 1e9
-    sample = ("%s grid %dx%d, first %d shots, first %d of %d steps per step, fwd + reference adjoint, "
-              "FP32 C++/OpenMP restatement of the reference kernels" % (wl.name, wl.nx, wl.ny, shots, nt, wl.nt))
+    sample = _sample_text(wl, shots, nt, batches) + " per step, FP32 C++/OpenMP restatement of the reference kernels"
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "%s: %dx%d compute grid, %d shots, nt=%d (bounded CPU sample: %d shots x %d steps)"
-                               % (wl.name, wl.nx, wl.ny, wl.shots, wl.nt, shots, nt)},
+                               % (wl.name, wl.nx, wl.ny, wl.shots, wl.nt, shots * batches, nt)},
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample, "cpu": _cpu_model()},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -125,15 +125,17 @@ void build_tiles(fg_plan* p) {
         }
     }
 
+    // events binned straight into their tiles (O(events), not O(tiles x events))
     const int bw = p->BW;
-    auto tile_events = [&](std::vector<Ev>& out, std::vector<int>& off, auto&& gen) {
+    std::vector<int> chunk_of_row(p->nx + 1, p->nc - 1);
+    for (int c = 0; c < p->nc; ++c)
+        for (int i = p->chunk_row[c]; i < p->chunk_row[c + 1]; ++i) chunk_of_row[i] = c;
+    auto tile_id = [&](int grp, int chunk, int band) { return (grp * p->nc + chunk) * p->nb + band; };
+    auto finish = [&](std::vector<std::vector<Ev>>& per, std::vector<Ev>& out, std::vector<int>& off) {
         out.clear();
         off.assign(p->ntiles + 1, 0);
-        std::vector<Ev> evs;
         for (int t = 0; t < p->ntiles; ++t) {
-            const int band = t % p->nb, rest = t / p->nb, chunk = rest % p->nc, grp = rest / p->nc;
-            evs.clear();
-            gen(evs, grp, p->chunk_row[chunk], p->chunk_row[chunk + 1], band * bw, band * bw + bw);
+            std::vector<Ev>& evs = per[t];
             std::stable_sort(evs.begin(), evs.end(), [](const Ev& a, const Ev& b) {
                 if (a.x != b.x) return a.x < b.x;
                 if (a.y != b.y) return a.y < b.y;
@@ -155,47 +157,36 @@ void build_tiles(fg_plan* p) {
     auto pos = [&](const std::vector<int32_t>& tab, int count, int s, int n, int c) {
         return tab[((size_t)s * count + n) * 3 + c];
     };
-    // the shots of a group: slot q is shot grp*SL + q
-    auto for_group = [&](int grp, auto&& fn) {
-        for (int q = 0; q < p->SL; ++q) {
-            const int s = grp * p->SL + q;
-            if (s >= p->S) break;
-            fn(s, q);
+    std::vector<std::vector<Ev>> src(p->ntiles), rxs(p->ntiles), inj(p->ntiles);
+    for (int s = 0; s < p->S; ++s) {
+        const int grp = s / p->SL, q = s % p->SL;
+        for (int n = 0; n < p->nsrc; ++n) {
+            if (!live[n]) continue;
+            const int i = pos(p->src, p->nsrc, s, n, 0), j = pos(p->src, p->nsrc, s, n, 1), k = pos(p->src, p->nsrc, s, n, 2);
+            if (classify(p, i, j, k) != 1) continue;
+            src[tile_id(grp, chunk_of_row[i], j / bw)].push_back(make_int4(i, q, j, n));
         }
-    };
-    tile_events(p->src_ev, p->src_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for_group(grp, [&](int s, int q) {
-            for (int n = 0; n < p->nsrc; ++n) {
-                if (!live[n]) continue;
-                const int i = pos(p->src, p->nsrc, s, n, 0), j = pos(p->src, p->nsrc, s, n, 1),
-                          k = pos(p->src, p->nsrc, s, n, 2);
-                if (classify(p, i, j, k) != 1) continue;
-                if (i >= i0 && i < i1 && j >= b0 && j < be) evs.push_back(make_int4(i, q, j, n));
-            }
-        });
-    });
-    tile_events(p->rx_ev, p->rx_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for_group(grp, [&](int s, int q) {
-            for (int r = 0; r < p->nrx; ++r) {
-                const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1),
-                          k = pos(p->rx, p->nrx, s, r, 2);
-                if (classify(p, i, j, k) != 1) continue;
-                if (i >= i0 && i < i1 && j >= b0 && j < be) evs.push_back(make_int4(i, q, j, r));
-            }
-        });
-    });
-    // adjoint injections: rows [i0, i1] and columns [b0, be] (row i1 and
-    // column be are recomputed as halo cells)
-    tile_events(p->inj_ev, p->inj_off, [&](std::vector<Ev>& evs, int grp, int i0, int i1, int b0, int be) {
-        for_group(grp, [&](int s, int q) {
-            for (int r = 0; r < p->nrx; ++r) {
-                const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1),
-                          k = pos(p->rx, p->nrx, s, r, 2);
-                if (classify(p, i, j, k) != 1) continue;
-                if (i >= i0 && i <= i1 && j >= b0 && j <= be) evs.push_back(make_int4(i, q, j, r));
-            }
-        });
-    });
+        for (int r = 0; r < p->nrx; ++r) {
+            const int i = pos(p->rx, p->nrx, s, r, 0), j = pos(p->rx, p->nrx, s, r, 1), k = pos(p->rx, p->nrx, s, r, 2);
+            if (classify(p, i, j, k) != 1) continue;
+            const int c = chunk_of_row[i], b = j / bw;
+            const Ev e = make_int4(i, q, j, r);
+            rxs[tile_id(grp, c, b)].push_back(e);
+            // adjoint injections: rows [i0, i1] and columns [b0, b0+bw] of a tile
+            // (row i1 and column b0+bw are recomputed as halo cells), so a cell on
+            // a tile's first row / first column also belongs to the tile above /
+            // to the left
+            inj[tile_id(grp, c, b)].push_back(e);
+            const bool up = c > 0 && i == p->chunk_row[c];
+            const bool left = b > 0 && j == b * bw;
+            if (up) inj[tile_id(grp, c - 1, b)].push_back(e);
+            if (left) inj[tile_id(grp, c, b - 1)].push_back(e);
+            if (up && left) inj[tile_id(grp, c - 1, b - 1)].push_back(e);
+        }
+    }
+    finish(src, p->src_ev, p->src_off);
+    finish(rxs, p->rx_ev, p->rx_off);
+    finish(inj, p->inj_ev, p->inj_off);
 }
 
 void layout(fg_plan* p) {
@@ -480,7 +471,8 @@ int encode_hist_map(const fg_plan* p, CUtensorMap* m, const float* hist) {
     return encode_map(m, hist, 3, dims, st, box);
 }
 
-// Persistent pipeline launches: TI consumer warps + 1 producer warp per CTA,
+// Persistent pipeline launches: WPB consumer warps (TI / WPB rows each) + 1
+// producer warp per CTA,
 // as many CTAs as are resident on the device (at most one per tile).
 template <class K>
 cudaError_t pipe_blocks(K kernel, int threads, size_t smem, int ntiles, int* blocks) {
@@ -499,10 +491,10 @@ cudaError_t launch_fwd_tile(fg_plan* p, const Dev& g, int t, cudaStream_t st) {
     const fg::TileSmem<W, SHOT> L(p->TI, false);
     const fg::PipeSmem M(p->th, p->D, L.total);
     auto kernel = fg::k_fwd_pipe<W, SHOT>;
-    const int threads = 32 * (p->TI + 1);
+    const int threads = 32 * (p->WPB + 1);
     const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->fwd_blocks);
     if (e != cudaSuccess) return e;
-    kernel<<<p->fwd_blocks, threads, M.total, st>>>(g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t, p->D);
+    kernel<<<p->fwd_blocks, threads, M.total, st>>>(g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t, p->D, p->TI);
     return cudaSuccess;
 }
 template <int W, bool SHOT>
@@ -510,11 +502,11 @@ cudaError_t launch_adj_tile(fg_plan* p, const Dev& g, const CUtensorMap& tmh, in
     const fg::TileSmem<W, SHOT> L(p->TI, true);
     const fg::PipeSmem M(p->th, p->D, L.total);
     auto kernel = fg::k_adj_pipe<W, SHOT>;
-    const int threads = 32 * (p->TI + 1);
+    const int threads = 32 * (p->WPB + 1);
     const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->adj_blocks);
     if (e != cudaSuccess) return e;
     kernel<<<p->adj_blocks, threads, M.total, st>>>(g, p->tm_aez, p->tm_ahx, p->tm_ahy, p->tm_co, tmh, it, rp,
-                                                     p->D);
+                                                     p->D, p->TI);
     return cudaSuccess;
 }
 using FwdTileFn = cudaError_t (*)(fg_plan*, const Dev&, int, cudaStream_t);
@@ -627,28 +619,30 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     }
     p->W = tune && tune->cells_per_thread ? tune->cells_per_thread : (p->shot ? 4 : 2);
     p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 4;
+    p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : (p->kernel == 0 ? std::min(p->TI, 4) : 4);
+    p->D = tune ? tune->stages : 0;
     if (p->kernel == 0) {
+        if (p->D == 0) p->D = 3;   // pipeline stages of the tile kernels
         const bool okw = p->shot ? (p->W == 4 || p->W == 8) : (p->W == 2 || p->W == 4);
-        const int st = tune ? tune->stages : 0;
-        if (!okw || !(p->TI == 2 || p->TI == 4 || p->TI == 8) || st < 0 || st == 1 || st > fg::MAX_STAGES) {
+        if (!okw || !(p->TI == 2 || p->TI == 4 || p->TI == 8 || p->TI == 16) || p->D < 2 || p->D > fg::MAX_STAGES ||
+            !(p->WPB == 1 || p->WPB == 2 || p->WPB == 4 || p->WPB == 8) || p->TI % p->WPB != 0) {
             delete p;
             return fail(FG_ERR_INVALID, "unsupported tuning: tiles take cells_per_thread 4/8 (shot lanes) or 2/4 "
-                                        "(column lanes), rows_per_tile 2/4/8 and stages 0 or 2..4");
+                                        "(column lanes), rows_per_tile 2/4/8/16 split evenly over warps_per_block "
+                                        "1/2/4/8 consumer warps, and stages 0 or 2..4");
         }
-    }
-    p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : 4;
-    p->D = tune ? tune->stages : 0;
-    if (p->kernel == 0 && p->D == 0) p->D = 3;   // pipeline stages of the tile kernels
-    if (!(p->W == 2 || p->W == 4 || p->W == 8) || p->TI < 1 || !(p->WPB == 1 || p->WPB == 2 || p->WPB == 4) ||
-        p->D < 0 || p->D == 1 || p->D > 8) {
-        delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning: cells_per_thread 2/4/8, rows_per_tile >= 1, "
-                                    "warps_per_block 1/2/4, stages 0 or 2..8");
-    }
-    // shot-lane stages copy coefficient rows from column j0-4: 16-byte aligned only for W >= 4
-    if (p->D > 0 && p->shot && p->W < 4) {
-        delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning: shot lanes with stages need cells_per_thread 4 or 8");
+    } else {
+        if (!(p->W == 2 || p->W == 4 || p->W == 8) || p->TI < 1 || !(p->WPB == 1 || p->WPB == 2 || p->WPB == 4) ||
+            p->D < 0 || p->D == 1 || p->D > 8) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: cells_per_thread 2/4/8, rows_per_tile >= 1, "
+                                        "warps_per_block 1/2/4, stages 0 or 2..8");
+        }
+        // shot-lane stages copy coefficient rows from column j0-4: 16-byte aligned only for W >= 4
+        if (p->D > 0 && p->shot && p->W < 4) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: shot lanes with stages need cells_per_thread 4 or 8");
+        }
     }
     if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
         delete p;

@@ -77,7 +77,7 @@ struct TileSmem {
     size_t ez, hx, hy, co, hs, en, total;
     __host__ __device__ TileSmem(int R, bool adjoint) {
         const size_t cs = G::CS * sizeof(float);
-        size_t o = 0;
+        size_t o = 128;   // header: tile (b0, i0, group, id) and its event-list offsets
         ez = o;
         o = align128(o + (adjoint ? (size_t)G::AEZ * (R + 1) : (size_t)G::FEZ * (R + 2)) * cs);
         hx = o;
@@ -104,6 +104,13 @@ struct TileSmem {
     }
 };
 
+// Stage header written by the producer (generic stores before it arms the
+// stage's barrier, so they are visible to the consumers after their wait).
+struct StageHead {
+    int4 tile;   // b0, i0, group, id
+    int4 ev;     // forward: source and receiver event ranges; adjoint: injection range
+};
+
 // Whole-CTA layout: barriers and flags, CPML profile, S stages.
 constexpr int MAX_STAGES = 4;
 struct PipeSmem {
@@ -111,7 +118,7 @@ struct PipeSmem {
     __host__ __device__ PipeSmem(int th, int S, size_t stage) {
         full = 0;
         empty = 8 * MAX_STAGES;
-        flag = 16 * MAX_STAGES;
+        flag = 16 * MAX_STAGES;   // [0] launch-abort copy of the error word, [1] this CTA gave up
         prof = 128;
         stages = align128(prof + (size_t)8 * th * sizeof(float));
         stage_bytes = stage;
@@ -166,55 +173,92 @@ __device__ __forceinline__ bool abort_launch(const Dev& g, volatile int* flag) {
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Barrier 1 among the R consumer warps, returning the AND of `ok` over them.
-__device__ __forceinline__ bool consumers_and(bool ok, int nthreads) {
-    uint32_t r;
-    asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-        : "=r"(r)
-        : "r"((uint32_t)ok), "r"(nthreads)
-        : "memory");
-    return r != 0;
-}
 __device__ __forceinline__ void consumers_sync(int nthreads) {
     asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
+// Bounded wait that gives up at once when the CTA has given up (`stop`); a
+// wait that runs out sets `stop` and the device error word.
+__device__ __forceinline__ bool wait_or_stop(const Dev& g, uint64_t* bar, uint32_t parity, volatile int* stop) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*stop) return false;
+        if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            *stop = 1;
+            atomicCAS(g.err, 0, ERR_WAIT_STAGE);
+            return false;
+        }
+        __nanosleep(20);
+    }
+    return true;
+}
+
 // Producer loop (lane 0 of warp R): for the CTA's k-th tile, wait until stage
-// k % S is free, arm its full barrier and issue the tile's copies.
+// k % S is free, write its header, arm its full barrier and issue the tile's
+// copies.  Before leaving it waits (bounded) for the stages it issued, so no
+// copy is still landing when the CTA retires.
 template <class Issue>
-__device__ __forceinline__ void produce_tiles(const Dev& g, uint64_t* full, uint64_t* empty, int S, Issue&& issue) {
+__device__ __forceinline__ void produce_tiles(const Dev& g, uint64_t* full, uint64_t* empty, int S, volatile int* stop,
+                                              Issue&& issue) {
     int s = 0;
     int k = 0;
     for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
         // the u-th reuse of a stage (u = k / S >= 1) waits for completion u-1
         // of its empty barrier
-        if (k >= S && !wait_stage(empty + s, (uint32_t)(k / S + 1) & 1u)) return;   // consumers stopped
+        if (k >= S && !wait_or_stop(g, empty + s, (uint32_t)(k / S + 1) & 1u, stop)) break;
         issue(p, s, full + s);
         if (++s == S) s = 0;
     }
+    // the last min(k, S) issued stages: tiles k-S .. k-1
+    for (int m = k - S < 0 ? 0 : k - S; m < k; ++m) wait_stage(full + (m % S), (uint32_t)(m / S) & 1u);
 }
 
-// Consumer side: wait for the k-th tile's stage; on a stage that never lands,
-// all consumers agree, wait (bounded) for the stages that may still be in
-// flight and report false.
-__device__ __forceinline__ bool consume_wait(const Dev& g, uint64_t* full, int s, uint32_t par, int k, int S,
-                                             int nthreads) {
-    const bool ok = wait_stage(full + s, par);
-    if (consumers_and(ok, nthreads)) return true;
-    if (threadIdx.x == 0) atomicCAS(g.err, 0, ERR_WAIT_STAGE);
-    // stages of tiles k .. k+S-1 may have been issued
-    int ss = s;
-    uint32_t pp = par;
-    for (int m = 0; m < S; ++m) {
-        if (blockIdx.x + (k + m) * gridDim.x >= g.ntiles) break;
-        wait_stage(full + ss, pp);
-        if (++ss == S) {
-            ss = 0;
-            pp ^= 1u;
+// Bulk prefetch of [p, p + bytes) into L2 (no data returned).
+__device__ __forceinline__ void prefetch_l2(const float* p, long long first, long long last) {
+    // [first, last] in floats, widened to 16-byte boundaries
+    const long long a = first & ~3LL, b = (last | 3LL) + 1;
+    if (b <= a) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + a), "r"((uint32_t)((b - a) * 4)) : "memory");
+}
+
+// Prefetch into L2 the CPML auxiliaries (read parity) a tile of rows
+// [r0, r1] and columns [jlo, jhi] touches, so that the consumers' gather
+// loads of a CPML tile hit L2.  Issued by the producer, S tiles ahead.
+template <int CS>
+__device__ __forceinline__ void prefetch_tile_psi(const Dev& g, int grp, int rp, int r0, int r1, int jlo, int jhi) {
+    const int th = g.th, nx = g.nx, ny = g.ny, P = g.P, TY = g.TY;
+    if (th <= 0) return;
+    r0 = max(r0, 0);
+    r1 = min(r1, nx - 1);
+    jlo = max(jlo, 0);
+    jhi = min(jhi, ny - 1);
+    if (r0 > r1 || jlo > jhi) return;
+    const PsiG rd = psi_group(g, rp, grp);
+    // x slabs: E rows 1..th (k = th-i), H rows 0..th-1 (k = th-1-i), both nx-th.. (k = th+i-(nx-th))
+    for (int i = r0; i <= r1; ++i) {
+        const int ke = (i >= 1 && i <= th) ? th - i : (i >= nx - th ? th + i - (nx - th) : -1);
+        const int kh = (i <= th - 1) ? th - 1 - i : (i >= nx - th ? th + i - (nx - th) : -1);
+        if (ke >= 0) prefetch_l2(rd.ex, ((long long)ke * P + jlo) * CS, ((long long)ke * P + jhi) * CS + CS - 1);
+        if (kh >= 0) prefetch_l2(rd.hx, ((long long)kh * P + jlo) * CS, ((long long)kh * P + jhi) * CS + CS - 1);
+    }
+    // y slabs: y0 columns 0..th (k = th-j for E, th-1-j for H), ymax columns ny-th.. (k = j-(ny-th))
+    const bool y0 = jlo <= th, ym = jhi >= ny - th;
+    if (!y0 && !ym) return;
+    const int k0lo = max(0, th - 1 - jhi), k0hi = min(th - 1, th - jlo);
+    const int kmlo = max(jlo, ny - th) - (ny - th), kmhi = jhi - (ny - th);
+    for (int i = r0; i <= r1; ++i) {
+        if (y0 && k0lo <= k0hi) {
+            const long long o = (long long)i * TY;
+            prefetch_l2(rd.ey, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
+            prefetch_l2(rd.hy, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
+        }
+        if (ym && kmlo <= kmhi) {
+            const long long o = (long long)(nx + 1 + i) * TY;
+            prefetch_l2(rd.ey, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
+            prefetch_l2(rd.hy, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
         }
     }
-    return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -223,34 +267,44 @@ __device__ __forceinline__ bool consume_wait(const Dev& g, uint64_t* full, int s
 template <int W, bool SHOT>
 __device__ __forceinline__ void fwd_tile_issue(const Dev& g, const CUtensorMap* tm_ez, const CUtensorMap* tm_hx,
                                                const CUtensorMap* tm_hy, const CUtensorMap* tm_co, unsigned char* st,
-                                               const TileSmem<W, SHOT>& L, int R, int4 T, int rp, uint64_t* bar) {
+                                               const TileSmem<W, SHOT>& L, int R, int p, int rp, uint64_t* bar) {
+    const int4 T = __ldg(g.tiles + p);
     const int b0 = T.x, i0 = T.y, grp = T.z;
+    StageHead* h = reinterpret_cast<StageHead*>(st);
+    h->tile = T;
+    h->ev = make_int4(__ldg(g.src_off + T.w), __ldg(g.src_off + T.w + 1), __ldg(g.rx_off + T.w),
+                      __ldg(g.rx_off + T.w + 1));
     mbar_expect_tx(bar, TileSmem<W, SHOT>::tx_bytes(R, false));
     const int cs = (SHOT ? b0 - 1 : b0 - 4) + PADC;   // first state column
     tma_state<SHOT>(st + L.ez, tm_ez, cs, i0 - 1, grp, 0, rp, bar);
     tma_state<SHOT>(st + L.hx, tm_hx, cs, i0, grp, 1, rp, bar);
     tma_state<SHOT>(st + L.hy, tm_hy, SHOT ? cs + 1 : cs, i0 - 1, grp, 2, rp, bar);
     tma_load_3d(st + L.co, tm_co, b0 - 4 + PADC, i0 - 1, 0, bar);
+    prefetch_tile_psi<TileGeom<W, SHOT>::CS>(g, grp, rp, i0 - 1, i0 + R - 1, b0 - 1, b0 + TileGeom<W, SHOT>::BW - 1);
 }
 
-// Row i0 + w of tile T from its stage.
+// Rows i0 + w*M .. i0 + w*M + M-1 of the stage's tile (R rows).
 template <int W, bool SHOT>
-__device__ __forceinline__ void fwd_tile_row(const Dev& g, const float* Rp, const unsigned char* st,
-                                             const TileSmem<W, SHOT>& L, int R, int w, int4 T, int t) {
+__device__ __forceinline__ void fwd_tile_rows(const Dev& g, const float* Rp, const unsigned char* st,
+                                              const TileSmem<W, SHOT>& L, int R, int w, int M, int t) {
+    const StageHead* hd = reinterpret_cast<const StageHead*>(st);
+    const int4 T = hd->tile;
+    const int4 E = hd->ev;
     using G = TileGeom<W, SHOT>;
     constexpr int CS = G::CS;
     const float* sEZ = reinterpret_cast<const float*>(st + L.ez);
     const float* sHX = reinterpret_cast<const float*>(st + L.hx);
     const float* sHY = reinterpret_cast<const float*>(st + L.hy);
     const float* sCO = reinterpret_cast<const float*>(st + L.co);
-    const int b0 = T.x, i0 = T.y, grp = T.z, tile = T.w;
+    const int b0 = T.x, i0 = T.y, grp = T.z;
     const int rp = t & 1, wp = rp ^ 1;
     const int lane = threadIdx.x & 31;
-    const int i = i0 + w;
+    const int rr0 = w * M;
+    const int ifirst = i0 + rr0;
     const int nx = g.nx, ny = g.ny, th = g.th;
     const int l = SHOT ? lane : 0;
     const int j0 = SHOT ? b0 : b0 + lane * W;
-    if (i >= nx || (!SHOT && j0 >= ny)) return;
+    if (ifirst >= nx || (!SHOT && j0 >= ny)) return;
     const int slot = SHOT ? lane : 0;
     const int s = SHOT ? grp * 32 + lane : grp;
     const long long go = (long long)grp * g.plane;
@@ -264,65 +318,72 @@ __device__ __forceinline__ void fwd_tile_row(const Dev& g, const float* Rp, cons
 #define HXS(r, k) sHX[((r) * G::FHX + cz + (k)) * CS + l]
 #define HYS(r, k) sHY[((r) * G::FHY + cy + (k)) * CS + l]
 #define COS(p, r, k) sCO[((p) * (R + 1) + (r)) * G::NCF + cc + (k)]
-    // box rows: Ez, Hy, coefficients start at i0-1 (index w+1 = row i); Hx at i0 (index w = row i)
-    FwdIn<W> B;
+    // box rows: Ez, Hy, coefficients start at i0-1 (index rr+1 = row i0+rr); Hx at i0
     float ezc[W + 2], hyu[W];
 #pragma unroll
-    for (int k = 0; k < W + 2; ++k) {
-        ezc[k] = EZS(w + 1, k);
-        B.en[k] = EZS(w + 2, k);
-    }
-#pragma unroll
-    for (int k = 0; k <= W; ++k) {
-        B.hxo[k] = HXS(w, k);
-        B.ch[k] = COS(3, w + 1, k);
-    }
-#pragma unroll
-    for (int q = 0; q < W; ++q) {
-        B.hyo[q] = HYS(w + 1, q + 1);
-        B.ca[q] = COS(0, w + 1, q + 1);
-        B.cb[q] = COS(1, w + 1, q + 1);
-    }
-    // new Hy of row i-1 (its auxiliaries are only read)
+    for (int k = 0; k < W + 2; ++k) ezc[k] = EZS(rr0 + 1, k);
+    // new Hy of row ifirst-1 (its auxiliaries are only read)
 #pragma unroll
     for (int q = 0; q < W; ++q) hyu[q] = 0.f;
-    if (i >= 1) {
+    if (ifirst >= 1) {
         float ha[W], dz[W], chu[W];
 #pragma unroll
         for (int q = 0; q < W; ++q) {
-            ha[q] = HYS(w, q + 1);
-            chu[q] = COS(3, w, q + 1);
-            dz[q] = __fsub_rn(ezc[q + 1], EZS(w, q + 1));
+            ha[q] = HYS(rr0, q + 1);
+            chu[q] = COS(3, rr0, q + 1);
+            dz[q] = __fsub_rn(ezc[q + 1], EZS(rr0, q + 1));
             hyu[q] = ha[q];
         }
-        const bool xcore = i - 1 >= th && i - 1 <= nx - th - 1;
+        const int iu = ifirst - 1;
+        const bool xcore = iu >= th && iu <= nx - th - 1;
         if (xcore && j0 >= 1 && j0 + W <= ny) {
 #pragma unroll
             for (int q = 0; q < W; ++q) hyu[q] = __fadd_rn(ha[q], __fmul_rn(chu[q], dz[q]));
         } else if (g.fast_cpml) {
-            hy_cells<W, CS, false>(g, Rp, i - 1, j0, l, hyu, dz, chu, rd, rd);
+            hy_cells<W, CS, false>(g, Rp, iu, j0, l, hyu, dz, chu, rd, rd);
         } else {
 #pragma unroll
             for (int q = 0; q < W; ++q)
-                if (j0 + q < ny) hyu[q] = hy_cell<CS, false>(g, Rp, i - 1, j0 + q, l, ha[q], dz[q], chu[q], rd, rd);
+                if (j0 + q < ny) hyu[q] = hy_cell<CS, false>(g, Rp, iu, j0 + q, l, ha[q], dz[q], chu[q], rd, rd);
         }
+    }
+    const bool bcore = j0 >= th + 1 && j0 + W <= ny - th;
+    int sc = E.x;
+    const int se = E.y;
+    int rc = E.z;
+    const int re = E.w;
+    // skip the events of the rows above this warp's rows
+    while (sc < se && __ldg(g.src_ev + sc).x < ifirst) ++sc;
+    while (rc < re && __ldg(g.rx_ev + rc).x < ifirst) ++rc;
+    const long long hrow = (long long)g.Ph * CS;
+    float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + grp) * nx) * hrow + (long long)j0 * CS + l : nullptr;
+    float* ezW = g.ez[wp] + go;
+    float* hxW = g.hx[wp] + go;
+    float* hyW = g.hy[wp] + go;
+    for (int m = 0; m < M; ++m) {
+        const int rr = rr0 + m, i = i0 + rr;
+        if (i >= nx) break;
+        FwdIn<W> B;
+#pragma unroll
+        for (int k = 0; k < W + 2; ++k) B.en[k] = EZS(rr + 2, k);
+#pragma unroll
+        for (int k = 0; k <= W; ++k) {
+            B.hxo[k] = HXS(rr, k);
+            B.ch[k] = COS(3, rr + 1, k);
+        }
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            B.hyo[q] = HYS(rr + 1, q + 1);
+            B.ca[q] = COS(0, rr + 1, q + 1);
+            B.cb[q] = COS(1, rr + 1, q + 1);
+        }
+        fwd_row<W, CS>(g, Rp, B, ezc, hyu, i, t, j0, l, slot, s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr, sc, se, rc,
+                       re);
     }
 #undef EZS
 #undef HXS
 #undef HYS
 #undef COS
-    const bool bcore = j0 >= th + 1 && j0 + W <= ny - th;
-    int sc = __ldg(g.src_off + tile);
-    const int se = __ldg(g.src_off + tile + 1);
-    int rc = __ldg(g.rx_off + tile);
-    const int re = __ldg(g.rx_off + tile + 1);
-    // skip the events of the rows above this warp's row
-    while (sc < se && __ldg(g.src_ev + sc).x < i) ++sc;
-    while (rc < re && __ldg(g.rx_ev + rc).x < i) ++rc;
-    const long long hrow = (long long)g.Ph * CS;
-    float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + grp) * nx) * hrow + (long long)j0 * CS + l : nullptr;
-    fwd_row<W, CS>(g, Rp, B, ezc, hyu, i, t, j0, l, slot, s, bcore, g.ez[wp] + go, g.hx[wp] + go, g.hy[wp] + go,
-                   hist, hrow, rd, wr, sc, se, rc, re);
 }
 
 template <int W, bool SHOT>
@@ -330,19 +391,22 @@ __global__ void __launch_bounds__(288) k_fwd_pipe(const Dev g, const __grid_cons
                                                   const __grid_constant__ CUtensorMap tm_hx,
                                                   const __grid_constant__ CUtensorMap tm_hy,
                                                   const __grid_constant__ CUtensorMap tm_co, const int t,
-                                                  const int S) {
+                                                  const int S, const int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int R = (blockDim.x >> 5) - 1;   // consumer warps; warp R produces
+    const int NW = (blockDim.x >> 5) - 1;   // consumer warps; warp NW produces
+    const int Mrows = R / NW;               // rows per consumer warp (R rows per tile)
     const TileSmem<W, SHOT> L(R, false);
     const PipeSmem M(g.th, S, L.total);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + M.full);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
     float* Rp = reinterpret_cast<float*>(smem + M.prof);
-    if (abort_launch(g, reinterpret_cast<volatile int*>(smem + M.flag))) return;
+    volatile int* flags = reinterpret_cast<volatile int*>(smem + M.flag);
+    if (abort_launch(g, flags)) return;
     if (threadIdx.x == 0) {
+        flags[1] = 0;
         for (int s = 0; s < S; ++s) {
             mbar_init(full + s, 1);
-            mbar_init(empty + s, R);
+            mbar_init(empty + s, NW);
         }
         fence_mbar_init();
     }
@@ -350,20 +414,21 @@ __global__ void __launch_bounds__(288) k_fwd_pipe(const Dev g, const __grid_cons
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int rp = t & 1;
-    if (warp == R) {
+    if (warp == NW) {
         if (lane == 0)
-            produce_tiles(g, full, empty, S, [&](int p, int s, uint64_t* bar) {
+            produce_tiles(g, full, empty, S, flags + 1, [&](int p, int s, uint64_t* bar) {
                 fwd_tile_issue<W, SHOT>(g, &tm_ez, &tm_hx, &tm_hy, &tm_co, smem + M.stages + (size_t)s * L.total, L, R,
-                                        __ldg(g.tiles + p), rp, bar);
+                                        p, rp, bar);
             });
         return;
     }
     int s = 0;
     uint32_t par = 0;
-    int k = 0;
-    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
-        if (!consume_wait(g, full, s, par, k, S, 32 * R)) return;
-        fwd_tile_row<W, SHOT>(g, Rp, smem + M.stages + (size_t)s * L.total, L, R, warp, __ldg(g.tiles + p), t);
+    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x) {
+        // after a stage that never landed every wait returns at once and the
+        // tiles are skipped; the error word reports it
+        if (wait_or_stop(g, full + s, par, flags + 1))
+            fwd_tile_rows<W, SHOT>(g, Rp, smem + M.stages + (size_t)s * L.total, L, R, warp, Mrows, t);
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + s);
         if (++s == S) {
@@ -380,9 +445,13 @@ template <int W, bool SHOT>
 __device__ __forceinline__ void adj_tile_issue(const Dev& g, const CUtensorMap* tm_ez, const CUtensorMap* tm_hx,
                                                const CUtensorMap* tm_hy, const CUtensorMap* tm_co,
                                                const CUtensorMap* tm_h, unsigned char* st,
-                                               const TileSmem<W, SHOT>& L, int R, int4 T, int rp, int it,
+                                               const TileSmem<W, SHOT>& L, int R, int p, int rp, int it,
                                                uint64_t* bar) {
+    const int4 T = __ldg(g.tiles + p);
     const int b0 = T.x, i0 = T.y, grp = T.z;
+    StageHead* h = reinterpret_cast<StageHead*>(st);
+    h->tile = T;
+    h->ev = make_int4(__ldg(g.inj_off + T.w), __ldg(g.inj_off + T.w + 1), 0, 0);
     mbar_expect_tx(bar, TileSmem<W, SHOT>::tx_bytes(R, true));
     const int cs = (SHOT ? b0 - 1 : b0 - 4) + PADC;
     tma_state<SHOT>(st + L.ez, tm_ez, SHOT ? cs + 1 : cs, i0, grp, 0, rp, bar);
@@ -391,6 +460,7 @@ __device__ __forceinline__ void adj_tile_issue(const Dev& g, const CUtensorMap* 
     tma_load_3d(st + L.co, tm_co, b0 - 4 + PADC, i0, 0, bar);
     if (SHOT) tma_load_4d(st + L.hs, tm_h, 0, b0, i0, it * g.ngroups + grp, bar);
     else tma_load_3d(st + L.hs, tm_h, b0, i0, it * g.ngroups + grp, bar);
+    prefetch_tile_psi<TileGeom<W, SHOT>::CS>(g, grp, rp, i0, i0 + R, b0, b0 + TileGeom<W, SHOT>::BW);
 }
 
 // Box column indices of one lane: j0 within the Ez/Hy/new-E boxes, j0-1 within
@@ -409,7 +479,10 @@ struct AdjCols {
 // stage's new-E rows; warp w takes row i0+w, warp 0 also the halo row.
 template <int W, bool SHOT>
 __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsigned char* st,
-                                           const TileSmem<W, SHOT>& L, int R, int w, int4 T, int it, int rp) {
+                                           const TileSmem<W, SHOT>& L, int R, int w, int M, int it, int rp) {
+    const StageHead* hd = reinterpret_cast<const StageHead*>(st);
+    const int4 T = hd->tile;
+    const int4 E = hd->ev;
     using G = TileGeom<W, SHOT>;
     constexpr int CS = G::CS;
     constexpr int NE = SHOT ? W + 1 : G::NWIN;
@@ -418,7 +491,7 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
     const float* sHY = reinterpret_cast<const float*>(st + L.hy);
     const float* sCO = reinterpret_cast<const float*>(st + L.co);
     float* sEN = reinterpret_cast<float*>(st + L.en);
-    const int b0 = T.x, i0 = T.y, grp = T.z, tile = T.w;
+    const int b0 = T.x, i0 = T.y, grp = T.z;
     const int lane = threadIdx.x & 31;
     const int nx = g.nx, ny = g.ny, th = g.th;
     const int l = SHOT ? lane : 0;
@@ -436,7 +509,10 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
 #define HYS(r, k) sHY[((r) * G::AHY + C.c0 + (k)) * CS + l]
 #define ENS(r, k) sEN[((r) * NE + C.c0 + (k)) * CS + l]
 #define COS(p, r, k) sCO[((p) * (R + 1) + (r)) * G::NCF + C.cc + (k)]
-    for (int rr = w; rr <= R; rr = (w == 0 && rr == 0) ? R : R + 1) {
+    // warp w: rows w*M .. w*M+M-1; warp 0 also row R (the halo row below)
+    for (int m = 0; m <= M; ++m) {
+        const int rr = m < M ? w * M + m : (w == 0 ? R : R + 1);
+        if (rr > R) break;
         const int r = i0 + rr;
         if (r >= nx) {
 #pragma unroll
@@ -455,8 +531,8 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
         }
 #pragma unroll
         for (int k = 0; k < W + 2; ++k) A.hxo[k] = HXS(rr, k);
-        int ic = __ldg(g.inj_off + tile);
-        const int ie = __ldg(g.inj_off + tile + 1);
+        int ic = E.x;
+        const int ie = E.y;
         while (ic < ie && __ldg(g.inj_ev + ic).x < r) ++ic;
         float e[W + 1];
         adj_e_row<W, CS>(g, Rp, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_s,
@@ -472,9 +548,12 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
 }
 
 // Phase 2: H of row i0+w from the new E, the imaging sums, the stores.
+
+// H of row i0 + w (w: row index within the tile) from the new E, imaging, stores.
 template <int W, bool SHOT>
-__device__ __forceinline__ void adj_tile_h(const Dev& g, const float* Rp, const unsigned char* st,
-                                           const TileSmem<W, SHOT>& L, int R, int w, int4 T, int it, int rp) {
+__device__ __forceinline__ void adj_tile_h_row(const Dev& g, const float* Rp, const unsigned char* st,
+                                                    const TileSmem<W, SHOT>& L, int R, int w, int it, int rp) {
+    const int4 T = reinterpret_cast<const StageHead*>(st)->tile;
     using G = TileGeom<W, SHOT>;
     constexpr int CS = G::CS;
     constexpr int NE = SHOT ? W + 1 : G::NWIN;
@@ -584,49 +663,57 @@ __device__ __forceinline__ void adj_tile_h(const Dev& g, const float* Rp, const 
     st_cells<W, CS>(g, g.hy[wp] + go + o, hy);
 }
 
+// Rows w*M .. w*M+M-1 of the tile, phase 2.
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_tile_h(const Dev& g, const float* Rp, const unsigned char* st,
+                                           const TileSmem<W, SHOT>& L, int R, int w, int M, int it, int rp) {
+    for (int m = 0; m < M; ++m) adj_tile_h_row<W, SHOT>(g, Rp, st, L, R, w * M + m, it, rp);
+}
+
 template <int W, bool SHOT>
 __global__ void __launch_bounds__(288) k_adj_pipe(const Dev g, const __grid_constant__ CUtensorMap tm_ez,
                                                   const __grid_constant__ CUtensorMap tm_hx,
                                                   const __grid_constant__ CUtensorMap tm_hy,
                                                   const __grid_constant__ CUtensorMap tm_co,
                                                   const __grid_constant__ CUtensorMap tm_h, const int it,
-                                                  const int rp, const int S) {
+                                                  const int rp, const int S, const int R) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int R = (blockDim.x >> 5) - 1;
+    const int NW = (blockDim.x >> 5) - 1;   // consumer warps; warp NW produces
+    const int Mrows = R / NW;               // rows per consumer warp (R rows per tile)
     const TileSmem<W, SHOT> L(R, true);
     const PipeSmem M(g.th, S, L.total);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + M.full);
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
     float* Rp = reinterpret_cast<float*>(smem + M.prof);
-    if (abort_launch(g, reinterpret_cast<volatile int*>(smem + M.flag))) return;
+    volatile int* flags = reinterpret_cast<volatile int*>(smem + M.flag);
+    if (abort_launch(g, flags)) return;
     if (threadIdx.x == 0) {
+        flags[1] = 0;
         for (int s = 0; s < S; ++s) {
             mbar_init(full + s, 1);
-            mbar_init(empty + s, R);
+            mbar_init(empty + s, NW);
         }
         fence_mbar_init();
     }
     for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) Rp[k] = __ldg(g.pml + k);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == R) {
+    if (warp == NW) {
         if (lane == 0)
-            produce_tiles(g, full, empty, S, [&](int p, int s, uint64_t* bar) {
+            produce_tiles(g, full, empty, S, flags + 1, [&](int p, int s, uint64_t* bar) {
                 adj_tile_issue<W, SHOT>(g, &tm_ez, &tm_hx, &tm_hy, &tm_co, &tm_h,
-                                        smem + M.stages + (size_t)s * L.total, L, R, __ldg(g.tiles + p), rp, it, bar);
+                                        smem + M.stages + (size_t)s * L.total, L, R, p, rp, it, bar);
             });
         return;
     }
     int s = 0;
     uint32_t par = 0;
-    int k = 0;
-    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x, ++k) {
-        if (!consume_wait(g, full, s, par, k, S, 32 * R)) return;
+    for (int p = blockIdx.x; p < g.ntiles; p += gridDim.x) {
+        const bool ok = wait_or_stop(g, full + s, par, flags + 1);
         unsigned char* st = smem + M.stages + (size_t)s * L.total;
-        const int4 T = __ldg(g.tiles + p);
-        adj_tile_e<W, SHOT>(g, Rp, st, L, R, warp, T, it, rp);
-        consumers_sync(32 * R);
-        adj_tile_h<W, SHOT>(g, Rp, st, L, R, warp, T, it, rp);
+        if (ok) adj_tile_e<W, SHOT>(g, Rp, st, L, R, warp, Mrows, it, rp);
+        consumers_sync(32 * NW);
+        if (ok) adj_tile_h<W, SHOT>(g, Rp, st, L, R, warp, Mrows, it, rp);
         __syncwarp();
         if (lane == 0) mbar_arrive(empty + s);
         if (++s == S) {

@@ -119,6 +119,9 @@ TUNINGS = [
     {"lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "stages": 4},
     {"lanes": 2, "cells_per_thread": 2, "rows_per_tile": 8},
     {"lanes": 2, "cells_per_thread": 4, "rows_per_tile": 2},
+    {"lanes": 1, "cells_per_thread": 4, "rows_per_tile": 16, "warps_per_block": 4},
+    {"lanes": 1, "cells_per_thread": 4, "rows_per_tile": 8, "warps_per_block": 1, "stages": 2},
+    {"lanes": 2, "cells_per_thread": 2, "rows_per_tile": 16, "warps_per_block": 8},
     # lane march
     {"kernel": 1, "lanes": 1, "cells_per_thread": 2, "rows_per_tile": 3},
     {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 7, "warps_per_block": 1},
