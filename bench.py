@@ -270,10 +270,7 @@ def run_ours(args, rank, local, world):
             ev[1].record(stream)
         if world > 1:
             plan.adjoint_reference(er_d, se_d, mr_d, hist, resid, ge, gs, normalize=False)
-            torch.distributed.all_reduce(ge)
-            torch.distributed.all_reduce(gs)
-            ge.div_(torch.linalg.vector_norm(ge))
-            gs.div_(torch.linalg.vector_norm(gs))
+            fg.shots.combine_gradients(ge, gs)
         else:
             plan.adjoint_reference(er_d, se_d, mr_d, hist, resid, ge, gs, normalize=True)
         if ev is not None:
@@ -335,6 +332,10 @@ def run_ours(args, rank, local, world):
     if not args.no_e2e:
         e2e = run_e2e(args, fg, wl, dev, rank, world)
 
+    per_shot = None
+    if rank == 0 and world == 1 and not args.no_e2e:
+        per_shot = run_per_shot(args, fg, wl, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(wl, setup, args.cpu_seconds)
@@ -359,6 +360,7 @@ def run_ours(args, rank, local, world):
             "kernels": other,
             "clocks": clk,
             "e2e": e2e,
+            "per_shot_path": per_shot,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -408,6 +410,43 @@ def run_e2e(args, fg, wl, dev, rank, world):
     return {"value": round(world * cells / (ms * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_step": round(ms, 3),
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "api": "compute(..., tv=False) + traces.backward(resid)"}
+
+
+def run_per_shot(args, fg, wl, dev, shots=4):
+    """The plain per-shot drop-in path: compute() with step=1, one call (and
+    one backward) per shot, inputs resident on the device, for the first
+    `shots` shots of the workload; same metric as the batched solve."""
+    er = torch.as_tensor(np.ascontiguousarray(wl.er)[:, :, None], device=dev).requires_grad_(True)
+    se = torch.as_tensor(np.ascontiguousarray(wl.se)[:, :, None], device=dev).requires_grad_(True)
+    mr = torch.as_tensor(np.ascontiguousarray(wl.mr)[:, :, None], device=dev)
+    loc = torch.tensor(wl.source_location, dtype=torch.float32)
+    dsrc = torch.tensor(wl.source_step, dtype=torch.float32)
+    rloc = torch.tensor(wl.receiver_location, dtype=torch.float32)
+    drx = torch.tensor(wl.receiver_step, dtype=torch.float32)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(4321)
+    resid = torch.randn((1, wl.nt, wl.nrx), device=dev, generator=gen) * 1e-3
+
+    def one(s):
+        kw = wl.kwargs(dev, er=er, se=se, mr=mr, tv=False, step=1, source_location=loc + s * dsrc,
+                       receiver_location=rloc if wl.fixed_receiver else rloc + s * drx)
+        traces, _ = fg.compute(**kw)
+        traces.backward(resid)
+
+    one(0)
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for s in range(shots):
+        one(s)
+    t1.record()
+    torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1)
+    torch.cuda.empty_cache()
+    return {"value": round(wl.nx * wl.ny * shots * wl.nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+            "shots": shots, "ms_per_shot": round(ms / shots, 3),
+            "api": "compute(..., step=1, tv=False) + traces.backward(resid), looped over shots"}
 
 
 # ---------------------------------------------------------------------------

@@ -13,7 +13,7 @@ The package directory name is not a Python identifier; import it with
 ``importlib.import_module("fast-gpr-fwi_b200")`` (or alias it, e.g.
 ``sys.modules["src"] = ...`` for code written against the reference).
 """
-from . import grid, workloads
+from . import grid, shots, workloads
 from .compute import GPRFWI, Solve, compute
 from .multiscale import apply_filter, design_fir_filter
 from .tv import total_variation

@@ -1,6 +1,7 @@
 // libfastgpr: plan construction, workspace layout and the C ABI declared in
 // include/fastgpr.h.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -63,6 +64,8 @@ struct fg_plan {
         o_sums, o_partial, o_norms, o_err, total;
     // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
     int fwd_blocks = 0, adj_blocks = 0;
+    // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
+    float dinv = 0.f;
     long long plane, pxs, pys;
     size_t state_bytes, psi_bytes;
     char* ws = nullptr;
@@ -231,7 +234,7 @@ void fill_grid(fg_plan* p) {
     char* w = p->ws;
     g.nx = p->nx; g.ny = p->ny; g.P = p->P; g.th = p->th; g.TY = p->TY;
     g.S = p->S; g.nt = p->nt; g.nrx = p->nrx; g.Ph = p->Ph; g.ngroups = p->ngroups;
-    g.d = p->dx; g.dt = p->dt;
+    g.d = p->dx; g.dt = p->dt; g.dinv = p->dinv;
     g.plane = p->plane; g.pxs = p->pxs; g.pys = p->pys;
     const long long cplane = (long long)(p->nx + 1) * p->P;
     float* coef = (float*)(w + p->o_coef);
@@ -701,6 +704,22 @@ int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     FG_CUDA(up(p->o_srcw, p->srcw.data(), p->srcw.size() * sizeof(float)));
     FG_CUDA(up(p->o_pml, p->pml.data(), p->pml.size() * sizeof(float)));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_err, 0, sizeof(int) * 4, st));
+    // division by the cell size: the reciprocal step of div_d is enabled when
+    // it returns __fdiv_rn's bits for every significand (one binade decides all)
+    {
+        const float d = p->dx, dinv = 1.0f / p->dx;
+        p->dinv = 0.f;
+        if (d >= 0x1p-30f && d <= 0x1p30f && std::fabs((double)d * (double)dinv - 1.0) < 0x1p-25) {
+            int* bad = (int*)(p->ws + p->o_err) + 2;
+            fg::k_div_check<<<512, 256, 0, st>>>(d, dinv, bad);
+            FG_CUDA(cudaGetLastError());
+            int nbad = -1;
+            FG_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+            FG_CUDA(cudaStreamSynchronize(st));
+            if (nbad == 0) p->dinv = dinv;
+        }
+        p->g.dinv = p->dinv;
+    }
     if (p->kernel == 0) {
         const int rc = encode_tile_maps(p);
         if (rc) return rc;

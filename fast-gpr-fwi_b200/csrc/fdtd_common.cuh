@@ -48,6 +48,7 @@ struct Dev {
     int Ph;              // row pitch of the Ez history (cells, >= ny)
     int ngroups;         // shot groups
     float d;             // cell size (CPML derivative divisor)
+    float dinv;          // RN(1/d) when div_d may use it (checked at bind), else 0
     float dt;            // time step (sigma imaging factor)
     long long plane;     // floats of one group's plane of one field
     long long pxs, pys;  // floats of one group's x-slab / y-slab auxiliaries
@@ -159,6 +160,15 @@ __device__ __forceinline__ void st_cells(const Dev& g, float* p, const float* x)
     }
 }
 
+// a += x on a float64 imaging accumulator: a reduction applied by the memory
+// system (red.global.add.f64, round to nearest), so the warp does not wait
+// for the old value.  Every address has one adder per launch, so the result
+// is the plain a + x.
+__device__ __forceinline__ void acc_add(const Dev& g, double* a, double x) {
+    if (!FG_OK_PTR(g, a, 8)) return;
+    asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(a), "d"(x) : "memory");
+}
+
 // N consecutive coefficients of one row (planes are not per shot).
 template <int N>
 __device__ __forceinline__ void ld_coef(const Dev& g, float* x, const float* p) {
@@ -172,6 +182,31 @@ __device__ __forceinline__ float madd2(float a, float b, float c, float d) {
 }
 __device__ __forceinline__ float msub2(float a, float b, float c, float d) {
     return __fmaf_rn(a, b, -__fmul_rn(c, d));
+}
+
+// x / d rounded to nearest, as __fdiv_rn(x, d).  With dinv = RN(1/d) the
+// quotient is q = RN(x * dinv), then one correction step q' = RN(q + r * dinv)
+// with the exact remainder r = x - q d from an FMA (Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic,
+// ch. 5).  The step returns RN(x/d) when q is within one ulp of x/d, which
+// holds when |d * dinv - 1| < 2^-25.  The quotient of x and of x * 2^e round
+// alike, so one binade of x decides every x whose exponent keeps q and r
+// normal: the library enables dinv only after checking all 2^23 significands
+// of [1, 2) against __fdiv_rn on the device, and only for d in [2^-30, 2^30];
+// other x (|x| outside [2^-90, 2^90), NaN, infinity) take __fdiv_rn.
+__device__ __forceinline__ float div_d_step(float x, float d, float dinv) {
+    const float q = __fmul_rn(x, dinv);
+    const float r = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(r, dinv, q);
+}
+__device__ __forceinline__ float div_d(const Dev& g, float x) {
+    if (g.dinv != 0.f) {
+        const float ax = fabsf(x);
+        if (ax >= 0x1p-90f && ax < 0x1p90f) return div_d_step(x, g.d, g.dinv);
+        if (ax == 0.f) return __fmul_rn(x, g.dinv);   // +-0 / d keeps the sign of x (d > 0)
+    }
+    return __fdiv_rn(x, g.d);
 }
 
 // One HORIPML order-1 correction: F +-= u4*((RA-1)*D + RB*psi); psi = RE*psi - RF*D.
@@ -226,28 +261,28 @@ __device__ __forceinline__ float e_cell(const Dev& g, const float* R, int i, int
                 const int k = th - i;
                 const long long o = ((long long)k * P + j) * CS + l;
                 float psi = ldro(g, rd.ex + o);
-                ez = cpml<true>(g, ez, __fdiv_rn(dhy, g.d), cd, psi, R, k);
+                ez = cpml<true>(g, ez, div_d(g, dhy), cd, psi, R, k);
                 if (STORE) st1(g, wr.ex + o, psi);
             }
             if (y0) {
                 const int k = th - j;
                 const long long o = ((long long)i * g.TY + k) * CS + l;
                 float psi = ldro(g, rd.ey + o);
-                ez = cpml<false>(g, ez, __fdiv_rn(dhx, g.d), cd, psi, R, k);
+                ez = cpml<false>(g, ez, div_d(g, dhx), cd, psi, R, k);
                 if (STORE) st1(g, wr.ey + o, psi);
             }
             if (xm) {
                 const int k = i - (nx - th);
                 const long long o = ((long long)(th + k) * P + j) * CS + l;
                 float psi = ldro(g, rd.ex + o);
-                ez = cpml<true>(g, ez, __fdiv_rn(dhy, g.d), cd, psi, R, k);
+                ez = cpml<true>(g, ez, div_d(g, dhy), cd, psi, R, k);
                 if (STORE) st1(g, wr.ex + o, psi);
             }
             if (ym) {
                 const int k = j - (ny - th);
                 const long long o = ((long long)(nx + 1 + i) * g.TY + k) * CS + l;
                 float psi = ldro(g, rd.ey + o);
-                ez = cpml<false>(g, ez, __fdiv_rn(dhx, g.d), cd, psi, R, k);
+                ez = cpml<false>(g, ez, div_d(g, dhx), cd, psi, R, k);
                 if (STORE) st1(g, wr.ey + o, psi);
             }
         }
@@ -272,14 +307,14 @@ __device__ __forceinline__ float hx_cell(const Dev& g, const float* R, int i, in
                 const int k = th - 1 - j;
                 const long long o = ((long long)i * g.TY + k) * CS + l;
                 float psi = ldro(g, rd.hy + o);
-                hx = cpml<false>(g, hx, __fdiv_rn(dzx, g.d), ci, psi, HR, k);
+                hx = cpml<false>(g, hx, div_d(g, dzx), ci, psi, HR, k);
                 if (STORE) st1(g, wr.hy + o, psi);
             }
             if (ym) {
                 const int k = j - (ny - th);
                 const long long o = ((long long)(g.nx + 1 + i) * g.TY + k) * CS + l;
                 float psi = ldro(g, rd.hy + o);
-                hx = cpml<false>(g, hx, __fdiv_rn(dzx, g.d), ci, psi, HR, k);
+                hx = cpml<false>(g, hx, div_d(g, dzx), ci, psi, HR, k);
                 if (STORE) st1(g, wr.hy + o, psi);
             }
         }
@@ -304,14 +339,14 @@ __device__ __forceinline__ float hy_cell(const Dev& g, const float* R, int i, in
                 const int k = th - 1 - i;
                 const long long o = ((long long)k * P + j) * CS + l;
                 float psi = ldro(g, rd.hx + o);
-                hy = cpml<true>(g, hy, __fdiv_rn(dzy, g.d), ci, psi, HR, k);
+                hy = cpml<true>(g, hy, div_d(g, dzy), ci, psi, HR, k);
                 if (STORE) st1(g, wr.hx + o, psi);
             }
             if (xm) {
                 const int k = i - (nx - th);
                 const long long o = ((long long)(th + k) * P + j) * CS + l;
                 float psi = ldro(g, rd.hx + o);
-                hy = cpml<true>(g, hy, __fdiv_rn(dzy, g.d), ci, psi, HR, k);
+                hy = cpml<true>(g, hy, div_d(g, dzy), ci, psi, HR, k);
                 if (STORE) st1(g, wr.hx + o, psi);
             }
         }
@@ -362,9 +397,9 @@ __device__ __forceinline__ void e_cells(const Dev& g, const float* R, int i, int
         if (i >= 1 && j >= 1) e = __fmaf_rn(-cb[n], dhx[n], madd2(ca[n], e, cb[n], dhy[n]));
         const bool fy = fy0[n] || fym[n];
         const int ky = fy0[n] ? th - j : j - (ny - th);
-        if (fxr && !(xm && fy0[n])) e = cpml<true>(g, e, __fdiv_rn(dhy[n], g.d), cd[n], px[n], R, kx);
-        if (fy) e = cpml<false>(g, e, __fdiv_rn(dhx[n], g.d), cd[n], py[n], R, ky);
-        if (xm && fy0[n]) e = cpml<true>(g, e, __fdiv_rn(dhy[n], g.d), cd[n], px[n], R, kx);
+        if (fxr && !(xm && fy0[n])) e = cpml<true>(g, e, div_d(g, dhy[n]), cd[n], px[n], R, kx);
+        if (fy) e = cpml<false>(g, e, div_d(g, dhx[n]), cd[n], py[n], R, ky);
+        if (xm && fy0[n]) e = cpml<true>(g, e, div_d(g, dhy[n]), cd[n], px[n], R, kx);
         ez[n] = e;
     }
     if (!own_row) return;
@@ -406,7 +441,7 @@ __device__ __forceinline__ void hx_cells(const Dev& g, const float* R, int i, in
         if (i >= 1) h = msub2(1.0f, h, ch[n], dzx[n]);
         if (fy0[n] || fym[n]) {
             const int ky = fy0[n] ? th - 1 - j : j - (ny - th);
-            h = cpml<false>(g, h, __fdiv_rn(dzx[n], g.d), ci[n], py[n], HR, ky);
+            h = cpml<false>(g, h, div_d(g, dzx[n]), ci[n], py[n], HR, ky);
         }
         hx[n] = h;
     }
@@ -444,7 +479,7 @@ __device__ __forceinline__ void hy_cells(const Dev& g, const float* R, int i, in
         if (j >= ny) continue;
         float h = hy[n];
         if (j >= 1) h = madd2(1.0f, h, ch[n], dzy[n]);
-        if (fxr) h = cpml<true>(g, h, __fdiv_rn(dzy[n], g.d), ci[n], px[n], HR, kx);
+        if (fxr) h = cpml<true>(g, h, div_d(g, dzy[n]), ci[n], px[n], HR, kx);
         hy[n] = h;
     }
     if constexpr (STORE) {
@@ -501,6 +536,19 @@ __global__ void k_coefficients(const float* __restrict__ er, const float* __rest
     out[2 * plane + idx] = uE4;
     out[3 * plane + idx] = uH1;
     out[4 * plane + idx] = uH4;
+}
+
+// ---------------------------------------------------------------------------
+// Check of div_d's correction step against __fdiv_rn for every significand
+// of [1, 2): bad[0] counts the mismatches (bit patterns).
+// ---------------------------------------------------------------------------
+__global__ void k_div_check(float d, float dinv, int* bad) {
+    int n = 0;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < (1 << 23); m += gridDim.x * blockDim.x) {
+        const float x = __int_as_float(0x3f800000 | m);
+        n += __float_as_int(div_d_step(x, d, dinv)) != __float_as_int(__fdiv_rn(x, d));
+    }
+    if (n) atomicAdd(bad, n);
 }
 
 // ---------------------------------------------------------------------------

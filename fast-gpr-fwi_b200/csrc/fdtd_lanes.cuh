@@ -47,6 +47,7 @@
 #pragma once
 
 #include "fdtd_common.cuh"
+#include "fdtd_shot.cuh"
 
 namespace fg {
 
@@ -239,8 +240,9 @@ struct FwdIn {                 // operands of row i
 // Row i of the forward step from its operands; carries ezc (Ez_old of row i,
 // columns j0-1 .. j0+W) and hyu (Hy_new of row i-1) to the next row.
 template <int W, int CS>
-__device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const FwdIn<W>& B, float (&ezc)[W + 2],
-                                        float (&hyu)[W], int i, int t, int j0, int l, int slot, int s, bool bcore,
+__device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const BandY& by, const FwdIn<W>& B,
+                                        float (&ezc)[W + 2], float (&hyu)[W], int i, int t, int j0, int l, int slot,
+                                        int s, bool bcore,
                                         float* ezW, float* hxW, float* hyW, float* hist, long long hrow,
                                         const PsiG& rd, const PsiG& wr, int& sc, int se, int& rc, int re) {
     const int nx = g.nx, ny = g.ny, th = g.th;
@@ -255,6 +257,9 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const FwdI
         for (int w = 0; w < W; ++w)
             ezn[w] = __fmaf_rn(-B.cb[w], __fsub_rn(hxn[w + 1], hxn[w]),
                                madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
+    } else if (CS == 32 && by.lean) {
+        if constexpr (CS == 32)
+            fwd_row_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn, ezn);
     } else if (g.fast_cpml) {
         float dzx[W + 1], dzy[W], dhy[W], dhx[W];
 #pragma unroll
@@ -361,7 +366,7 @@ __device__ __forceinline__ void issue_fwd(const Dev& g, uint64_t* bar, float* st
 }
 
 template <int W, bool SHOT, bool RING>
-__global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int D) {
+__global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -427,6 +432,8 @@ __global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int
         const PsiG rd = psi_group(g, rp, T.grp), wr = psi_group(g, wp, T.grp);
         // H at columns j0-1 .. j0+W-1 and E at j0 .. j0+W-1 are all interior cells
         const bool bcore = j0 >= th + 1 && j0 + W <= ny - th;
+        BandY by{};
+        if constexpr (SHOT) by = band_fwd<W>(g, j0);
         int sc = __ldg(g.src_off + T.id);
         const int se = __ldg(g.src_off + T.id + 1);
         int rc = __ldg(g.rx_off + T.id);
@@ -436,12 +443,30 @@ __global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int
         // Ez_old of row i0, columns j0-1 .. j0+W, and the new Hy of the row
         // above the chunk (its auxiliaries are only read)
         float ezc[W + 2], hyu[W];
+        // operands of row i (direct loads)
+        FwdIn<W> B;
+        auto load_row = [&](int i) {
+            const long long crow = coef_at(g, i, j0);
+            B.en[0] = ldro(g, ezR + FG_CELL(i + 1, j0 - 1));
+            ld_cells<W, CS>(g, B.en + 1, ezR + FG_CELL(i + 1, j0));
+            B.en[W + 1] = ldro(g, ezR + FG_CELL(i + 1, j0 + W));
+            B.hxo[0] = ldro(g, hxR + FG_CELL(i, j0 - 1));
+            ld_cells<W, CS>(g, B.hxo + 1, hxR + FG_CELL(i, j0));
+            ld_cells<W, CS>(g, B.hyo, hyR + FG_CELL(i, j0));
+            ld_coef<W>(g, B.ca, g.ca + crow);
+            ld_coef<W>(g, B.cb, g.cb + crow);
+            B.ch[0] = ldro(g, g.ch + crow - 1);
+            ld_coef<W>(g, B.ch + 1, g.ch + crow);
+        };
 #pragma unroll
         for (int w = 0; w < W; ++w) hyu[w] = 0.f;
         if (T.live) {
             ezc[0] = ldro(g, ezR + FG_CELL(T.i0, j0 - 1));
             ld_cells<W, CS>(g, ezc + 1, ezR + FG_CELL(T.i0, j0));
             ezc[W + 1] = ldro(g, ezR + FG_CELL(T.i0, j0 + W));
+            // the first row's operands go out with the halo row's, so the tile
+            // start costs one memory round trip
+            if (!RING) load_row(T.i0);
             if (T.i0 >= 1) {
                 const int ih = T.i0 - 1;
                 float ea[W], ha[W], ca[W], dz[W];
@@ -453,7 +478,9 @@ __global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int
                     hyu[w] = ha[w];
                     dz[w] = __fsub_rn(ezc[w + 1], ea[w]);
                 }
-                if (g.fast_cpml) {
+                if (SHOT && by.lean) {
+                    if constexpr (SHOT) fwd_hy_halo_shot<W>(g, R, by, ih, j0, l, hyu, dz, ca, rd);
+                } else if (g.fast_cpml) {
                     hy_cells<W, CS, false>(g, R, ih, j0, l, hyu, dz, ca, rd, rd);
                 } else {
 #pragma unroll
@@ -465,7 +492,6 @@ __global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int
         const int nrow = T.i1 - T.i0;
         for (int n = 0; n < nrow; ++n) {
             const int i = T.i0 + n;
-            FwdIn<W> B;
             if (RING) {
                 const bool ok = wait_stage(bars + cslot, cpar);
                 if (!__all_sync(FULL, ok)) {
@@ -506,21 +532,11 @@ __global__ void __launch_bounds__(128) k_fwd(const Dev g, const int t, const int
                     fence_proxy_async();
                     produce();
                 }
-            } else if (T.live) {
-                const long long crow = coef_at(g, i, j0);
-                B.en[0] = ldro(g, ezR + FG_CELL(i + 1, j0 - 1));
-                ld_cells<W, CS>(g, B.en + 1, ezR + FG_CELL(i + 1, j0));
-                B.en[W + 1] = ldro(g, ezR + FG_CELL(i + 1, j0 + W));
-                B.hxo[0] = ldro(g, hxR + FG_CELL(i, j0 - 1));
-                ld_cells<W, CS>(g, B.hxo + 1, hxR + FG_CELL(i, j0));
-                ld_cells<W, CS>(g, B.hyo, hyR + FG_CELL(i, j0));
-                ld_coef<W>(g, B.ca, g.ca + crow);
-                ld_coef<W>(g, B.cb, g.cb + crow);
-                B.ch[0] = ldro(g, g.ch + crow - 1);
-                ld_coef<W>(g, B.ch + 1, g.ch + crow);
+            } else if (T.live && n > 0) {
+                load_row(i);
             }
             if (T.live)
-                fwd_row<W, CS>(g, R, B, ezc, hyu, i, t, j0, l, slot, T.s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr,
+                fwd_row<W, CS>(g, R, by, B, ezc, hyu, i, t, j0, l, slot, T.s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr,
                                sc, se, rc, re);
         }
         cur = nxt;
@@ -566,8 +582,8 @@ __device__ __forceinline__ void adj_e_load(const Dev& g, AdjEIn<W>& A, int r, in
 // own cells when `own` (row r inside the chunk); the halo column and the halo
 // row below the chunk only read theirs.
 template <int W, int CS>
-__device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, AdjEIn<W>& A, int r, int j0, int l, int slot,
-                                          bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
+__device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A, int r, int j0,
+                                          int l, int slot, bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
                                           const float* resid_s, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
     // back_source (back.cu:34): Ez -= residual, no scaling
     for (; ic < ie; ++ic) {
@@ -583,6 +599,9 @@ __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, AdjEIn<W
         for (int k = 0; k <= W; ++k)
             out[k] = __fmaf_rn(-A.cb[k], __fsub_rn(A.hxo[k + 1], A.hxo[k]),
                                madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
+    } else if (CS == 32 && by.lean) {
+        if constexpr (CS == 32)
+            adj_e_row_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
     } else if (g.fast_cpml) {
         float dhy[W + 1], dhx[W + 1];
 #pragma unroll
@@ -667,7 +686,7 @@ __device__ __forceinline__ void issue_adj(const Dev& g, uint64_t* bar, float* st
 }
 
 template <int W, bool SHOT, bool RING>
-__global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const int rp, const int D) {
+__global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -733,6 +752,8 @@ __global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const in
         const PsiG rd = psi_group(g, rp, T.grp), wr = psi_group(g, wp, T.grp);
         // E at columns j0 .. j0+W (incl. the halo) and H at j0 .. j0+W-1 are interior cells
         const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
+        BandY by{};
+        if constexpr (SHOT) by = band_adj<W>(g, j0);
         int ic = __ldg(g.inj_off + T.id);
         const int ie = __ldg(g.inj_off + T.id + 1);
         const float* resid_s = g.resid + ((long long)T.s * g.nt + it) * g.nrx;
@@ -757,7 +778,7 @@ __global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const in
             adj_e_load<W, CS>(g, A, T.i0, j0, l, ezR, hxR, hyR);
 #pragma unroll
             for (int w = 0; w < W; ++w) eoc[w] = A.ez[w];
-            adj_e_row<W, CS>(g, R, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
+            adj_e_row<W, CS>(g, R, by, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
                              ezc, resid_s, ic, ie, rd, wr);
 #pragma unroll
             for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
@@ -829,7 +850,7 @@ __global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const in
             if (r < nx) {
 #pragma unroll
                 for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
-                adj_e_row<W, CS>(g, R, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < T.i1, hyc, ezr,
+                adj_e_row<W, CS>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < T.i1, hyc, ezr,
                                  resid_s, ic, ie, rd, wr);
             } else {
 #pragma unroll
@@ -847,6 +868,16 @@ __global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const in
                     hx[w] = __fsub_rn(hxc[w + 1], __fmul_rn(ch[w], __fsub_rn(ezc[w + 1], ezc[w])));
                     hy[w] = __fadd_rn(hyc[w], __fmul_rn(ch[w], __fsub_rn(ezr[w], ezc[w])));
                 }
+            } else if (SHOT && by.lean) {
+                float dzx[W], dzy[W];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    hx[w] = hxc[w + 1];
+                    hy[w] = hyc[w];
+                    dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
+                    dzy[w] = __fsub_rn(ezr[w], ezc[w]);
+                }
+                if constexpr (SHOT) adj_h_row_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
             } else if (g.fast_cpml) {
                 float dzx[W], dzy[W];
 #pragma unroll
@@ -891,15 +922,15 @@ __global__ void __launch_bounds__(128) k_adj(const Dev g, const int it, const in
                     const int w = e < W ? e : e - W;
                     if (j0 + w < ny) {
                         double* a = (e < W ? gae : gas) + go2 + w;
-                        if (FG_OK_PTR(g, a, 8)) *a += (double)x;
+                        acc_add(g, a, (double)x);
                     }
                 }
             } else {
 #pragma unroll
                 for (int w = 0; w < W; ++w)
                     if (j0 + w < ny) {
-                        if (FG_OK_PTR(g, gae + go2 + w, 8)) gae[go2 + w] += (double)v[w];
-                        if (FG_OK_PTR(g, gas + go2 + w, 8)) gas[go2 + w] += (double)v[W + w];
+                        acc_add(g, gae + go2 + w, (double)v[w]);
+                        acc_add(g, gas + go2 + w, (double)v[W + w]);
                     }
             }
             const long long o = ((long long)i * P + j0 + PADC) * CS + l;

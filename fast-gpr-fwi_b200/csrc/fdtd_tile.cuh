@@ -309,6 +309,8 @@ __device__ __forceinline__ void fwd_tile_rows(const Dev& g, const float* Rp, con
     const int s = SHOT ? grp * 32 + lane : grp;
     const long long go = (long long)grp * g.plane;
     const PsiG rd = psi_group(g, rp, grp), wr = psi_group(g, wp, grp);
+    BandY by{};
+    if constexpr (SHOT) by = band_fwd<W>(g, j0);
     // column index of j0-1 within the boxes: Ez and Hx start at j0-1 (shot
     // lanes) or b0-4 (column lanes); Hy one column later in shot lanes
     const int cz = SHOT ? 0 : lane * W + 3;
@@ -339,6 +341,8 @@ __device__ __forceinline__ void fwd_tile_rows(const Dev& g, const float* Rp, con
         if (xcore && j0 >= 1 && j0 + W <= ny) {
 #pragma unroll
             for (int q = 0; q < W; ++q) hyu[q] = __fadd_rn(ha[q], __fmul_rn(chu[q], dz[q]));
+        } else if (SHOT && by.lean) {
+            if constexpr (SHOT) fwd_hy_halo_shot<W>(g, Rp, by, iu, j0, l, hyu, dz, chu, rd);
         } else if (g.fast_cpml) {
             hy_cells<W, CS, false>(g, Rp, iu, j0, l, hyu, dz, chu, rd, rd);
         } else {
@@ -377,7 +381,7 @@ __device__ __forceinline__ void fwd_tile_rows(const Dev& g, const float* Rp, con
             B.ca[q] = COS(0, rr + 1, q + 1);
             B.cb[q] = COS(1, rr + 1, q + 1);
         }
-        fwd_row<W, CS>(g, Rp, B, ezc, hyu, i, t, j0, l, slot, s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr, sc, se, rc,
+        fwd_row<W, CS>(g, Rp, by, B, ezc, hyu, i, t, j0, l, slot, s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr, sc, se, rc,
                        re);
     }
 #undef EZS
@@ -502,6 +506,8 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
     const PsiG rd = psi_group(g, rp, grp), wr = psi_group(g, rp ^ 1, grp);
     const int i1 = min(i0 + R, nx);
     const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
+    BandY by{};
+    if constexpr (SHOT) by = band_adj<W>(g, j0);
     const float* resid_s = g.resid + ((long long)s * g.nt + it) * g.nrx;
     const AdjCols<W, SHOT> C(lane);
 #define EZS(r, k) sEZ[((r) * G::AEZ + C.c0 + (k)) * CS + l]
@@ -535,7 +541,7 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
         const int ie = E.y;
         while (ic < ie && __ldg(g.inj_ev + ic).x < r) ++ic;
         float e[W + 1];
-        adj_e_row<W, CS>(g, Rp, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_s,
+        adj_e_row<W, CS>(g, Rp, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_s,
                          ic, ie, rd, wr);
 #pragma unroll
         for (int k = 0; k <= W; ++k) ENS(rr, k) = e[k];
@@ -605,6 +611,21 @@ __device__ __forceinline__ void adj_tile_h_row(const Dev& g, const float* Rp, co
                 hx[q] = __fsub_rn(hx[q], __fmul_rn(ch[q], __fsub_rn(ezc[q + 1], ezc[q])));
                 hy[q] = __fadd_rn(hy[q], __fmul_rn(ch[q], __fsub_rn(ezr[q], ezc[q])));
             }
+        } else if (SHOT && g.fast_cpml) {
+            float dzx[W], dzy[W];
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                dzx[q] = __fsub_rn(ezc[q + 1], ezc[q]);
+                dzy[q] = __fsub_rn(ezr[q], ezc[q]);
+            }
+            if constexpr (SHOT) {
+                const BandY by = band_adj<W>(g, j0);
+                if (by.lean) adj_h_row_shot<W>(g, Rp, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+                else {
+                    hx_cells<W, CS>(g, Rp, i, j0, l, hx, dzx, ch, 0, rd, wr);
+                    hy_cells<W, CS, true>(g, Rp, i, j0, l, hy, dzy, ch, rd, wr);
+                }
+            }
         } else if (g.fast_cpml) {
             float dzx[W], dzy[W];
 #pragma unroll
@@ -645,15 +666,15 @@ __device__ __forceinline__ void adj_tile_h_row(const Dev& g, const float* Rp, co
             const int q = e < W ? e : e - W;
             if (j0 + q < ny) {
                 double* a = (e < W ? gae : gas) + go2 + q;
-                if (FG_OK_PTR(g, a, 8)) *a += (double)x;
+                acc_add(g, a, (double)x);
             }
         }
     } else if (live) {
 #pragma unroll
         for (int q = 0; q < W; ++q)
             if (j0 + q < ny) {
-                if (FG_OK_PTR(g, gae + go2 + q, 8)) gae[go2 + q] += (double)v[q];
-                if (FG_OK_PTR(g, gas + go2 + q, 8)) gas[go2 + q] += (double)v[W + q];
+                acc_add(g, gae + go2 + q, (double)v[q]);
+                acc_add(g, gas + go2 + q, (double)v[W + q]);
             }
     }
     if (!live) return;
