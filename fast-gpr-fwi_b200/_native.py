@@ -28,7 +28,7 @@ FG_ERR_TIMEOUT = 4
 EXPORTS = (
     "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_shape", "fg_plan_workspace_bytes", "fg_plan_bind",
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
-    "fg_forward_static",
+    "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
 )
 
 
@@ -102,6 +102,11 @@ def lib() -> ctypes.CDLL:
     L.fg_adjoint_reference.restype = ctypes.c_int
     L.fg_forward_static.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.fg_forward_static.restype = ctypes.c_int
+    L.fg_tv_workspace_bytes.argtypes = [i32, i32]
+    L.fg_tv_workspace_bytes.restype = i64
+    L.fg_total_variation.argtypes = [vp, i32, i32, ctypes.c_double, ctypes.c_double, i32, ctypes.c_double, vp, vp,
+                                     i64, ctypes.POINTER(i32), vp]
+    L.fg_total_variation.restype = ctypes.c_int
     L.fg_plan_check.argtypes = [vp, vp]
     L.fg_plan_check.restype = ctypes.c_int
     L.fg_last_error.argtypes = []
@@ -211,3 +216,20 @@ def coefficients(er32, se32, mr32, dt32, dx32, adjoint, pitch=None):
     check(lib().fg_coefficients(ptr(er32), ptr(se32), ptr(mr32), nx, ny, float(dt32), float(dx32),
                                 1 if adjoint else 0, ptr(out), pitch, stream_handle(er32.device)))
     return out
+
+
+def total_variation(data: torch.Tensor, lamda: float, rho: float, num_iter: int, tol: float):
+    """fg_total_variation on a 2-D float32 CUDA tensor: (denoised copy, iterations)."""
+    if data.dim() != 2 or data.dtype != torch.float32 or not data.is_cuda:
+        raise ValueError("total_variation kernel: needs a 2-D float32 CUDA tensor")
+    L = lib()
+    d = data.contiguous()
+    M, N = d.shape
+    out = torch.empty_like(d)
+    ws = torch.empty(int(L.fg_tv_workspace_bytes(M, N)), dtype=torch.uint8, device=d.device)
+    iters = ctypes.c_int32(0)
+    with torch.cuda.device(d.device):
+        stream = torch.cuda.current_stream(d.device).cuda_stream
+        check(L.fg_total_variation(d.data_ptr(), M, N, float(lamda), float(rho), int(num_iter), float(tol),
+                                   out.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(iters), stream))
+    return out, int(iters.value)

@@ -14,6 +14,7 @@
 #include "fdtd_common.cuh"
 #include "fdtd_lanes.cuh"
 #include "fdtd_tile.cuh"
+#include "tv.cuh"
 
 using fg::Dev;
 using fg::Ev;
@@ -564,6 +565,83 @@ int static_scratch(void** out) {
 extern "C" {
 
 const char* fg_last_error(void) { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// Total-variation regulariser
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kTvMaxBlocks = 4096;
+struct TvLayout {
+    size_t arr, partial, pmax, words, total;
+    TvLayout(int M, int N) {
+        const size_t A = 256, cells = (size_t)(M + 2) * (N + 2);
+        arr = align_up(cells * sizeof(float), A);
+        partial = 7 * arr;
+        pmax = partial + align_up(2 * kTvMaxBlocks * sizeof(double), A);
+        words = pmax + align_up(kTvMaxBlocks * sizeof(float), A);
+        total = words + A;
+    }
+};
+}  // namespace
+
+int64_t fg_tv_workspace_bytes(int32_t M, int32_t N) {
+    if (M < 1 || N < 1) return -1;
+    return (int64_t)TvLayout(M, N).total;
+}
+
+int fg_total_variation(const float* data, int32_t M, int32_t N, double lamda, double rho, int32_t num_iter,
+                       double tol, float* out, void* workspace, int64_t bytes, int32_t* iters, void* stream) {
+    if (!data || !out) return fail(FG_ERR_INVALID, "fg_total_variation: NULL argument");
+    if (M < 1 || N < 1 || num_iter < 0) return fail(FG_ERR_INVALID, "fg_total_variation: bad shape or iteration count");
+    if (!(rho != 0.0)) return fail(FG_ERR_INVALID, "fg_total_variation: rho must be non-zero");
+    const TvLayout L(M, N);
+    if (!workspace || bytes < (int64_t)L.total) return fail(FG_ERR_WORKSPACE, "fg_total_variation: workspace too small");
+    if (((uintptr_t)workspace) % 256) return fail(FG_ERR_WORKSPACE, "fg_total_variation: workspace not 256-byte aligned");
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0, sms = 0, per_sm = 0, coop = 0;
+    FG_CUDA(cudaGetDevice(&dev));
+    FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    FG_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return fail(FG_ERR_CUDA, "fg_total_variation: device without cooperative launch");
+    FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fg::k_total_variation, fg::TV_THREADS, 0));
+    const long long cells = (long long)(M + 2) * (N + 2);
+    // one CTA per SM at most (cheap barriers), fewer for small models
+    long long blocks = std::min<long long>((cells + fg::TV_THREADS * 4 - 1) / (fg::TV_THREADS * 4), sms);
+    blocks = std::max<long long>(1, std::min<long long>(blocks, (long long)per_sm * sms));
+    blocks = std::min<long long>(blocks, kTvMaxBlocks);
+    char* w = (char*)workspace;
+    fg::TvArgs a;
+    a.data = data;
+    a.out = out;
+    a.M = M;
+    a.N = N;
+    // scalars as float32 tensor arithmetic sees them: products in double, then rounded
+    a.lam = (float)lamda;
+    a.lr = (float)(lamda * rho);
+    a.rho = (float)rho;
+    a.inv_rho = (float)(1.0 / rho);
+    a.den = (float)(1.0 + 4.0 * lamda * rho);
+    a.num_iter = num_iter;
+    a.tol = (double)(float)tol;
+    float* arr[7];
+    for (int k = 0; k < 7; ++k) arr[k] = (float*)(w + k * L.arr);
+    a.x0 = arr[0]; a.x1 = arr[1]; a.y = arr[2]; a.zx = arr[3]; a.zy = arr[4]; a.ux = arr[5]; a.uy = arr[6];
+    a.partial = (double*)(w + L.partial);
+    a.pmax = (float*)(w + L.pmax);
+    a.bar = (unsigned*)(w + L.words);
+    a.err = (int*)(w + L.words + 8);
+    a.iters = (int*)(w + L.words + 12);
+    FG_CUDA(cudaMemsetAsync(w + L.words, 0, 16, st));
+    void* args[] = {&a};
+    FG_CUDA(cudaLaunchCooperativeKernel((const void*)fg::k_total_variation, dim3((unsigned)blocks),
+                                        dim3(fg::TV_THREADS), args, 0, st));
+    int words[2] = {0, 0};
+    FG_CUDA(cudaMemcpyAsync(words, w + L.words + 8, sizeof(words), cudaMemcpyDeviceToHost, st));
+    FG_CUDA(cudaStreamSynchronize(st));
+    if (words[0] != 0) return fail(FG_ERR_TIMEOUT, "fg_total_variation: a grid barrier gave up");
+    if (iters) *iters = words[1];
+    return FG_OK;
+}
 
 int fg_plan_check(fg_plan* p, void* stream) {
     if (!p || !p->ws) return fail(FG_ERR_INVALID, "fg_plan_check: plan has no workspace");

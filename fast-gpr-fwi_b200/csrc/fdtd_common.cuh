@@ -169,12 +169,37 @@ __device__ __forceinline__ void acc_add(const Dev& g, double* a, double x) {
     asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(a), "d"(x) : "memory");
 }
 
-// N consecutive coefficients of one row (planes are not per shot).
-template <int N>
+// N consecutive coefficients of one row (planes are not per shot); p is
+// aligned to A floats (4: 16 bytes, 2: 8 bytes), so the run is read with
+// vector loads.
+template <int N, int A = 1>
 __device__ __forceinline__ void ld_coef(const Dev& g, float* x, const float* p) {
+    constexpr int V = A >= 4 ? 4 : (A >= 2 ? 2 : 1);
+    constexpr int NV = V > 1 ? N / V * V : 0;
 #pragma unroll
-    for (int k = 0; k < N; ++k) x[k] = ldro(g, p + k);
+    for (int k = 0; k < NV; k += V) {
+        if (!FG_OK_PTR(g, p + k, 4 * V)) {
+#pragma unroll
+            for (int q = 0; q < V; ++q) x[k + q] = 0.f;
+            continue;
+        }
+        if constexpr (V == 4) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(p + k));
+            x[k] = v.x; x[k + 1] = v.y; x[k + 2] = v.z; x[k + 3] = v.w;
+        } else if constexpr (V == 2) {
+            const float2 v = __ldg(reinterpret_cast<const float2*>(p + k));
+            x[k] = v.x; x[k + 1] = v.y;
+        }
+    }
+#pragma unroll
+    for (int k = NV; k < N; ++k) x[k] = ldro(g, p + k);
 }
+
+__device__ __forceinline__ long long coef_at(const Dev& g, int i, int j) { return (long long)i * g.P + j + PADC; }
+// Alignment (floats) of coef_at(i, j0) for a thread's first column j0: the
+// row pitch P and the pad are multiples of 4 and j0 is a multiple of W.
+template <int W>
+constexpr int CALIGN = W % 4 == 0 ? 4 : (W % 2 == 0 ? 2 : 1);
 
 // a*b + c*d with the first product fused, a*b - c*d likewise.
 __device__ __forceinline__ float madd2(float a, float b, float c, float d) {

@@ -51,7 +51,6 @@
 
 namespace fg {
 
-__device__ __forceinline__ long long coef_at(const Dev& g, int i, int j) { return (long long)i * g.P + j + PADC; }
 
 // ---------------------------------------------------------------------------
 // mbarrier / bulk-copy primitives (no multicast anywhere)
@@ -259,7 +258,8 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
                                madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
-            fwd_row_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn, ezn);
+            fwd_row_cpml_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn,
+                                 ezn);
     } else if (g.fast_cpml) {
         float dzx[W + 1], dzy[W], dhy[W], dhx[W];
 #pragma unroll
@@ -453,10 +453,10 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
             B.hxo[0] = ldro(g, hxR + FG_CELL(i, j0 - 1));
             ld_cells<W, CS>(g, B.hxo + 1, hxR + FG_CELL(i, j0));
             ld_cells<W, CS>(g, B.hyo, hyR + FG_CELL(i, j0));
-            ld_coef<W>(g, B.ca, g.ca + crow);
-            ld_coef<W>(g, B.cb, g.cb + crow);
+            ld_coef<W, CALIGN<W>>(g, B.ca, g.ca + crow);
+            ld_coef<W, CALIGN<W>>(g, B.cb, g.cb + crow);
             B.ch[0] = ldro(g, g.ch + crow - 1);
-            ld_coef<W>(g, B.ch + 1, g.ch + crow);
+            ld_coef<W, CALIGN<W>>(g, B.ch + 1, g.ch + crow);
         };
 #pragma unroll
         for (int w = 0; w < W; ++w) hyu[w] = 0.f;
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
                 float ea[W], ha[W], ca[W], dz[W];
                 ld_cells<W, CS>(g, ea, ezR + FG_CELL(ih, j0));
                 ld_cells<W, CS>(g, ha, hyR + FG_CELL(ih, j0));
-                ld_coef<W>(g, ca, g.ch + coef_at(g, ih, j0));
+                ld_coef<W, CALIGN<W>>(g, ca, g.ch + coef_at(g, ih, j0));
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
                     hyu[w] = ha[w];
@@ -572,8 +572,8 @@ __device__ __forceinline__ void adj_e_load(const Dev& g, AdjEIn<W>& A, int r, in
     A.hxo[W + 1] = ldro(g, hxR + (rb + W) * CS + l);
     ld_cells<W, CS>(g, A.hyo, hyR + rb * CS + l);
     A.hyo[W] = ldro(g, hyR + (rb + W) * CS + l);
-    ld_coef<W + 1>(g, A.ca, g.ca + rb);
-    ld_coef<W + 1>(g, A.cb, g.cb + rb);
+    ld_coef<W + 1, CALIGN<W>>(g, A.ca, g.ca + rb);
+    ld_coef<W + 1, CALIGN<W>>(g, A.cb, g.cb + rb);
 }
 
 // New E of row r, columns j0 .. j0+W (column j0+W is the halo), from the old
@@ -601,7 +601,7 @@ __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const Ba
                                madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
-            adj_e_row_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
+            adj_e_row_cpml_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
     } else if (g.fast_cpml) {
         float dhy[W + 1], dhx[W + 1];
 #pragma unroll
@@ -837,7 +837,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
             } else {
                 if (!work) continue;
                 if (r < nx) adj_e_load<W, CS>(g, A, r, j0, l, ezR, hxR, hyR);
-                ld_coef<W>(g, ch, g.ch + coef_at(g, i, j0));
+                ld_coef<W, CALIGN<W>>(g, ch, g.ch + coef_at(g, i, j0));
                 if (hist_ok) {
                     ld_cells<W, CS>(g, f1, f1g + (long long)i * hrow);
                 } else {
@@ -877,7 +877,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
                     dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
                     dzy[w] = __fsub_rn(ezr[w], ezc[w]);
                 }
-                if constexpr (SHOT) adj_h_row_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+                if constexpr (SHOT) adj_h_row_cpml_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
             } else if (g.fast_cpml) {
                 float dzx[W], dzy[W];
 #pragma unroll

@@ -620,7 +620,7 @@ __device__ __forceinline__ void adj_tile_h_row(const Dev& g, const float* Rp, co
             }
             if constexpr (SHOT) {
                 const BandY by = band_adj<W>(g, j0);
-                if (by.lean) adj_h_row_shot<W>(g, Rp, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+                if (by.lean) adj_h_row_cpml_shot<W>(g, Rp, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
                 else {
                     hx_cells<W, CS>(g, Rp, i, j0, l, hx, dzx, ch, 0, rd, wr);
                     hy_cells<W, CS, true>(g, Rp, i, j0, l, hy, dzy, ch, rd, wr);

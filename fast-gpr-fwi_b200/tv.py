@@ -29,7 +29,18 @@ def _d(x: torch.Tensor, dim: int) -> torch.Tensor:
 
 
 def total_variation(data, lamda=0.02, rho=1.0, num_iter=500, tol=1e-5):
+    """float32 CUDA models run the whole ADMM solve as one kernel
+    (fg_total_variation, libfastgpr.so); other tensors (CPU, float64) take
+    the tensor arithmetic below, which is the reference's own."""
     data.squeeze_(-1)
+    if data.is_cuda and data.dtype == torch.float32 and data.dim() == 2:
+        from . import _native
+        out, _ = _native.total_variation(data, lamda, rho, num_iter, tol)
+        return out.unsqueeze(-1)
+    return _total_variation_tensor(data, lamda, rho, num_iter, tol)
+
+
+def _total_variation_tensor(data, lamda=0.02, rho=1.0, num_iter=500, tol=1e-5):
     data_max = data.max()
     scaled = data / (data_max + 1e-6)
     M, N = scaled.shape

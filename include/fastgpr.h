@@ -164,6 +164,22 @@ int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const 
 int fg_forward_static(fg_plan* plan, const float* er, const float* se, const float* mr,
                       float* traces, float* hist, void* stream);
 
+/* Total-variation denoising of an (M, N) float32 model (reference
+ * src/tv.py:135-217, the regulariser of the default gradient,
+ * src/compute.py:916-933): ADMM on the model scaled by 1/(max + 1e-6) with a
+ * one-cell zero border, at most num_iter iterations, stopping when the
+ * update's L2 norm drops below tol; out = the result times max(data).  Each
+ * iteration repeats the float32 arithmetic of the reference's tensor
+ * operations; the convergence norm is summed in float64.  data, out and
+ * workspace are device memory (workspace: fg_tv_workspace_bytes(M, N) bytes,
+ * 256-byte aligned, not overlapping data or out).  One cooperative launch on
+ * `stream`, then a synchronisation of `stream`: *iters (host, may be NULL)
+ * receives the iteration count.  Returns FG_ERR_TIMEOUT if a device-side
+ * barrier gave up. */
+int64_t fg_tv_workspace_bytes(int32_t M, int32_t N);
+int fg_total_variation(const float* data, int32_t M, int32_t N, double lamda, double rho, int32_t num_iter,
+                       double tol, float* out, void* workspace, int64_t bytes, int32_t* iters, void* stream);
+
 /* Wait for the plan's work on `stream`, then read and clear the device-side
  * error word its kernels set (an out-of-range access caught by the checked
  * build, or a bounded wait that gave up).  Returns FG_OK, FG_ERR_TIMEOUT or

@@ -60,3 +60,11 @@ def test_plan_validation_without_gpu(fg):
     assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_ERR_INVALID
     with pytest.raises(nat.FastGprError):
         nat.check(nat.FG_ERR_INVALID)
+
+
+def test_tv_workspace_size_without_gpu(fg):
+    from importlib import import_module
+    nat = import_module("fast-gpr-fwi_b200._native")
+    L = nat.lib()
+    assert L.fg_tv_workspace_bytes(440, 340) >= 7 * 442 * 342 * 4
+    assert L.fg_tv_workspace_bytes(0, 5) == -1
