@@ -115,6 +115,22 @@ def strip_cells(nx, ny, th):
     return 2 * th * ny + 2 * th * nx
 
 
+def kernel_name(tuning, direction):
+    """The step kernel a default (or given) launch shape runs, for the report."""
+    t = tuning or {}
+    if direction == "forward":
+        k = t.get("kernel", 1)
+    else:
+        ak = t.get("adj_kernel", 0)
+        k = (t.get("kernel", 1) if t else 0) if ak == 0 else (0 if ak == 1 else 1)
+    pair = t.get("lanes") == 3
+    if k == 0:
+        return "fg::k_%s_pipe (tensor-map tile pipeline, %s step)" % ("fwd" if direction == "forward" else "adj",
+                                                                      direction)
+    return "fg::k_%s%s (lane march%s, %s step)" % ("fwd" if direction == "forward" else "adj", "2" if pair else "",
+                                                  ", shot pairs" if pair else "", direction)
+
+
 def algorithmic_bytes(nx, ny, shots, th):
     """Per launch of the forward / adjoint step kernel.
 
@@ -317,7 +333,7 @@ def run_ours(args, rank, local, world):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None if ncu is None else int(ncu * S * nx * ny),
-                "kernel": "fg::k_adj (reference adjoint step)" if dom == "adjoint" else "fg::k_fwd (forward step)",
+                "kernel": kernel_name(tuning, dom),
                 "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 5)}
     other = {"forward": {"launch_ms": round(fwd_launch_ms, 5), "algorithmic_bytes_per_launch": int(fwd_b),
                          "achieved_gbs": round(fwd_b / (fwd_launch_ms * 1e-3) / 1e9, 1),
@@ -351,7 +367,7 @@ def run_ours(args, rank, local, world):
                        "shots_per_gpu": S, "nx": nx, "ny": ny, "nt": nt,
                        "history_gb": round(plan.hist_floats * 4 / 1e9, 1),
                        "l2": "inputs larger than L2 (state %.0f MB read + written per step, history %.0f GB)"
-                             % (plan.workspace.numel() / 1e6, plan.hist_floats * 4 / 1e9),
+                             % (24 * S * nx * ny / 1e6, plan.hist_floats * 4 / 1e9),
                        "tuning": tuning or "default",
                        "parallelism": "replicas: shots per GPU, one all-reduce of the imaging sums" if world > 1
                        else "single GPU"},

@@ -29,6 +29,7 @@ EXPORTS = (
     "fg_plan_create", "fg_plan_destroy", "fg_plan_hist_shape", "fg_plan_workspace_bytes", "fg_plan_bind",
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
+    "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
 )
 
 
@@ -47,9 +48,12 @@ class FgTuning(ctypes.Structure):
     _fields_ = [
         ("lanes", ctypes.c_int32), ("cells_per_thread", ctypes.c_int32), ("rows_per_tile", ctypes.c_int32),
         ("warps_per_block", ctypes.c_int32), ("stages", ctypes.c_int32), ("kernel", ctypes.c_int32),
+        ("adj_kernel", ctypes.c_int32), ("adj_rows_per_tile", ctypes.c_int32),
+        ("adj_warps_per_block", ctypes.c_int32), ("adj_stages", ctypes.c_int32),
     ]
 
-    KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel")
+    KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel",
+            "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages")
 
 
 class FastGprError(RuntimeError):
@@ -102,6 +106,12 @@ def lib() -> ctypes.CDLL:
     L.fg_adjoint_reference.restype = ctypes.c_int
     L.fg_forward_static.argtypes = [vp, vp, vp, vp, vp, vp, vp]
     L.fg_forward_static.restype = ctypes.c_int
+    L.fg_plan_checkpoint_bytes.argtypes = [vp, i32]
+    L.fg_plan_checkpoint_bytes.restype = i64
+    L.fg_forward_checkpointed.argtypes = [vp, vp, vp, vp, vp, vp, i64, i32, vp]
+    L.fg_forward_checkpointed.restype = ctypes.c_int
+    L.fg_adjoint_reference_checkpointed.argtypes = [vp, vp, vp, vp, vp, i64, i32, vp, vp, vp, vp, i32, vp, vp]
+    L.fg_adjoint_reference_checkpointed.restype = ctypes.c_int
     L.fg_tv_workspace_bytes.argtypes = [i32, i32]
     L.fg_tv_workspace_bytes.restype = i64
     L.fg_total_variation.argtypes = [vp, i32, i32, ctypes.c_double, ctypes.c_double, i32, ctypes.c_double, vp, vp,
@@ -203,6 +213,37 @@ class Plan:
         check(lib().fg_adjoint_reference(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(hist), ptr(resid),
                                          ptr(grad_eps), ptr(grad_sig), 1 if normalize else 0, ptr(norms),
                                          stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
+    # checkpointed solve (fg_forward_checkpointed / fg_adjoint_reference_checkpointed)
+    def checkpoint_bytes(self, interval: int) -> int:
+        return int(lib().fg_plan_checkpoint_bytes(self._h, int(interval)))
+
+    def new_checkpoints(self, interval: int) -> torch.Tensor:
+        """Checkpoint buffer for `interval` (at least 16 bytes, so it has an address)."""
+        return torch.empty(max(16, self.checkpoint_bytes(interval)), dtype=torch.uint8, device=self.device)
+
+    def new_segment(self, interval: int) -> torch.Tensor:
+        """History buffer of one segment of `interval` steps (flat float32)."""
+        return torch.empty(min(int(interval), self.nt) * (self.hist_floats // self.nt), dtype=torch.float32,
+                           device=self.device)
+
+    def forward_checkpointed(self, er32, se32, mr32, traces, ckpt, interval):
+        check(lib().fg_forward_checkpointed(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(traces), ptr(ckpt),
+                                            ckpt.numel() * ckpt.element_size(), int(interval),
+                                            stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
+    def adjoint_reference_checkpointed(self, er32, se32, mr32, ckpt, interval, segment, resid, grad_eps, grad_sig,
+                                       normalize=True, norms=None):
+        if segment.numel() < min(int(interval), self.nt) * (self.hist_floats // self.nt):
+            raise ValueError("segment buffer too small for interval %d" % interval)
+        check(lib().fg_adjoint_reference_checkpointed(
+            self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(ckpt), ckpt.numel() * ckpt.element_size(), int(interval),
+            ptr(segment), ptr(resid), ptr(grad_eps), ptr(grad_sig), 1 if normalize else 0, ptr(norms),
+            stream_handle(self.device)))
         if checked_build():
             self.device_check()
 

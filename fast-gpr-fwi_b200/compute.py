@@ -42,11 +42,43 @@ def _model2d(t: torch.Tensor, nx: int, ny: int) -> torch.Tensor:
     return t.to(torch.float32).contiguous()
 
 
+class Checkpoints:
+    """What a checkpointed forward solve keeps for its gradient: the state at
+    the start of every `interval`-th step (fg_forward_checkpointed)."""
+
+    def __init__(self, buf: torch.Tensor, interval: int):
+        self.buf = buf
+        self.interval = interval
+
+
+def checkpoint_interval(plan, checkpoint) -> Optional[int]:
+    """None (keep the whole Ez history) or the checkpoint interval in steps.
+    checkpoint=True picks the interval that minimises checkpoints + one
+    segment of history; an int is taken as the interval."""
+    if checkpoint is None or checkpoint is False:
+        return None
+    nt = plan.nt
+    if checkpoint is True:
+        step = plan.hist_floats // nt * 4
+        best = None
+        for k in range(1, nt + 1):
+            mem = plan.checkpoint_bytes(k) + k * step
+            if best is None or mem < best[0]:
+                best = (mem, k)
+            if k * step > best[0]:
+                break
+        return best[1]
+    k = int(checkpoint)
+    if k < 1:
+        raise ValueError("checkpoint interval must be >= 1")
+    return min(k, nt)
+
+
 class Solve:
     """One planned forward/adjoint solve: geometry, plan and workspace."""
 
     def __init__(self, device, setup: SolveSetup, tuning: Optional[dict] = None, tv: bool = True,
-                 tv_weight: float = 0.01, adjoint: str = "reference"):
+                 tv_weight: float = 0.01, adjoint: str = "reference", checkpoint=None):
         if adjoint not in ("reference",):
             raise ValueError("adjoint must be 'reference'")
         self.device = torch.device(device)
@@ -60,6 +92,7 @@ class Solve:
         pml = s.profile.packed() if s.profile is not None else None
         self.plan = _native.Plan(s.nx, s.ny, s.shots, s.nt, s.th, s.dx, s.dt32,
                                  s.src.cpu().numpy(), s.rx.cpu().numpy(), s.srcw, pml, self.device, tuning)
+        self.interval = checkpoint_interval(self.plan, checkpoint)
 
     def materials(self, er, se, mr):
         s = self.setup
@@ -70,6 +103,10 @@ class Solve:
         s = self.setup
         er32, se32, mr32 = self.materials(er, se, mr)
         traces = torch.empty((s.shots, s.nt, self.plan.nrx), dtype=torch.float32, device=self.device)
+        if keep_history and self.interval is not None:
+            ck = self.plan.new_checkpoints(self.interval)
+            self.plan.forward_checkpointed(er32, se32, mr32, traces, ck, self.interval)
+            return traces, Checkpoints(ck, self.interval)
         hist = self.plan.new_hist() if keep_history else None
         self.plan.forward(er32, se32, mr32, traces, hist)
         return traces, hist
@@ -82,7 +119,12 @@ class Solve:
             raise ValueError("residual shape %s != (%d, %d, %d)" % (tuple(resid.shape), s.shots, s.nt, self.plan.nrx))
         ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device) if need_eps else None
         gs = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device) if need_sig else None
-        self.plan.adjoint_reference(er32, se32, mr32, hist, resid, ge, gs, normalize=normalize)
+        if isinstance(hist, Checkpoints):
+            seg = self.plan.new_segment(hist.interval)
+            self.plan.adjoint_reference_checkpointed(er32, se32, mr32, hist.buf, hist.interval, seg, resid, ge, gs,
+                                                     normalize=normalize)
+        else:
+            self.plan.adjoint_reference(er32, se32, mr32, hist, resid, ge, gs, normalize=normalize)
         return ge, gs
 
 
@@ -132,12 +174,16 @@ def compute(device, dx, ny, nx, nz, source, source_apmlitudes, step, er, se, mr,
             receiver_location=None, receiver_step=None, pmlthick=0, freq=None,
             dt=None, pml_formulation='HORIPML', total_step=None, tv=True,
             Fixedreceiver=False, nseg=None, customsource=None, customreceiver=None,
-            adjoint='reference', tv_weight=0.01, tuning=None):
+            adjoint='reference', tv_weight=0.01, tuning=None, checkpoint=None):
     """Forward-model GPR traces; differentiable w.r.t. ``er`` and ``se``.
 
     Arguments and return value as the reference's compute() (src/compute.py:33-50).
     ``nseg`` (the reference's history-segmenting switch) does not change the
-    result and is accepted for compatibility.
+    result and is accepted for compatibility.  ``checkpoint`` (not in the
+    reference): None keeps the whole Ez history for the gradient, as the
+    reference does; an int K keeps the solver state every K steps instead and
+    recomputes the history segment by segment during the backward pass (one
+    extra forward solve, same results bit for bit); True picks K.
     """
     if pml_formulation != 'HORIPML':
         raise ValueError("only the HORIPML formulation is implemented (as in the reference)")
@@ -150,6 +196,6 @@ def compute(device, dx, ny, nx, nz, source, source_apmlitudes, step, er, se, mr,
     # (compute.py:825-826); the call is kept for its argument checking.
     if freq is not None and freq != source_apmlitudes[2]:
         apply_filter(torch.from_numpy(setup.srcw[0].copy()), 1 / dt, freq)
-    solve = Solve(device, setup, tuning=tuning, tv=tv, tv_weight=tv_weight, adjoint=adjoint)
+    solve = Solve(device, setup, tuning=tuning, tv=tv, tv_weight=tv_weight, adjoint=adjoint, checkpoint=checkpoint)
     traces = GPRFWI.apply(solve, er, se, mr)
     return traces, setup.dt

@@ -15,6 +15,7 @@
 #include "fdtd_lanes.cuh"
 #include "fdtd_tile.cuh"
 #include "tv.cuh"
+#include "fdtd_pairs.cuh"
 
 using fg::Dev;
 using fg::Ev;
@@ -50,7 +51,8 @@ struct fg_plan {
     std::vector<float> srcw, pml;
     // launch shape
     int kernel;         // 0 = tensor-map tiles, 1 = lane march
-    bool shot;          // shot lanes (CS = 32) or column lanes (CS = 1)
+    bool shot;          // shot lanes (CS = 32 or, with pair, 64) or column lanes (CS = 1)
+    bool pair = false;  // two shots per lane (CS = 64, lane march only)
     int W, TI, WPB, D;  // cells per thread, rows per tile, warps per block, ring stages (0 = direct loads)
     // tensor maps of the tile kernels (encoded when a workspace is bound)
     CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
@@ -67,6 +69,10 @@ struct fg_plan {
     int fwd_blocks = 0, adj_blocks = 0;
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
     float dinv = 0.f;
+    // the adjoint's own plan (own state, coefficients, accumulators and launch
+    // shape); its workspace follows this plan's in the caller's workspace
+    fg_plan* adj = nullptr;
+    ~fg_plan() { delete adj; }
     long long plane, pxs, pys;
     size_t state_bytes, psi_bytes;
     char* ws = nullptr;
@@ -87,8 +93,8 @@ int classify(const fg_plan* p, int i, int j, int k) {
 }
 
 void build_tiles(fg_plan* p) {
-    p->SL = p->shot ? 32 : 1;
-    p->CS = p->shot ? 32 : 1;
+    p->SL = p->pair ? 64 : (p->shot ? 32 : 1);
+    p->CS = p->SL;
     p->BW = p->shot ? p->W : 32 * p->W;
     p->nb = (p->ny + p->BW - 1) / p->BW;
     // PADC leading zero columns, then columns up to nb*BW + 3 (halo column and
@@ -354,6 +360,33 @@ AdjFn pick_adj_w(int W) {
 }
 AdjFn pick_adj(bool shot, int W) { return shot ? pick_adj_w<true>(W) : pick_adj_w<false>(W); }
 
+template <int W>
+cudaError_t launch_fwd2(const Dev& g, int t, int, int, int* blocks, cudaStream_t st) {
+    const size_t smem = fg::prof_bytes(g.th);
+    auto kernel = fg::k_fwd2<W>;
+    if (*blocks == 0) {
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e == cudaSuccess) e = persistent_blocks(kernel, 4, smem, g.ntiles, blocks);
+        if (e != cudaSuccess) return e;
+    }
+    kernel<<<*blocks, 128, smem, st>>>(g, t);
+    return cudaSuccess;
+}
+template <int W>
+cudaError_t launch_adj2(const Dev& g, int it, int rp, int, int, int* blocks, cudaStream_t st) {
+    const size_t smem = fg::prof_bytes(g.th);
+    auto kernel = fg::k_adj2<W>;
+    if (*blocks == 0) {
+        cudaError_t e = allow_smem(kernel, smem);
+        if (e == cudaSuccess) e = persistent_blocks(kernel, 4, smem, g.ntiles, blocks);
+        if (e != cudaSuccess) return e;
+    }
+    kernel<<<*blocks, 128, smem, st>>>(g, it, rp);
+    return cudaSuccess;
+}
+FwdFn pick_fwd2(int W) { return W == 2 ? launch_fwd2<2> : W == 4 ? launch_fwd2<4> : nullptr; }
+AdjFn pick_adj2(int W) { return W == 2 ? launch_adj2<2> : W == 4 ? launch_adj2<4> : nullptr; }
+
 // Shared memory of the larger (adjoint) ring, or 0 for direct loads.
 size_t plan_ring_smem(const fg_plan* p) {
     if (p->D == 0) return 0;
@@ -460,9 +493,9 @@ int encode_tile_maps(fg_plan* p) {
 
 // Box over the Ez history: W (shot lanes, all 32 slots) or BW (column lanes)
 // columns of R rows of one (step, group).
-int encode_hist_map(const fg_plan* p, CUtensorMap* m, const float* hist) {
+int encode_hist_map(const fg_plan* p, CUtensorMap* m, const float* hist, int nsteps) {
     const uint64_t f4 = sizeof(float);
-    const uint64_t steps = (uint64_t)p->nt * p->ngroups;
+    const uint64_t steps = (uint64_t)nsteps * p->ngroups;
     if (p->shot) {
         const uint64_t dims[4] = {32, (uint64_t)p->Ph, (uint64_t)p->nx, steps};
         const uint64_t st[3] = {32 * f4, (uint64_t)p->Ph * 32 * f4, (uint64_t)p->nx * p->Ph * 32 * f4};
@@ -646,16 +679,25 @@ int fg_total_variation(const float* data, int32_t M, int32_t N, double lamda, do
 int fg_plan_check(fg_plan* p, void* stream) {
     if (!p || !p->ws) return fail(FG_ERR_INVALID, "fg_plan_check: plan has no workspace");
     cudaStream_t st = (cudaStream_t)stream;
-    int code = 0;
-    FG_CUDA(cudaMemcpyAsync(&code, p->ws + p->o_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    fg_plan* plans[2] = {p, p->adj};
+    int code[2] = {0, 0};
+    for (int k = 0; k < 2; ++k)
+        if (plans[k] && plans[k]->ws)
+            FG_CUDA(cudaMemcpyAsync(&code[k], plans[k]->ws + plans[k]->o_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
-    if (code == 0) return FG_OK;
-    FG_CUDA(cudaMemsetAsync(p->ws + p->o_err, 0, sizeof(int), st));
-    if (code == 100) return fail(FG_ERR_INVALID, "device: out-of-range access caught by the checked build");
-    return fail(FG_ERR_TIMEOUT, "device: bounded wait gave up (code " + std::to_string(code) + ")");
+    int c = 0;
+    for (int k = 0; k < 2; ++k)
+        if (code[k]) {
+            FG_CUDA(cudaMemsetAsync(plans[k]->ws + plans[k]->o_err, 0, sizeof(int), st));
+            if (!c) c = code[k];
+        }
+    if (c == 0) return FG_OK;
+    if (c == 100) return fail(FG_ERR_INVALID, "device: out-of-range access caught by the checked build");
+    return fail(FG_ERR_TIMEOUT, "device: bounded wait gave up (code " + std::to_string(c) + ")");
 }
 
-int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out) {
+// One plan: the problem's tables and one launch shape.
+static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** out) {
     if (!prob || !out) return fail(FG_ERR_INVALID, "fg_plan_create: NULL argument");
     *out = nullptr;
     const fg_problem& q = *prob;
@@ -684,11 +726,12 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             return fail(FG_ERR_INVALID, "receiver position outside the grid");
         }
     const int lanes = tune ? tune->lanes : 0;
-    if (lanes < 0 || lanes > 2) {
+    if (lanes < 0 || lanes > 3) {
         delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning: lanes must be 0, 1 or 2");
+        return fail(FG_ERR_INVALID, "unsupported tuning: lanes must be 0, 1, 2 or 3");
     }
-    p->shot = lanes == 1 || (lanes == 0 && q.shots >= 8);
+    p->pair = lanes == 3;
+    p->shot = p->pair || lanes == 1 || (lanes == 0 && q.shots >= 8);
     // defaults: the fastest measured shapes on the 440 x 340 benchmark grid --
     // lane march (4 cells x 4 rows) for shot lanes, tile pipeline (2 cells x 4
     // rows) for column lanes
@@ -702,6 +745,10 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 4;
     p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : (p->kernel == 0 ? std::min(p->TI, 4) : 4);
     p->D = tune ? tune->stages : 0;
+    if (p->kernel == 0 && p->pair) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: shot pairs (lanes 3) take the lane march (kernel 1)");
+    }
     if (p->kernel == 0) {
         if (p->D == 0) p->D = 3;   // pipeline stages of the tile kernels
         const bool okw = p->shot ? (p->W == 4 || p->W == 8) : (p->W == 2 || p->W == 4);
@@ -718,6 +765,11 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
             delete p;
             return fail(FG_ERR_INVALID, "unsupported tuning: cells_per_thread 2/4/8, rows_per_tile >= 1, "
                                         "warps_per_block 1/2/4, stages 0 or 2..8");
+        }
+        if (p->pair && (p->D != 0 || p->W > 4)) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: shot pairs take the lane march with cells_per_thread 2 "
+                                        "or 4 and no stages");
         }
         // shot-lane stages copy coefficient rows from column j0-4: 16-byte aligned only for W >= 4
         if (p->D > 0 && p->shot && p->W < 4) {
@@ -739,12 +791,59 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     return FG_OK;
 }
 
+int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out) {
+    fg_plan* p = nullptr;
+    int rc = create_one(prob, tune, &p);
+    if (rc) return rc;
+    // the adjoint's launch shape: the forward's when the caller gave one and no
+    // adj_* field, else adj_* with defaults (shot lanes: tile pipeline of 8
+    // rows over 4 consumer warps, 2 stages -- the fastest measured adjoint on
+    // the 440 x 340 benchmark grid)
+    const bool tuned = tune && (tune->kernel || tune->stages || tune->rows_per_tile || tune->cells_per_thread);
+    const int ak = tune ? tune->adj_kernel : 0;
+    if (ak < 0 || ak > 2) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: adj_kernel must be 0, 1 (tiles) or 2 (lane march)");
+    }
+    fg_tuning at = {};
+    at.lanes = p->pair ? 3 : (p->shot ? 1 : 2);
+    at.cells_per_thread = p->W;
+    if (ak == 0 && (tuned || !p->shot || p->pair)) {
+        at.kernel = p->kernel;
+        at.rows_per_tile = p->TI;
+        at.warps_per_block = p->WPB;
+        at.stages = p->D;
+    } else {
+        at.kernel = ak == 2 ? 1 : 0;
+        at.rows_per_tile = tune && tune->adj_rows_per_tile ? tune->adj_rows_per_tile : (at.kernel == 0 ? 8 : 4);
+        at.warps_per_block = tune && tune->adj_warps_per_block ? tune->adj_warps_per_block
+                                                               : (at.kernel == 0 ? std::min(at.rows_per_tile, 4) : 4);
+        at.stages = tune && tune->adj_stages ? tune->adj_stages : (at.kernel == 0 ? 2 : 0);
+    }
+    fg_plan* a = nullptr;
+    rc = create_one(prob, &at, &a);
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    p->adj = a;
+    *out = p;
+    return FG_OK;
+}
+
 int fg_plan_destroy(fg_plan* plan) {
     delete plan;
     return FG_OK;
 }
 
-int64_t fg_plan_workspace_bytes(const fg_plan* plan) { return plan ? (int64_t)plan->total : -1; }
+namespace {
+size_t own_bytes(const fg_plan* p) { return align_up(p->total, 256); }
+}  // namespace
+
+int64_t fg_plan_workspace_bytes(const fg_plan* plan) {
+    if (!plan) return -1;
+    return (int64_t)(own_bytes(plan) + (plan->adj ? plan->adj->total : 0));
+}
 
 int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
     if (!p || !shape) return fail(FG_ERR_INVALID, "fg_plan_hist_shape: NULL argument");
@@ -756,7 +855,7 @@ int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
     return FG_OK;
 }
 
-int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
+static int bind_one(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     if (!p) return fail(FG_ERR_INVALID, "fg_plan_bind: NULL plan");
     if (!workspace || bytes < (int64_t)p->total) return fail(FG_ERR_WORKSPACE, "workspace missing or too small");
     if (((uintptr_t)workspace) % 256) return fail(FG_ERR_WORKSPACE, "workspace must be 256-byte aligned");
@@ -807,6 +906,15 @@ int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     return FG_OK;
 }
 
+int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
+    if (!p) return fail(FG_ERR_INVALID, "fg_plan_bind: NULL plan");
+    if (bytes < fg_plan_workspace_bytes(p)) return fail(FG_ERR_WORKSPACE, "workspace missing or too small");
+    int rc = bind_one(p, workspace, (int64_t)own_bytes(p), stream);
+    if (rc == FG_OK && p->adj)
+        rc = bind_one(p->adj, (char*)workspace + own_bytes(p), bytes - (int64_t)own_bytes(p), stream);
+    return rc;
+}
+
 int fg_coefficients(const float* er, const float* se, const float* mr, int32_t nx, int32_t ny, float dt, float dx,
                     int32_t adjoint, float* out, int32_t pitch, void* stream) {
     if (!er || !se || !mr || !out) return fail(FG_ERR_INVALID, "fg_coefficients: NULL argument");
@@ -814,13 +922,119 @@ int fg_coefficients(const float* er, const float* se, const float* mr, int32_t n
     return coefficients(er, se, mr, nx, ny, dt, dx, adjoint, out, pitch, 0, (cudaStream_t)stream);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Forward steps [t0, t1) of plan p with descriptor g.
+int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
+    if (p->kernel == 0) {
+        FwdTileFn tfn = pick_fwd_tile(p->shot, p->W);
+        if (!tfn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = t0; t < t1; ++t) FG_CUDA(tfn(p, g, t, st));
+    } else {
+        FwdFn fn = p->pair ? pick_fwd2(p->W) : pick_fwd(p->shot, p->W);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = t0; t < t1; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// Adjoint iterations it = hi, hi-1, .., lo (>= 1) of plan a; g.hist holds steps
+// from g.hist_t0 on, nsteps of them.
+int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t st) {
+    if (a->kernel == 0) {
+        AdjTileFn tfn = pick_adj_tile(a->shot, a->W);
+        if (!tfn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        CUtensorMap tmh;
+        const int rc = encode_hist_map(a, &tmh, g.hist, nsteps);
+        if (rc) return rc;
+        for (int it = hi; it >= lo; --it) FG_CUDA(tfn(a, g, tmh, it, (a->nt - 1 - it) & 1, st));
+    } else {
+        AdjFn fn = a->pair ? pick_adj2(a->W) : pick_adj(a->shot, a->W);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = hi; it >= lo; --it) FG_CUDA(fn(g, it, (a->nt - 1 - it) & 1, a->WPB, a->D, &a->adj_blocks, st));
+    }
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+// Start of an adjoint solve on plan a: Ucgeta coefficients, zero state and accumulators.
+int adj_begin(fg_plan* a, const float* er, const float* se, const float* mr, cudaStream_t st) {
+    int rc = coefficients(er, se, mr, a->nx, a->ny, a->dt, a->dx, 1, (float*)(a->ws + a->o_coef), a->P, fg::PADC, st);
+    if (rc) return rc;
+    if ((rc = reset_state(a, st))) return rc;
+    const size_t n = (size_t)a->nx * a->ny;
+    FG_CUDA(cudaMemsetAsync(a->ws + a->o_gacc, 0, (size_t)a->ngroups * 2 * n * sizeof(double), st));
+    return FG_OK;
+}
+
+// End of an adjoint solve: the last imaging term (g.hist must hold step 0),
+// the group sum, the norms and the scaled gradients.
+int adj_finish(fg_plan* a, const Dev& g, float* grad_eps, float* grad_sig, int normalize, double* norms,
+               cudaStream_t st) {
+    if (a->nt >= 2) {
+        // the adjoint Ez after the last step (it = 1) is in the buffer that launch wrote
+        const float* ez_final = g.ez[((a->nt - 2) & 1) ^ 1];
+        const long long cells = (long long)a->ngroups * a->nx * a->ny;
+        const int tb = (int)((cells + 255) / 256);
+        if (a->pair) fg::k_imaging_tail<64><<<tb, 256, 0, st>>>(g, ez_final);
+        else if (a->shot) fg::k_imaging_tail<32><<<tb, 256, 0, st>>>(g, ez_final);
+        else fg::k_imaging_tail<1><<<tb, 256, 0, st>>>(g, ez_final);
+    }
+    const size_t n = (size_t)a->nx * a->ny;
+    double* sums = (double*)(a->ws + a->o_sums);
+    double* partial = (double*)(a->ws + a->o_partial);
+    double* nrm = norms ? norms : (double*)(a->ws + a->o_norms);
+    fg::k_grad_sum<<<kRedBlocks, 256, 0, st>>>(g.gacc, a->ngroups, (long long)n, sums, partial);
+    fg::k_grad_norm<<<1, 32, 0, st>>>(partial, kRedBlocks, nrm);
+    const int blocks = (int)((n + 255) / 256);
+    fg::k_grad_scale<<<blocks, 256, 0, st>>>(sums, nrm, (long long)n, normalize, grad_eps, grad_sig);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
+size_t hist_step_floats(const fg_plan* p) { return (size_t)p->ngroups * p->nx * p->Ph * p->CS; }
+
+// One checkpoint: the state of one parity (Ez, Hx, Hy of every group, then
+// the four CPML auxiliary arrays).
+size_t checkpoint_floats(const fg_plan* p) {
+    return 3 * (size_t)p->ngroups * p->plane + 2 * (size_t)p->ngroups * (p->pxs + p->pys);
+}
+
+// Copy the state of parity `par` to (save) or from (restore) a checkpoint.
+int checkpoint_copy(fg_plan* p, int par, float* ck, bool save, cudaStream_t st) {
+    const Dev& g = p->g;
+    const size_t fp = (size_t)p->ngroups * p->plane, fx = (size_t)p->ngroups * p->pxs, fy = (size_t)p->ngroups * p->pys;
+    float* parts[7] = {g.ez[par], g.hx[par], g.hy[par], g.pex[par], g.phx[par], g.pey[par], g.phy[par]};
+    const size_t len[7] = {fp, fp, fp, fx, fx, fy, fy};
+    for (int k = 0; k < 7; ++k) {
+        if (len[k] == 0) continue;
+        if (save) FG_CUDA(cudaMemcpyAsync(ck, parts[k], len[k] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        else FG_CUDA(cudaMemcpyAsync(parts[k], ck, len[k] * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        ck += len[k];
+    }
+    return FG_OK;
+}
+
+int checkpoint_args(const fg_plan* p, int interval, int64_t bytes, const void* ck, const char* who) {
+    if (interval < 1) return fail(FG_ERR_INVALID, std::string(who) + ": interval must be >= 1");
+    const int64_t need = fg_plan_checkpoint_bytes(p, interval);
+    if (need > 0 && (!ck || bytes < need))
+        return fail(FG_ERR_WORKSPACE, std::string(who) + ": checkpoint buffer missing or too small");
+    if (((uintptr_t)ck) % 16) return fail(FG_ERR_INVALID, std::string(who) + ": checkpoint buffer not 16-byte aligned");
+    return FG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, float* traces, float* hist,
                void* stream) {
     if (!p || !er || !se || !mr || (!traces && p->nrx > 0)) return fail(FG_ERR_INVALID, "fg_forward: NULL argument");
     if (!p->ws) return fail(FG_ERR_WORKSPACE, "fg_forward: plan has no workspace");
-    FwdFn fn = pick_fwd(p->shot, p->W);
-    FwdTileFn tfn = pick_fwd_tile(p->shot, p->W);
-    if ((p->kernel == 1 && !fn) || (p->kernel == 0 && !tfn)) return fail(FG_ERR_INVALID, "no kernel for this tuning");
     cudaStream_t st = (cudaStream_t)stream;
     int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st);
     if (rc) return rc;
@@ -831,15 +1045,9 @@ int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, fl
     g.hist = hist;
     if (hist) {
         g.out_lo = (const char*)hist;
-        g.out_hi = (const char*)(hist + (size_t)p->nt * p->ngroups * p->nx * p->Ph * p->CS);
+        g.out_hi = (const char*)(hist + (size_t)p->nt * hist_step_floats(p));
     }
-    if (p->kernel == 0) {
-        for (int t = 0; t < p->nt; ++t) FG_CUDA(tfn(p, g, t, st));
-    } else {
-        for (int t = 0; t < p->nt; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
-    }
-    FG_CUDA(cudaGetLastError());
-    return FG_OK;
+    return fwd_steps(p, g, 0, p->nt, st);
 }
 
 int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
@@ -847,49 +1055,94 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
                          void* stream) {
     if (!p || !er || !se || !mr || !hist || (!resid && p->nrx > 0))
         return fail(FG_ERR_INVALID, "fg_adjoint_reference: NULL argument");
-    if (!p->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_reference: plan has no workspace");
-    AdjFn fn = pick_adj(p->shot, p->W);
-    AdjTileFn tfn = pick_adj_tile(p->shot, p->W);
-    if ((p->kernel == 1 && !fn) || (p->kernel == 0 && !tfn)) return fail(FG_ERR_INVALID, "no kernel for this tuning");
-    CUtensorMap tmh;
-    if (p->kernel == 0) {
-        const int rc = encode_hist_map(p, &tmh, hist);
-        if (rc) return rc;
-    }
+    fg_plan* a = p->adj ? p->adj : p;
+    if (!a->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_reference: plan has no workspace");
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 1, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st);
+    int rc = adj_begin(a, er, se, mr, st);
     if (rc) return rc;
-    if ((rc = reset_state(p, st))) return rc;
-    const size_t n = (size_t)p->nx * p->ny;
-    FG_CUDA(cudaMemsetAsync(p->ws + p->o_gacc, 0, (size_t)p->ngroups * 2 * n * sizeof(double), st));
-    Dev g = p->g;
+    Dev g = a->g;
     g.hist = const_cast<float*>(hist);
     g.out_lo = (const char*)hist;
-    g.out_hi = (const char*)(hist + (size_t)p->nt * p->ngroups * p->nx * p->Ph * p->CS);
+    g.out_hi = (const char*)(hist + (size_t)a->nt * hist_step_floats(a));
     g.resid = resid;
-    if (p->kernel == 0) {
-        for (int it = p->nt - 1; it >= 1; --it) FG_CUDA(tfn(p, g, tmh, it, (p->nt - 1 - it) & 1, st));
-    } else {
-        for (int it = p->nt - 1; it >= 1; --it)
-            FG_CUDA(fn(g, it, (p->nt - 1 - it) & 1, p->WPB, p->D, &p->adj_blocks, st));
+    if ((rc = adj_steps(a, g, a->nt - 1, 1, a->nt, st))) return rc;
+    return adj_finish(a, g, grad_eps, grad_sig, normalize, norms, st);
+}
+
+int64_t fg_plan_checkpoint_bytes(const fg_plan* p, int32_t interval) {
+    if (!p || interval < 1) return -1;
+    const int64_t segments = (p->nt + interval - 1) / interval;
+    return (segments - 1) * (int64_t)(checkpoint_floats(p) * sizeof(float));
+}
+
+int fg_forward_checkpointed(fg_plan* p, const float* er, const float* se, const float* mr, float* traces, void* ckpt,
+                            int64_t ckpt_bytes, int32_t interval, void* stream) {
+    if (!p || !er || !se || !mr || (!traces && p->nrx > 0))
+        return fail(FG_ERR_INVALID, "fg_forward_checkpointed: NULL argument");
+    if (!p->ws) return fail(FG_ERR_WORKSPACE, "fg_forward_checkpointed: plan has no workspace");
+    int rc = checkpoint_args(p, interval, ckpt_bytes, ckpt, "fg_forward_checkpointed");
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st)))
+        return rc;
+    if ((rc = reset_state(p, st))) return rc;
+    if (p->nrx > 0) FG_CUDA(cudaMemsetAsync(traces, 0, (size_t)p->S * p->nt * p->nrx * sizeof(float), st));
+    Dev g = p->g;
+    g.traces = traces;
+    const size_t cf = checkpoint_floats(p);
+    for (int s0 = 0; s0 < p->nt; s0 += interval) {
+        // checkpoint c >= 1 holds the state at the start of step c * interval
+        if (s0 > 0 && (rc = checkpoint_copy(p, s0 & 1, (float*)ckpt + (size_t)(s0 / interval - 1) * cf, true, st)))
+            return rc;
+        if ((rc = fwd_steps(p, g, s0, std::min(s0 + interval, p->nt), st))) return rc;
     }
-    if (p->nt >= 2) {
-        // the adjoint Ez after the last step (it = 1) is in the buffer that launch wrote
-        const float* ez_final = g.ez[((p->nt - 2) & 1) ^ 1];
-        const long long cells = (long long)p->ngroups * p->nx * p->ny;
-        const int tb = (int)((cells + 255) / 256);
-        if (p->shot) fg::k_imaging_tail<32><<<tb, 256, 0, st>>>(g, ez_final);
-        else fg::k_imaging_tail<1><<<tb, 256, 0, st>>>(g, ez_final);
-    }
-    double* sums = (double*)(p->ws + p->o_sums);
-    double* partial = (double*)(p->ws + p->o_partial);
-    double* nrm = norms ? norms : (double*)(p->ws + p->o_norms);
-    fg::k_grad_sum<<<kRedBlocks, 256, 0, st>>>(g.gacc, p->ngroups, (long long)n, sums, partial);
-    fg::k_grad_norm<<<1, 32, 0, st>>>(partial, kRedBlocks, nrm);
-    const int blocks = (int)((n + 255) / 256);
-    fg::k_grad_scale<<<blocks, 256, 0, st>>>(sums, nrm, (long long)n, normalize, grad_eps, grad_sig);
-    FG_CUDA(cudaGetLastError());
     return FG_OK;
+}
+
+int fg_adjoint_reference_checkpointed(fg_plan* p, const float* er, const float* se, const float* mr, const void* ckpt,
+                                      int64_t ckpt_bytes, int32_t interval, float* segment, const float* resid,
+                                      float* grad_eps, float* grad_sig, int32_t normalize, double* norms,
+                                      void* stream) {
+    if (!p || !er || !se || !mr || !segment || (!resid && p->nrx > 0))
+        return fail(FG_ERR_INVALID, "fg_adjoint_reference_checkpointed: NULL argument");
+    if (!p->adj) return fail(FG_ERR_INVALID, "fg_adjoint_reference_checkpointed: plan without an adjoint plan");
+    fg_plan* a = p->adj;
+    if (!p->ws || !a->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_reference_checkpointed: plan has no workspace");
+    int rc = checkpoint_args(p, interval, ckpt_bytes, ckpt, "fg_adjoint_reference_checkpointed");
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    // forward recompute on this plan (Ucget coefficients), adjoint on its adjoint plan
+    if ((rc = coefficients(er, se, mr, p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P, fg::PADC, st)))
+        return rc;
+    if ((rc = adj_begin(a, er, se, mr, st))) return rc;
+    const size_t cf = checkpoint_floats(p), hs = hist_step_floats(p);
+    Dev gf = p->g;
+    gf.traces = nullptr;
+    gf.hist = segment;
+    gf.out_lo = (const char*)segment;
+    gf.out_hi = (const char*)(segment + (size_t)interval * hs);
+    Dev ga = a->g;
+    ga.hist = segment;
+    ga.out_lo = gf.out_lo;
+    ga.out_hi = gf.out_hi;
+    ga.resid = resid;
+    const int segments = (p->nt + interval - 1) / interval;
+    for (int c = segments - 1; c >= 0; --c) {
+        const int s0 = c * interval, s1 = std::min(s0 + interval, p->nt);
+        // the forward state at the start of step s0, then its history over [s0, s1)
+        if (c == 0) {
+            if ((rc = reset_state(p, st))) return rc;
+        } else {
+            if ((rc = checkpoint_copy(p, s0 & 1, (float*)ckpt + (size_t)(c - 1) * cf, false, st))) return rc;
+            FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 2 * sizeof(int), st));
+        }
+        gf.hist_t0 = s0;
+        if ((rc = fwd_steps(p, gf, s0, s1, st))) return rc;
+        ga.hist_t0 = s0;
+        const int lo = std::max(s0, 1);
+        if (s1 - 1 >= lo && (rc = adj_steps(a, ga, s1 - 1, lo, s1 - s0, st))) return rc;
+    }
+    return adj_finish(a, ga, grad_eps, grad_sig, normalize, norms, st);
 }
 
 int fg_forward_static(fg_plan* p, const float* er, const float* se, const float* mr, float* traces, float* hist,
@@ -904,7 +1157,7 @@ int fg_forward_static(fg_plan* p, const float* er, const float* se, const float*
     if (rc) return rc;
     char* saved = p->ws;
     const int64_t saved_bytes = p->ws_bytes;
-    rc = fg_plan_bind(p, scratch, (int64_t)FG_STATIC_SCRATCH_BYTES, stream);
+    rc = bind_one(p, scratch, (int64_t)FG_STATIC_SCRATCH_BYTES, stream);
     if (rc == FG_OK) rc = fg_forward(p, er, se, mr, traces, hist, stream);
     p->ws = saved;
     p->ws_bytes = saved_bytes;

@@ -72,7 +72,8 @@ struct Dev {
     const float* srcw;   // (nsrc, nt)
     // solve I/O
     float* traces;       // (S, nt, nrx)
-    float* hist;         // (nt, ngroups, nx, Ph, CS)
+    float* hist;         // (steps, ngroups, nx, Ph, CS): step t at index t - hist_t0
+    int hist_t0;         // first step the history buffer holds (0 = the whole run)
     const float* resid;  // (S, nt, nrx)
     double* gacc;        // (ngroups, 2, nx, ny)
     // bounds of every buffer the kernels touch (checked builds)

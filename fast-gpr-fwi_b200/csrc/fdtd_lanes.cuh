@@ -207,7 +207,7 @@ __device__ __forceinline__ TileQ tile_q(const Dev& g, int pos, int it) {
     q.sbase = (long long)T.grp * g.plane + (long long)(c0s + PADC) * CS;
     q.cbase = T.b0 - 4 + PADC;
     const long long hrow = (long long)g.Ph * CS;
-    q.hbase = ((long long)it * g.ngroups + T.grp) * g.nx * hrow + (long long)T.b0 * CS;
+    q.hbase = ((long long)(it - g.hist_t0) * g.ngroups + T.grp) * g.nx * hrow + (long long)T.b0 * CS;
     // history cells of the band that exist in a history row
     const int hcells = SHOT ? W : max(0, min(32 * W, g.Ph - T.b0));
     q.hs = (uint32_t)hcells * CS * 4;
@@ -258,8 +258,7 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
                                madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
-            fwd_row_cpml_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn,
-                                 ezn);
+            fwd_row_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn, ezn);
     } else if (g.fast_cpml) {
         float dzx[W + 1], dzy[W], dhy[W], dhx[W];
 #pragma unroll
@@ -332,7 +331,7 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
         if (e.y != slot || t + 1 >= g.nt) continue;
 #pragma unroll
         for (int w = 0; w < W; ++w)
-            if (j0 + w == e.z) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezn[w];
+            if (j0 + w == e.z && g.traces) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezn[w];
     }
 #pragma unroll
     for (int k = 0; k < W + 2; ++k) ezc[k] = B.en[k];
@@ -438,7 +437,7 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
         const int se = __ldg(g.src_off + T.id + 1);
         int rc = __ldg(g.rx_off + T.id);
         const int re = __ldg(g.rx_off + T.id + 1);
-        float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + T.grp) * g.nx) * hrow + (long long)j0 * CS + l
+        float* hist = g.hist ? g.hist + (((long long)(t - g.hist_t0) * g.ngroups + T.grp) * g.nx) * hrow + (long long)j0 * CS + l
                              : nullptr;
         // Ez_old of row i0, columns j0-1 .. j0+W, and the new Hy of the row
         // above the chunk (its auxiliaries are only read)
@@ -601,7 +600,7 @@ __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const Ba
                                madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
-            adj_e_row_cpml_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
+            adj_e_row_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
     } else if (g.fast_cpml) {
         float dhy[W + 1], dhx[W + 1];
 #pragma unroll
@@ -757,7 +756,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
         int ic = __ldg(g.inj_off + T.id);
         const int ie = __ldg(g.inj_off + T.id + 1);
         const float* resid_s = g.resid + ((long long)T.s * g.nt + it) * g.nrx;
-        const float* f1g = g.hist + ((long long)it * g.ngroups + T.grp) * nx * hrow + (long long)j0 * CS + l;
+        const float* f1g = g.hist + ((long long)(it - g.hist_t0) * g.ngroups + T.grp) * nx * hrow + (long long)j0 * CS + l;
         double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
         double* gas = gae + (long long)nx * ny;
         const bool hist_ok = j0 < g.Ph;
@@ -877,7 +876,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
                     dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
                     dzy[w] = __fsub_rn(ezr[w], ezc[w]);
                 }
-                if constexpr (SHOT) adj_h_row_cpml_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+                if constexpr (SHOT) adj_h_row_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
             } else if (g.fast_cpml) {
                 float dzx[W], dzy[W];
 #pragma unroll
@@ -969,7 +968,7 @@ __global__ void k_imaging_tail(const Dev g, const float* __restrict__ ez_final) 
     const int grp = (int)(idx / n);
     const long long c = idx % n;
     const int i = (int)(c / g.ny), j = (int)(c % g.ny);
-    const float* f0 = g.hist + (((long long)grp * g.nx + i) * g.Ph + j) * CS;
+    const float* f0 = g.hist + ((((long long)(0 - g.hist_t0) * g.ngroups + grp) * g.nx + i) * g.Ph + j) * CS;
     const float* lam = ez_final + (long long)grp * g.plane + ((long long)i * g.P + j + PADC) * CS;
     float acc = 0.f;
 #pragma unroll 8

@@ -83,19 +83,9 @@ __device__ __forceinline__ XRow x_row(const Dev& g, int i, bool efield) {
 // y-slab geometry of a band: the H run and the E run of its rows.
 //   forward: Hx at j0-1 .. j0+W-1 (W+1 cells), Hy and E at j0 .. j0+W-1
 //   adjoint: E at j0 .. j0+W (W+1 cells), Hx and Hy at j0 .. j0+W-1
-//   xonly: no cell of either run is in a y slab, every cell is in the grid
-//          and j0 >= 1 (x-slab rows take the straight-line x path)
-//   yside: 1 (y0) or 2 (ymax) when every cell of the band's own columns
-//          j0 .. j0+W-1 is in that y slab for both updates (y-slab bands take
-//          the straight-line y path); the one extra cell of a run (the H halo
-//          column j0-1 forward, the E halo column j0+W adjoint) is described
-//          by xin (in the grid) and xslab (in the same slab)
 struct BandY {
     YRun h, e;
     bool lean;   // the shot-lane CPML rows apply (fast_cpml and one-sided runs)
-    bool xonly;
-    int yside;
-    bool xin, xslab;
 };
 __device__ __forceinline__ uint32_t low_bits(int n) { return n >= 32 ? 0xffffffffu : ((1u << n) - 1u); }
 template <int W>
@@ -104,12 +94,6 @@ __device__ __forceinline__ BandY band_fwd(const Dev& g, int j0) {
     b.h = y_run<W + 1>(g, j0 - 1, false);
     b.e = y_run<W>(g, j0, true);
     b.lean = g.fast_cpml && b.h.one_side && b.e.one_side;
-    const uint32_t fw = low_bits(W), fh = low_bits(W + 1);
-    b.xonly = b.lean && b.h.m == 0 && b.e.m == 0 && b.h.in == fh && b.e.in == fw && j0 >= 1;
-    const bool yfull = b.lean && b.e.m == fw && (b.h.m >> 1) == fw && b.h.off == b.e.off;
-    b.yside = yfull ? (b.e.off == 0 ? 1 : 2) : 0;
-    b.xin = b.h.in & 1u;
-    b.xslab = b.h.m & 1u;
     return b;
 }
 template <int W>
@@ -118,12 +102,6 @@ __device__ __forceinline__ BandY band_adj(const Dev& g, int j0) {
     b.h = y_run<W>(g, j0, false);
     b.e = y_run<W + 1>(g, j0, true);
     b.lean = g.fast_cpml && b.h.one_side && b.e.one_side;
-    const uint32_t fw = low_bits(W), fe = low_bits(W + 1);
-    b.xonly = b.lean && b.h.m == 0 && b.e.m == 0 && b.h.in == fw && b.e.in == fe && j0 >= 1;
-    const bool yfull = b.lean && (b.e.m & fw) == fw && b.h.m == fw && b.h.off == b.e.off;
-    b.yside = yfull ? (b.e.off == 0 ? 1 : 2) : 0;
-    b.xin = (b.e.in >> W) & 1u;
-    b.xslab = (b.e.m >> W) & 1u;
     return b;
 }
 
@@ -365,309 +343,6 @@ __device__ __forceinline__ void adj_h_row_shot(const Dev& g, const float* R, con
     hy_shot<W>(g, R, j0, xh, in, hy, dzy, ch, ci, px);
     st_yrun<W>(g, wr.hy, i, by.h, ~0u, lane, py);
     if (xh.on) st_xrun<W>(g, wr.hx, xh.r, j0, in, lane, px);
-}
-
-// ---------------------------------------------------------------------------
-// Straight-line rows.  The masked rows above take any band; the rows below
-// take the common CPML cases without per-cell tests: an x-slab row of a band
-// with no y-slab cell, and a row outside the x slabs of a band whose own
-// columns all lie in one y slab (slab column k = k0 + DK n, DK = -1 in the y0
-// slab and +1 in the ymax slab, a compile-time step).  Same arithmetic, same
-// order, same stores.
-// ---------------------------------------------------------------------------
-
-// Profile vectors at index k: RA - 1, RB, RE, RF.
-struct Prof {
-    float a1, b, e, f;
-};
-__device__ __forceinline__ Prof prof_at(const float* R, int th, int k) {
-    Prof q;
-    q.a1 = __fsub_rn(R[k], 1.0f);
-    q.b = R[th + k];
-    q.e = R[2 * th + k];
-    q.f = R[3 * th + k];
-    return q;
-}
-// F + s u4 ((RA-1) dd + RB psi), psi <- RE psi - RF dd  (s = +1 when PLUS)
-template <bool PLUS>
-__device__ __forceinline__ float corr(float f, float dd, float u4, float& psi, const Prof& q) {
-    const float out = __fmaf_rn(PLUS ? u4 : -u4, madd2(q.a1, dd, q.b, psi), f);
-    psi = msub2(q.e, psi, q.f, dd);
-    return out;
-}
-
-// Whether row i lies in an x slab of the E update or of the H update.
-__device__ __forceinline__ bool x_slab_row(const Dev& g, int i) {
-    return g.th > 0 && (i <= g.th || i >= g.nx - g.th);
-}
-
-// Forward, x-slab row of a band with no y-slab cell (BandY::xonly).
-template <int W>
-__device__ __forceinline__ void fwd_row_shot_x(const Dev& g, const float* R, int i, int j0, int lane,
-                                               const float (&hxo)[W + 1], const float (&hyo)[W],
-                                               const float (&en)[W + 2], const float (&ezc)[W + 2],
-                                               const float (&hyu)[W], const float* ca, const float* cb,
-                                               const float* ch, const PsiG& rd, const PsiG& wr, float (&hxn)[W + 1],
-                                               float (&hyn)[W], float (&ezn)[W]) {
-    const int th = g.th;
-    const XRow xh = x_row(g, i, false), xe = x_row(g, i, true);
-    const long long crow = coef_at(g, i, j0);
-    const long long oh = ((long long)xh.r * g.P + j0) * 32 + lane, oe = ((long long)xe.r * g.P + j0) * 32 + lane;
-    float ci[W], cd[W], pxh[W], pxe[W];
-#pragma unroll
-    for (int n = 0; n < W; ++n) ci[n] = cd[n] = pxh[n] = pxe[n] = 0.f;
-    if (xh.on) {
-        ld_coef<W, CALIGN<W>>(g, ci, g.ci + crow);
-#pragma unroll
-        for (int n = 0; n < W; ++n) pxh[n] = ldro(g, rd.hx + oh + n * 32);
-    }
-    if (xe.on) {
-        ld_coef<W, CALIGN<W>>(g, cd, g.cd + crow);
-#pragma unroll
-        for (int n = 0; n < W; ++n) pxe[n] = ldro(g, rd.ex + oe + n * 32);
-    }
-#pragma unroll
-    for (int n = 0; n <= W; ++n) {
-        const float dz = __fsub_rn(ezc[n + 1], ezc[n]);
-        hxn[n] = i >= 1 ? msub2(1.0f, hxo[n], ch[n], dz) : hxo[n];
-    }
-    if (xh.on) {
-        const Prof q = prof_at(R + 4 * th, th, xh.k);
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            const float dz = __fsub_rn(en[w + 1], ezc[w + 1]);
-            hyn[w] = corr<true>(madd2(1.0f, hyo[w], ch[w + 1], dz), div_d(g, dz), ci[w], pxh[w], q);
-        }
-#pragma unroll
-        for (int n = 0; n < W; ++n) st1(g, wr.hx + oh + n * 32, pxh[n]);
-    } else {
-#pragma unroll
-        for (int w = 0; w < W; ++w) hyn[w] = madd2(1.0f, hyo[w], ch[w + 1], __fsub_rn(en[w + 1], ezc[w + 1]));
-    }
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-        const float dhy = __fsub_rn(hyn[w], hyu[w]), dhx = __fsub_rn(hxn[w + 1], hxn[w]);
-        float e = ezc[w + 1];
-        if (i >= 1) e = __fmaf_rn(-cb[w], dhx, madd2(ca[w], e, cb[w], dhy));
-        ezn[w] = e;
-    }
-    if (xe.on) {
-        const Prof q = prof_at(R, th, xe.k);
-#pragma unroll
-        for (int w = 0; w < W; ++w) ezn[w] = corr<true>(ezn[w], div_d(g, __fsub_rn(hyn[w], hyu[w])), cd[w], pxe[w], q);
-#pragma unroll
-        for (int n = 0; n < W; ++n) st1(g, wr.ex + oe + n * 32, pxe[n]);
-    }
-}
-
-// Forward, row outside the x slabs of a band inside one y slab (BandY::yside).
-template <int W, bool YM>
-__device__ __forceinline__ void fwd_row_shot_y(const Dev& g, const float* R, const BandY& by, int i, int j0, int lane,
-                                               const float (&hxo)[W + 1], const float (&hyo)[W],
-                                               const float (&en)[W + 2], const float (&ezc)[W + 2],
-                                               const float (&hyu)[W], const float* ca, const float* cb,
-                                               const float* ch, const PsiG& rd, const PsiG& wr, float (&hxn)[W + 1],
-                                               float (&hyn)[W], float (&ezn)[W]) {
-    constexpr int DK = YM ? 32 : -32;
-    const int th = g.th;
-    const float* HR = R + 4 * th;
-    const long long crow = coef_at(g, i, j0);
-    const long long oh = ((long long)(i + by.h.off) * g.TY + by.h.k0) * 32 + lane;   // H run cell 0 (column j0-1)
-    const long long oe = ((long long)(i + by.e.off) * g.TY + by.e.k0) * 32 + lane;   // E run cell 0 (column j0)
-    float ci[W + 1], cd[W], pyh[W + 1], pye[W];
-    ld_coef<W, CALIGN<W>>(g, ci + 1, g.ci + crow);
-    ci[0] = by.xslab ? ldro(g, g.ci + crow - 1) : 0.f;
-    ld_coef<W, CALIGN<W>>(g, cd, g.cd + crow);
-    pyh[0] = by.xslab ? ldro(g, rd.hy + oh) : 0.f;
-#pragma unroll
-    for (int n = 1; n <= W; ++n) pyh[n] = ldro(g, rd.hy + oh + n * DK);
-#pragma unroll
-    for (int w = 0; w < W; ++w) pye[w] = ldro(g, rd.ey + oe + w * DK);
-    hxn[0] = hxo[0];
-    if (by.xin) {
-        const float dz = __fsub_rn(ezc[1], ezc[0]);
-        float h = msub2(1.0f, hxo[0], ch[0], dz);
-        if (by.xslab) h = corr<false>(h, div_d(g, dz), ci[0], pyh[0], prof_at(HR, th, by.h.k0));
-        hxn[0] = h;
-    }
-#pragma unroll
-    for (int n = 1; n <= W; ++n) {
-        const float dz = __fsub_rn(ezc[n + 1], ezc[n]);
-        hxn[n] = corr<false>(msub2(1.0f, hxo[n], ch[n], dz), div_d(g, dz), ci[n], pyh[n],
-                             prof_at(HR, th, by.h.k0 + (DK / 32) * n));
-    }
-#pragma unroll
-    for (int w = 0; w < W; ++w) hyn[w] = madd2(1.0f, hyo[w], ch[w + 1], __fsub_rn(en[w + 1], ezc[w + 1]));
-#pragma unroll
-    for (int w = 0; w < W; ++w) {
-        const float dhy = __fsub_rn(hyn[w], hyu[w]), dhx = __fsub_rn(hxn[w + 1], hxn[w]);
-        const float e = __fmaf_rn(-cb[w], dhx, madd2(ca[w], ezc[w + 1], cb[w], dhy));
-        ezn[w] = corr<false>(e, div_d(g, dhx), cd[w], pye[w], prof_at(R, th, by.e.k0 + (DK / 32) * w));
-    }
-#pragma unroll
-    for (int n = 1; n <= W; ++n) st1(g, wr.hy + oh + n * DK, pyh[n]);
-#pragma unroll
-    for (int w = 0; w < W; ++w) st1(g, wr.ey + oe + w * DK, pye[w]);
-}
-
-// Forward row outside the interior core: the straight-line rows where they
-// apply, else the masked row.
-template <int W>
-__device__ __forceinline__ void fwd_row_cpml_shot(const Dev& g, const float* R, const BandY& by, int i, int j0,
-                                                  int lane, const float (&hxo)[W + 1], const float (&hyo)[W],
-                                                  const float (&en)[W + 2], const float (&ezc)[W + 2],
-                                                  const float (&hyu)[W], const float* ca, const float* cb,
-                                                  const float* ch, const PsiG& rd, const PsiG& wr,
-                                                  float (&hxn)[W + 1], float (&hyn)[W], float (&ezn)[W]) {
-    if (by.xonly)
-        fwd_row_shot_x<W>(g, R, i, j0, lane, hxo, hyo, en, ezc, hyu, ca, cb, ch, rd, wr, hxn, hyn, ezn);
-    else if (by.yside == 1 && !x_slab_row(g, i))
-        fwd_row_shot_y<W, false>(g, R, by, i, j0, lane, hxo, hyo, en, ezc, hyu, ca, cb, ch, rd, wr, hxn, hyn, ezn);
-    else if (by.yside == 2 && !x_slab_row(g, i))
-        fwd_row_shot_y<W, true>(g, R, by, i, j0, lane, hxo, hyo, en, ezc, hyu, ca, cb, ch, rd, wr, hxn, hyn, ezn);
-    else
-        fwd_row_shot<W>(g, R, by, i, j0, lane, hxo, hyo, en, ezc, hyu, ca, cb, ch, rd, wr, hxn, hyn, ezn);
-}
-
-// Adjoint E row r, x-slab row of a band with no y-slab cell.
-template <int W>
-__device__ __forceinline__ void adj_e_row_shot_x(const Dev& g, const float* R, int r, int j0, int lane, bool own_row,
-                                                 const float* ez, const float* hxo, const float* hyo,
-                                                 const float* hyu, const float* ca, const float* cb, const PsiG& rd,
-                                                 const PsiG& wr, float (&out)[W + 1]) {
-    const XRow xe = x_row(g, r, true);
-    const long long oe = ((long long)xe.r * g.P + j0) * 32 + lane;
-    float cd[W + 1], px[W + 1];
-#pragma unroll
-    for (int n = 0; n <= W; ++n) cd[n] = px[n] = 0.f;
-    if (xe.on) {
-        ld_coef<W + 1, CALIGN<W>>(g, cd, g.cd + coef_at(g, r, j0));
-#pragma unroll
-        for (int n = 0; n <= W; ++n) px[n] = ldro(g, rd.ex + oe + n * 32);
-    }
-#pragma unroll
-    for (int n = 0; n <= W; ++n) {
-        float e = ez[n];
-        if (r >= 1)
-            e = __fmaf_rn(-cb[n], __fsub_rn(hxo[n + 1], hxo[n]), madd2(ca[n], e, cb[n], __fsub_rn(hyo[n], hyu[n])));
-        out[n] = e;
-    }
-    if (xe.on) {
-        const Prof q = prof_at(R, g.th, xe.k);
-#pragma unroll
-        for (int n = 0; n <= W; ++n) out[n] = corr<true>(out[n], div_d(g, __fsub_rn(hyo[n], hyu[n])), cd[n], px[n], q);
-        if (own_row) {
-#pragma unroll
-            for (int n = 0; n < W; ++n) st1(g, wr.ex + oe + n * 32, px[n]);
-        }
-    }
-}
-
-// Adjoint E row r outside the x slabs, band inside one y slab.
-template <int W, bool YM>
-__device__ __forceinline__ void adj_e_row_shot_y(const Dev& g, const float* R, const BandY& by, int r, int j0,
-                                                 int lane, bool own_row, const float* ez, const float* hxo,
-                                                 const float* hyo, const float* hyu, const float* ca, const float* cb,
-                                                 const PsiG& rd, const PsiG& wr, float (&out)[W + 1]) {
-    constexpr int DK = YM ? 32 : -32;
-    const int th = g.th;
-    const long long crow = coef_at(g, r, j0);
-    const long long oe = ((long long)(r + by.e.off) * g.TY + by.e.k0) * 32 + lane;
-    float cd[W + 1], py[W + 1];
-    ld_coef<W, CALIGN<W>>(g, cd, g.cd + crow);
-    cd[W] = by.xslab ? ldro(g, g.cd + crow + W) : 0.f;
-#pragma unroll
-    for (int n = 0; n < W; ++n) py[n] = ldro(g, rd.ey + oe + n * DK);
-    py[W] = by.xslab ? ldro(g, rd.ey + oe + W * DK) : 0.f;
-#pragma unroll
-    for (int n = 0; n < W; ++n) {
-        const float dhx = __fsub_rn(hxo[n + 1], hxo[n]);
-        const float e = __fmaf_rn(-cb[n], dhx, madd2(ca[n], ez[n], cb[n], __fsub_rn(hyo[n], hyu[n])));
-        out[n] = corr<false>(e, div_d(g, dhx), cd[n], py[n], prof_at(R, th, by.e.k0 + (DK / 32) * n));
-    }
-    out[W] = ez[W];
-    if (by.xin) {
-        const float dhx = __fsub_rn(hxo[W + 1], hxo[W]);
-        float e = __fmaf_rn(-cb[W], dhx, madd2(ca[W], ez[W], cb[W], __fsub_rn(hyo[W], hyu[W])));
-        if (by.xslab) e = corr<false>(e, div_d(g, dhx), cd[W], py[W], prof_at(R, th, by.e.k0 + (DK / 32) * W));
-        out[W] = e;
-    }
-    if (own_row) {
-#pragma unroll
-        for (int n = 0; n < W; ++n) st1(g, wr.ey + oe + n * DK, py[n]);
-    }
-}
-
-template <int W>
-__device__ __forceinline__ void adj_e_row_cpml_shot(const Dev& g, const float* R, const BandY& by, int r, int j0,
-                                                    int lane, bool own_row, const float* ez, const float* hxo,
-                                                    const float* hyo, const float* hyu, const float* ca,
-                                                    const float* cb, const PsiG& rd, const PsiG& wr,
-                                                    float (&out)[W + 1]) {
-    const bool xr = g.th > 0 && ((r >= 1 && r <= g.th) || r >= g.nx - g.th);
-    if (by.xonly)
-        adj_e_row_shot_x<W>(g, R, r, j0, lane, own_row, ez, hxo, hyo, hyu, ca, cb, rd, wr, out);
-    else if (by.yside == 1 && !xr)
-        adj_e_row_shot_y<W, false>(g, R, by, r, j0, lane, own_row, ez, hxo, hyo, hyu, ca, cb, rd, wr, out);
-    else if (by.yside == 2 && !xr)
-        adj_e_row_shot_y<W, true>(g, R, by, r, j0, lane, own_row, ez, hxo, hyo, hyu, ca, cb, rd, wr, out);
-    else
-        adj_e_row_shot<W>(g, R, by, r, j0, lane, own_row, ez, hxo, hyo, hyu, ca, cb, rd, wr, out);
-}
-
-// Adjoint H row i (cells j0 .. j0+W-1) from the new E.
-template <int W>
-__device__ __forceinline__ void adj_h_row_cpml_shot(const Dev& g, const float* R, const BandY& by, int i, int j0,
-                                                    int lane, float (&hx)[W], float (&hy)[W], const float (&dzx)[W],
-                                                    const float (&dzy)[W], const float* ch, const PsiG& rd,
-                                                    const PsiG& wr) {
-    const int th = g.th;
-    const float* HR = R + 4 * th;
-    const long long crow = coef_at(g, i, j0);
-    const bool xr = th > 0 && (i <= th - 1 || i >= g.nx - th);
-    if (by.xonly) {
-        // Hx interior only; Hy interior plus the x correction in x-slab rows
-        const XRow xh = x_row(g, i, false);
-        const long long oh = ((long long)xh.r * g.P + j0) * 32 + lane;
-        float ci[W], px[W];
-#pragma unroll
-        for (int n = 0; n < W; ++n) ci[n] = px[n] = 0.f;
-        if (xh.on) {
-            ld_coef<W, CALIGN<W>>(g, ci, g.ci + crow);
-#pragma unroll
-            for (int n = 0; n < W; ++n) px[n] = ldro(g, rd.hx + oh + n * 32);
-        }
-#pragma unroll
-        for (int n = 0; n < W; ++n) {
-            if (i >= 1) hx[n] = msub2(1.0f, hx[n], ch[n], dzx[n]);
-            hy[n] = madd2(1.0f, hy[n], ch[n], dzy[n]);
-        }
-        if (xh.on) {
-            const Prof q = prof_at(HR, th, xh.k);
-#pragma unroll
-            for (int n = 0; n < W; ++n) hy[n] = corr<true>(hy[n], div_d(g, dzy[n]), ci[n], px[n], q);
-#pragma unroll
-            for (int n = 0; n < W; ++n) st1(g, wr.hx + oh + n * 32, px[n]);
-        }
-    } else if (by.yside != 0 && !xr) {
-        // Hx interior plus the y correction for every cell; Hy interior only
-        const long long oh = ((long long)(i + by.h.off) * g.TY + by.h.k0) * 32 + lane;
-        const int dk = by.yside == 2 ? 1 : -1;
-        float ci[W], py[W];
-        ld_coef<W, CALIGN<W>>(g, ci, g.ci + crow);
-#pragma unroll
-        for (int n = 0; n < W; ++n) py[n] = ldro(g, rd.hy + oh + n * 32 * dk);
-#pragma unroll
-        for (int n = 0; n < W; ++n) {
-            hx[n] = corr<false>(msub2(1.0f, hx[n], ch[n], dzx[n]), div_d(g, dzx[n]), ci[n], py[n],
-                                prof_at(HR, th, by.h.k0 + dk * n));
-            hy[n] = madd2(1.0f, hy[n], ch[n], dzy[n]);
-        }
-#pragma unroll
-        for (int n = 0; n < W; ++n) st1(g, wr.hy + oh + n * 32 * dk, py[n]);
-    } else {
-        adj_h_row_shot<W>(g, R, by, i, j0, lane, hx, hy, dzx, dzy, ch, rd, wr);
-    }
 }
 
 }  // namespace fg

@@ -360,7 +360,8 @@ __device__ __forceinline__ void fwd_tile_rows(const Dev& g, const float* Rp, con
     while (sc < se && __ldg(g.src_ev + sc).x < ifirst) ++sc;
     while (rc < re && __ldg(g.rx_ev + rc).x < ifirst) ++rc;
     const long long hrow = (long long)g.Ph * CS;
-    float* hist = g.hist ? g.hist + (((long long)t * g.ngroups + grp) * nx) * hrow + (long long)j0 * CS + l : nullptr;
+    float* hist = g.hist ? g.hist + (((long long)(t - g.hist_t0) * g.ngroups + grp) * nx) * hrow + (long long)j0 * CS + l
+                             : nullptr;
     float* ezW = g.ez[wp] + go;
     float* hxW = g.hx[wp] + go;
     float* hyW = g.hy[wp] + go;
@@ -462,8 +463,9 @@ __device__ __forceinline__ void adj_tile_issue(const Dev& g, const CUtensorMap* 
     tma_state<SHOT>(st + L.hx, tm_hx, cs, i0, grp, 1, rp, bar);
     tma_state<SHOT>(st + L.hy, tm_hy, SHOT ? cs + 1 : cs, i0 - 1, grp, 2, rp, bar);
     tma_load_3d(st + L.co, tm_co, b0 - 4 + PADC, i0, 0, bar);
-    if (SHOT) tma_load_4d(st + L.hs, tm_h, 0, b0, i0, it * g.ngroups + grp, bar);
-    else tma_load_3d(st + L.hs, tm_h, b0, i0, it * g.ngroups + grp, bar);
+    const int hz = (it - g.hist_t0) * g.ngroups + grp;
+    if (SHOT) tma_load_4d(st + L.hs, tm_h, 0, b0, i0, hz, bar);
+    else tma_load_3d(st + L.hs, tm_h, b0, i0, hz, bar);
     prefetch_tile_psi<TileGeom<W, SHOT>::CS>(g, grp, rp, i0, i0 + R, b0, b0 + TileGeom<W, SHOT>::BW);
 }
 
@@ -620,7 +622,7 @@ __device__ __forceinline__ void adj_tile_h_row(const Dev& g, const float* Rp, co
             }
             if constexpr (SHOT) {
                 const BandY by = band_adj<W>(g, j0);
-                if (by.lean) adj_h_row_cpml_shot<W>(g, Rp, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+                if (by.lean) adj_h_row_shot<W>(g, Rp, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
                 else {
                     hx_cells<W, CS>(g, Rp, i, j0, l, hx, dzx, ch, 0, rd, wr);
                     hy_cells<W, CS, true>(g, Rp, i, j0, l, hy, dzy, ch, rd, wr);

@@ -69,7 +69,9 @@ typedef struct fg_problem {
 typedef struct fg_tuning {
     int32_t lanes;             /* 0 = choose (shot lanes when shots >= 8), 1 = shot lanes: the 32
                                   lanes of a warp are 32 shots of the same cells, 2 = column
-                                  lanes: one shot per warp, lanes own consecutive columns */
+                                  lanes: one shot per warp, lanes own consecutive columns,
+                                  3 = shot pairs: 64 shots of the same cells, two per lane
+                                  (lane march only, cells_per_thread 2 or 4, no stages) */
     int32_t cells_per_thread;  /* 2, 4 or 8 (default 4 with shot lanes, 2 with column lanes) */
     int32_t rows_per_tile;     /* rows of one tile, >= 1 (default 4) */
     int32_t warps_per_block;   /* 1, 2 or 4 (default 4) */
@@ -83,6 +85,16 @@ typedef struct fg_tuning {
                                   (column lanes); 1 = lane march (persistent warps).  With no
                                   kernel, stages, rows or cells given, shot lanes take the lane
                                   march and column lanes the tile pipeline. */
+    /* The adjoint runs on a plan of its own (own state and accumulators); its
+     * launch shape: adj_kernel 0 = the forward's shape when the fields above
+     * name one, else the default adjoint shape (shot lanes: tile pipeline,
+     * 8 rows over 4 consumer warps, 2 stages; column lanes: the forward's);
+     * 1 = tile pipeline, 2 = lane march, shaped by the three fields below
+     * (0 = their defaults).  cells_per_thread and lanes are shared. */
+    int32_t adj_kernel;
+    int32_t adj_rows_per_tile;
+    int32_t adj_warps_per_block;
+    int32_t adj_stages;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
@@ -100,7 +112,8 @@ int fg_plan_destroy(fg_plan* plan);
  * solve's count are padding.  The buffer holds the product of the five
  * extents in floats. */
 int fg_plan_hist_shape(const fg_plan* plan, int64_t shape[5]);
-/* Device scratch a plan needs, in bytes (>= 0), or -1 on a NULL plan. */
+/* Device scratch a plan needs (its own and its adjoint plan's), in bytes
+ * (>= 0), or -1 on a NULL plan. */
 int64_t fg_plan_workspace_bytes(const fg_plan* plan);
 /* Attach a workspace (256-byte aligned device memory of at least
  * fg_plan_workspace_bytes bytes) and upload the plan's tables into it. */
@@ -131,6 +144,29 @@ int fg_forward(fg_plan* plan, const float* er, const float* se, const float* mr,
 int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const float* mr,
                          const float* hist, const float* resid, float* grad_eps, float* grad_sig,
                          int32_t normalize, double* norms, void* stream);
+
+/* Checkpointed solve, for histories that do not fit in device memory (the
+ * reference keeps the whole Ez history, src/compute.py:553, which limits it
+ * to nt * shots * nx * ny * 4 bytes of HBM).  fg_forward_checkpointed runs the
+ * forward solve and saves the state (fields and CPML auxiliaries) at the
+ * start of every `interval`-th step instead of the history;
+ * fg_adjoint_reference_checkpointed then walks the segments backwards:
+ * it restores a segment's checkpoint, recomputes that segment's Ez history
+ * into `segment` (interval steps in the layout of fg_plan_hist_shape, i.e.
+ * interval * groups * nx * pitch * slots floats) and runs the segment's
+ * adjoint steps.  One extra forward solve of work; traces, gradients and
+ * norms are bit-identical to fg_forward + fg_adjoint_reference.  ckpt: device
+ * memory of fg_plan_checkpoint_bytes(plan, interval) bytes (may be 0 when
+ * interval >= nt), 16-byte aligned.  The adjoint call uses the plan's
+ * forward state as scratch, so the two calls of one solve must not overlap
+ * with other solves on the same plan. */
+int64_t fg_plan_checkpoint_bytes(const fg_plan* plan, int32_t interval);
+int fg_forward_checkpointed(fg_plan* plan, const float* er, const float* se, const float* mr, float* traces,
+                            void* ckpt, int64_t ckpt_bytes, int32_t interval, void* stream);
+int fg_adjoint_reference_checkpointed(fg_plan* plan, const float* er, const float* se, const float* mr,
+                                      const void* ckpt, int64_t ckpt_bytes, int32_t interval, float* segment,
+                                      const float* resid, float* grad_eps, float* grad_sig, int32_t normalize,
+                                      double* norms, void* stream);
 
 /* Forward solve that allocates no device memory: no counterpart in the
  * reference (whose launchers take buffers allocated by torch).

@@ -68,3 +68,37 @@ def test_tv_workspace_size_without_gpu(fg):
     L = nat.lib()
     assert L.fg_tv_workspace_bytes(440, 340) >= 7 * 442 * 342 * 4
     assert L.fg_tv_workspace_bytes(0, 5) == -1
+
+
+def test_checkpoint_sizes_and_adjoint_tuning_without_gpu(fg):
+    """Checkpoint buffer sizes and adjoint launch-shape validation are host-side."""
+    import numpy as np
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    L = nat.lib()
+    src = np.array([[[3, 3, 0]]], np.int32)
+    rx = np.array([[[5, 5, 0]]], np.int32)
+    nt = 50
+    srcw = np.ones((1, nt), np.float32)
+    prob = nat.FgProblem()
+    prob.nx, prob.ny, prob.shots, prob.nt, prob.th = 16, 12, 1, nt, 0
+    prob.dx, prob.dt = 0.1, 1e-10
+    prob.nsrc, prob.nrx = 1, 1
+    prob.src = src.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    prob.rx = rx.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    prob.srcw = srcw.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    h = ctypes.c_void_p()
+    assert L.fg_plan_create(ctypes.byref(prob), None, ctypes.byref(h)) == nat.FG_OK
+    one = L.fg_plan_checkpoint_bytes(h, 49)          # two segments: one checkpoint
+    assert one > 0
+    assert L.fg_plan_checkpoint_bytes(h, 50) == 0     # one segment: the initial state is zero
+    assert L.fg_plan_checkpoint_bytes(h, 1000) == 0
+    assert L.fg_plan_checkpoint_bytes(h, 10) == 4 * one
+    assert L.fg_plan_checkpoint_bytes(h, 1) == (nt - 1) * one
+    assert L.fg_plan_checkpoint_bytes(h, 0) == -1
+    L.fg_plan_destroy(h)
+    bad = nat.FgTuning(*([0] * 6 + [3, 0, 0, 0]))     # adj_kernel 3 does not exist
+    assert L.fg_plan_create(ctypes.byref(prob), ctypes.byref(bad), ctypes.byref(h)) == nat.FG_ERR_INVALID
+    assert b"adj_kernel" in L.fg_last_error()
+    ok = nat.FgTuning(*([0] * 6 + [2, 3, 2, 0]))      # lane-march adjoint
+    assert L.fg_plan_create(ctypes.byref(prob), ctypes.byref(ok), ctypes.byref(h)) == nat.FG_OK
+    L.fg_plan_destroy(h)

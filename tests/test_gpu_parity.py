@@ -129,6 +129,13 @@ TUNINGS = [
     {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 9, "stages": 2},
     {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 16, "warps_per_block": 2, "stages": 4},
     {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 6, "stages": 3},
+    # shot pairs (two shots per lane)
+    {"kernel": 1, "lanes": 3, "cells_per_thread": 2, "rows_per_tile": 4},
+    {"kernel": 1, "lanes": 3, "cells_per_thread": 4, "rows_per_tile": 5},
+    # forward and adjoint on different launch shapes
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 1, "adj_rows_per_tile": 8,
+     "adj_warps_per_block": 4, "adj_stages": 2},
+    {"kernel": 0, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 8, "adj_kernel": 2, "adj_rows_per_tile": 3},
 ]
 
 
@@ -224,12 +231,18 @@ def test_shot_alone_equals_shot_in_batch(fg, dev, lanes):
         assert torch.equal(tr1[0], tr[s])
 
 
-def test_two_shot_groups_vs_oracle(fg, orc, dev):
-    """More shots than one warp's 32 lanes: two shot groups, the second padded."""
-    wl = fg.workloads.small(shots=37, nt=70, fixed=True)
+@pytest.mark.parametrize("shots,tuning", [
+    (37, None),
+    (37, {"lanes": 3, "kernel": 1, "cells_per_thread": 2}),
+    (70, {"lanes": 3, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 3}),
+])
+def test_two_shot_groups_vs_oracle(fg, orc, dev, shots, tuning):
+    """More shots than one group holds (32 shot lanes, 64 shot pairs): two
+    shot groups, the second padded; or one padded group of pairs."""
+    wl = fg.workloads.small(shots=shots, nt=70, fixed=True, nx=64)
     wl.source_step = [0.03, 0.01, 0.0]
     prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
-    solve = fg.Solve(dev, setup, tv=False)
+    solve = fg.Solve(dev, setup, tv=False, tuning=tuning)
     er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
     traces, hist = solve.forward(er, se, mr)
     o_tr, o_hist = orc.forward(prob, np.float32)
