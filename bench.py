@@ -59,11 +59,12 @@ PKG = "fast-gpr-fwi_b200"
 METRIC = "Gcell-steps/s fwd+adjoint"
 UNIT = "Gcell-steps/s"
 
-# DRAM bytes per shot-cell-step of the default step kernels, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch on the
-# 64-shot 440x340 grid, summarised under profiles/): forward
-# 261.3 MB, adjoint 282.5 MB per launch over 64 x 440 x 340 shot-cells.
-NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 261.3e6 / (64 * 440 * 340), "adjoint": 282.5e6 / (64 * 440 * 340)}
+# DRAM bytes per shot-cell-step of the default step kernels (forward: lane
+# march, adjoint: tile pipeline), from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch on the 64-shot 440x340 grid, summarised
+# under profiles/): forward 262.0 MB, adjoint 280.5 MB per launch over
+# 64 x 440 x 340 shot-cells.
+NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 262.0e6 / (64 * 440 * 340), "adjoint": 280.5e6 / (64 * 440 * 340)}
 
 
 def _fg():

@@ -13,9 +13,10 @@ The package directory name is not a Python identifier; import it with
 ``importlib.import_module("fast-gpr-fwi_b200")`` (or alias it, e.g.
 ``sys.modules["src"] = ...`` for code written against the reference).
 """
-from . import grid, shots, workloads
+from . import fwi, grid, shots, workloads
 from .compute import GPRFWI, Solve, compute
 from .multiscale import apply_filter, design_fir_filter
 from .tv import total_variation
+from .fwi import Inversion
 
-__all__ = ["compute", "GPRFWI", "Solve", "apply_filter", "design_fir_filter", "total_variation"]
+__all__ = ["compute", "GPRFWI", "Solve", "apply_filter", "design_fir_filter", "total_variation", "Inversion"]

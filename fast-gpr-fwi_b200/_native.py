@@ -30,6 +30,7 @@ EXPORTS = (
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
     "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
+    "fg_fir_causal", "fg_adjoint_reference_l1",
 )
 
 
@@ -112,6 +113,10 @@ def lib() -> ctypes.CDLL:
     L.fg_forward_checkpointed.restype = ctypes.c_int
     L.fg_adjoint_reference_checkpointed.argtypes = [vp, vp, vp, vp, vp, i64, i32, vp, vp, vp, vp, i32, vp, vp]
     L.fg_adjoint_reference_checkpointed.restype = ctypes.c_int
+    L.fg_adjoint_reference_l1.argtypes = [vp, vp, vp, vp, vp, vp, vp, f32, vp, vp, i32, vp, vp]
+    L.fg_adjoint_reference_l1.restype = ctypes.c_int
+    L.fg_fir_causal.argtypes = [vp, i64, i32, i32, vp, i32, vp, vp]
+    L.fg_fir_causal.restype = ctypes.c_int
     L.fg_tv_workspace_bytes.argtypes = [i32, i32]
     L.fg_tv_workspace_bytes.restype = i64
     L.fg_total_variation.argtypes = [vp, i32, i32, ctypes.c_double, ctypes.c_double, i32, ctypes.c_double, vp, vp,
@@ -216,6 +221,15 @@ class Plan:
         if checked_build():
             self.device_check()
 
+    def adjoint_reference_l1(self, er32, se32, mr32, hist, traces, observed, scale, grad_eps, grad_sig,
+                             normalize=True, norms=None):
+        """Adjoint of the L1 misfit scale * sum |traces - observed|, injected on the fly."""
+        check(lib().fg_adjoint_reference_l1(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(hist), ptr(traces),
+                                            ptr(observed), float(scale), ptr(grad_eps), ptr(grad_sig),
+                                            1 if normalize else 0, ptr(norms), stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
     # checkpointed solve (fg_forward_checkpointed / fg_adjoint_reference_checkpointed)
     def checkpoint_bytes(self, interval: int) -> int:
         return int(lib().fg_plan_checkpoint_bytes(self._h, int(interval)))
@@ -274,3 +288,18 @@ def total_variation(data: torch.Tensor, lamda: float, rho: float, num_iter: int,
         check(L.fg_total_variation(d.data_ptr(), M, N, float(lamda), float(rho), int(num_iter), float(tol),
                                    out.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(iters), stream))
     return out, int(iters.value)
+
+
+def fir_causal(x: torch.Tensor, taps: torch.Tensor) -> torch.Tensor:
+    """fg_fir_causal on a float32 CUDA tensor of shape (batch, T, R); taps (k,)."""
+    if x.dim() != 3 or x.dtype != torch.float32 or not x.is_cuda:
+        raise ValueError("fir kernel: needs a 3-D float32 CUDA tensor (batch, T, R)")
+    L = lib()
+    xc = x.contiguous()
+    h = taps.to(device=x.device, dtype=torch.float32).contiguous()
+    out = torch.empty_like(xc)
+    b, T, R = xc.shape
+    with torch.cuda.device(x.device):
+        check(L.fg_fir_causal(xc.data_ptr(), b, T, R, h.data_ptr(), h.numel(), out.data_ptr(),
+                              torch.cuda.current_stream(x.device).cuda_stream))
+    return out

@@ -16,6 +16,7 @@
 #include "fdtd_tile.cuh"
 #include "tv.cuh"
 #include "fdtd_pairs.cuh"
+#include "fir.cuh"
 
 using fg::Dev;
 using fg::Ev;
@@ -617,6 +618,29 @@ struct TvLayout {
 };
 }  // namespace
 
+int fg_fir_causal(const float* x, int64_t batch, int32_t T, int32_t R, const float* taps, int32_t k, float* out,
+                  void* stream) {
+    if (batch < 0 || T < 1 || R < 1) return fail(FG_ERR_INVALID, "fg_fir_causal: bad shape");
+    if (k < 1 || k > fg::FIR_MAX_TAPS) return fail(FG_ERR_INVALID, "fg_fir_causal: taps must number 1.." +
+                                                                       std::to_string(fg::FIR_MAX_TAPS));
+    if (k - 1 >= T) return fail(FG_ERR_INVALID, "fg_fir_causal: the reflect padding (taps - 1) must be shorter "
+                                                "than the series");
+    if (batch == 0) return FG_OK;
+    if (!x || !out || !taps) return fail(FG_ERR_INVALID, "fg_fir_causal: NULL argument");
+    const size_t bytes = (size_t)batch * T * R * sizeof(float);
+    if ((const char*)out < (const char*)x + bytes && (const char*)x < (const char*)out + bytes)
+        return fail(FG_ERR_INVALID, "fg_fir_causal: out overlaps x");
+    int dev = 0, sms = 0;
+    FG_CUDA(cudaGetDevice(&dev));
+    FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long n = batch * (long long)T * R;
+    const long long blocks = std::max<long long>(1, std::min<long long>((n + fg::FIR_THREADS - 1) / fg::FIR_THREADS,
+                                                                        (long long)sms * 8));
+    fg::k_fir_causal<<<(unsigned)blocks, fg::FIR_THREADS, 0, (cudaStream_t)stream>>>(x, batch, T, R, taps, k, out);
+    FG_CUDA(cudaGetLastError());
+    return FG_OK;
+}
+
 int64_t fg_tv_workspace_bytes(int32_t M, int32_t N) {
     if (M < 1 || N < 1) return -1;
     return (int64_t)TvLayout(M, N).total;
@@ -1050,13 +1074,13 @@ int fg_forward(fg_plan* p, const float* er, const float* se, const float* mr, fl
     return fwd_steps(p, g, 0, p->nt, st);
 }
 
-int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
-                         const float* resid, float* grad_eps, float* grad_sig, int32_t normalize, double* norms,
-                         void* stream) {
+static int adjoint_full(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
+                        const float* resid, const float* obs, float obs_scale, float* grad_eps, float* grad_sig,
+                        int32_t normalize, double* norms, void* stream, const char* who) {
     if (!p || !er || !se || !mr || !hist || (!resid && p->nrx > 0))
-        return fail(FG_ERR_INVALID, "fg_adjoint_reference: NULL argument");
+        return fail(FG_ERR_INVALID, std::string(who) + ": NULL argument");
     fg_plan* a = p->adj ? p->adj : p;
-    if (!a->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_reference: plan has no workspace");
+    if (!a->ws) return fail(FG_ERR_WORKSPACE, std::string(who) + ": plan has no workspace");
     cudaStream_t st = (cudaStream_t)stream;
     int rc = adj_begin(a, er, se, mr, st);
     if (rc) return rc;
@@ -1065,8 +1089,25 @@ int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const flo
     g.out_lo = (const char*)hist;
     g.out_hi = (const char*)(hist + (size_t)a->nt * hist_step_floats(a));
     g.resid = resid;
+    g.obs = obs;
+    g.obs_scale = obs_scale;
     if ((rc = adj_steps(a, g, a->nt - 1, 1, a->nt, st))) return rc;
     return adj_finish(a, g, grad_eps, grad_sig, normalize, norms, st);
+}
+
+int fg_adjoint_reference(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
+                         const float* resid, float* grad_eps, float* grad_sig, int32_t normalize, double* norms,
+                         void* stream) {
+    return adjoint_full(p, er, se, mr, hist, resid, nullptr, 0.f, grad_eps, grad_sig, normalize, norms, stream,
+                        "fg_adjoint_reference");
+}
+
+int fg_adjoint_reference_l1(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
+                            const float* traces, const float* observed, float scale, float* grad_eps,
+                            float* grad_sig, int32_t normalize, double* norms, void* stream) {
+    if (p && p->nrx > 0 && !observed) return fail(FG_ERR_INVALID, "fg_adjoint_reference_l1: NULL observed traces");
+    return adjoint_full(p, er, se, mr, hist, traces, observed, scale, grad_eps, grad_sig, normalize, norms, stream,
+                        "fg_adjoint_reference_l1");
 }
 
 int64_t fg_plan_checkpoint_bytes(const fg_plan* p, int32_t interval) {

@@ -74,7 +74,9 @@ struct Dev {
     float* traces;       // (S, nt, nrx)
     float* hist;         // (steps, ngroups, nx, Ph, CS): step t at index t - hist_t0
     int hist_t0;         // first step the history buffer holds (0 = the whole run)
-    const float* resid;  // (S, nt, nrx)
+    const float* resid;  // (S, nt, nrx): residual, or the synthetic traces when obs is set
+    const float* obs;    // (S, nt, nrx) observed traces: inject obs_scale * sign(resid - obs), else NULL
+    float obs_scale;
     double* gacc;        // (ngroups, 2, nx, ny)
     // bounds of every buffer the kernels touch (checked builds)
     const char* ws_lo; const char* ws_hi;
@@ -159,6 +161,18 @@ __device__ __forceinline__ void st_cells(const Dev& g, float* p, const float* x)
             else __stcg(p + k * CS, x[k]);
         }
     }
+}
+
+// Value injected at a receiver by the adjoint (back.cu:34 subtracts it from
+// Ez): the residual resid[o]; or, with observed traces, the derivative of
+// the L1 misfit sum |syn - obs| * scale formed on the fly from the synthetic
+// traces (in resid) and the observed ones, scale * sign(syn - obs), as
+// torch's L1 loss backward forms it (sign(0) = 0).
+__device__ __forceinline__ float inj_value(const Dev& g, long long o) {
+    const float syn = __ldg(g.resid + o);
+    if (!g.obs) return syn;
+    const float d = __fsub_rn(syn, __ldg(g.obs + o));
+    return __fmul_rn((float)((0.f < d) - (d < 0.f)), g.obs_scale);
 }
 
 // a += x on a float64 imaging accumulator: a reduction applied by the memory

@@ -583,7 +583,7 @@ __device__ __forceinline__ void adj_e_load(const Dev& g, AdjEIn<W>& A, int r, in
 template <int W, int CS>
 __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A, int r, int j0,
                                           int l, int slot, bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
-                                          const float* resid_s, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
+                                          long long resid_o, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
     // back_source (back.cu:34): Ez -= residual, no scaling
     for (; ic < ie; ++ic) {
         const Ev e = __ldg(g.inj_ev + ic);
@@ -591,7 +591,7 @@ __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const Ba
         if (e.y != slot) continue;
 #pragma unroll
         for (int k = 0; k <= W; ++k)
-            if (j0 + k == e.z) A.ez[k] = __fsub_rn(A.ez[k], __ldg(resid_s + e.w));
+            if (j0 + k == e.z) A.ez[k] = __fsub_rn(A.ez[k], inj_value(g, resid_o + e.w));
     }
     if (core) {
 #pragma unroll
@@ -755,7 +755,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
         if constexpr (SHOT) by = band_adj<W>(g, j0);
         int ic = __ldg(g.inj_off + T.id);
         const int ie = __ldg(g.inj_off + T.id + 1);
-        const float* resid_s = g.resid + ((long long)T.s * g.nt + it) * g.nrx;
+        const long long resid_o = ((long long)T.s * g.nt + it) * g.nrx;
         const float* f1g = g.hist + ((long long)(it - g.hist_t0) * g.ngroups + T.grp) * nx * hrow + (long long)j0 * CS + l;
         double* gae = g.gacc + (long long)T.grp * 2 * ((long long)nx * ny);
         double* gas = gae + (long long)nx * ny;
@@ -778,7 +778,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
 #pragma unroll
             for (int w = 0; w < W; ++w) eoc[w] = A.ez[w];
             adj_e_row<W, CS>(g, R, by, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
-                             ezc, resid_s, ic, ie, rd, wr);
+                             ezc, resid_o, ic, ie, rd, wr);
 #pragma unroll
             for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
 #pragma unroll
@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
 #pragma unroll
                 for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
                 adj_e_row<W, CS>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < T.i1, hyc, ezr,
-                                 resid_s, ic, ie, rd, wr);
+                                 resid_o, ic, ie, rd, wr);
             } else {
 #pragma unroll
                 for (int w = 0; w < W; ++w) eor[w] = 0.f;

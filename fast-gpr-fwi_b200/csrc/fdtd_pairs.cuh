@@ -5,9 +5,12 @@
 // access is then 256 contiguous bytes, and every per-cell cost that does not
 // depend on the shot -- addresses, coefficient loads, boundary tests, loop
 // control -- is paid once for two shots.  The interior arithmetic runs on the
-// paired fp32 instructions of sm_100 (add/sub/mul/fma .rn.f32x2), which round
-// each element exactly as the scalar instruction does, so every cell is the
-// scalar kernels' (and the reference's) value bit for bit.
+// paired fp32 instructions of sm_100 (add/sub/fma .rn.f32x2), which round each
+// element exactly as the scalar instruction does, so every cell is the scalar
+// kernels' (and the reference's) value bit for bit.  One exception is kept
+// out: ptxas fuses a paired multiply into a paired add or subtract that
+// consumes it (one rounding instead of two) even when both carry .rn, so a
+// product that feeds an add is taken as two scalar multiplies (mulbc).
 //
 // Rows outside the interior core (CPML slabs, the grid edges) take the
 // per-cell update of fdtd_common.cuh for each of the two slots in turn.
@@ -21,19 +24,41 @@ namespace fg {
 
 using f2 = float2;
 
+// Paired fp32 operations as PTX with an explicit .rn rounding.
 __device__ __forceinline__ f2 bc2(float s) { return make_float2(s, s); }
-__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
-    unsigned long long x, y, d;
+__device__ __forceinline__ unsigned long long as_u64(f2 a) {
+    unsigned long long x;
     memcpy(&x, &a, 8);
-    memcpy(&y, &b, 8);
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+    return x;
+}
+__device__ __forceinline__ f2 as_f2(unsigned long long x) {
     f2 r;
-    memcpy(&r, &d, 8);
+    memcpy(&r, &x, 8);
     return r;
 }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    return as_f2(d);
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    return as_f2(d);
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    unsigned long long d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)));
+    return as_f2(d);
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(as_u64(a)), "l"(as_u64(b)), "l"(as_u64(c)));
+    return as_f2(d);
+}
+// s * x rounded per element by scalar multiplies, for a product that an add
+// or subtract consumes (see the file comment).
+__device__ __forceinline__ f2 mulbc(float s, f2 x) { return make_float2(__fmul_rn(s, x.x), __fmul_rn(s, x.y)); }
 __device__ __forceinline__ float comp(f2 v, int k) { return k ? v.y : v.x; }
 __device__ __forceinline__ void set_comp(f2& v, int k, float x) {
     if (k) v.y = x;
@@ -131,7 +156,7 @@ __global__ void __launch_bounds__(128, 3) k_fwd2(const Dev g, const int t) {
             const bool hcore = (th == 0 || (ih >= th && ih <= nx - th - 1)) && j0 >= 1 && j0 + W <= ny;
             if (hcore) {
 #pragma unroll
-                for (int w = 0; w < W; ++w) hyu[w] = add2(hyu[w], mul2(bc2(cah[w]), sub2(ezc[w + 1], ea[w])));
+                for (int w = 0; w < W; ++w) hyu[w] = add2(hyu[w], mulbc(cah[w], sub2(ezc[w + 1], ea[w])));
             } else {
 #pragma unroll
                 for (int w = 0; w < W; ++w)
@@ -151,10 +176,10 @@ __global__ void __launch_bounds__(128, 3) k_fwd2(const Dev g, const int t) {
             f2 hxn[W + 1], hyn[W], ezn[W];
             if (bcore && i >= th + 1 && i <= nx - th - 1) {
 #pragma unroll
-                for (int k = 0; k <= W; ++k) hxn[k] = sub2(B.hxo[k], mul2(bc2(B.ch[k]), sub2(ezc[k + 1], ezc[k])));
+                for (int k = 0; k <= W; ++k) hxn[k] = sub2(B.hxo[k], mulbc(B.ch[k], sub2(ezc[k + 1], ezc[k])));
 #pragma unroll
                 for (int w = 0; w < W; ++w)
-                    hyn[w] = add2(B.hyo[w], mul2(bc2(B.ch[w + 1]), sub2(B.en[w + 1], ezc[w + 1])));
+                    hyn[w] = add2(B.hyo[w], mulbc(B.ch[w + 1], sub2(B.en[w + 1], ezc[w + 1])));
 #pragma unroll
                 for (int w = 0; w < W; ++w)
                     ezn[w] = fma2(bc2(-B.cb[w]), sub2(hxn[w + 1], hxn[w]),
@@ -281,7 +306,7 @@ __device__ __forceinline__ void adj_e_row2(const Dev& g, const float* R, AdjEIn2
         const Ev e = __ldg(g.inj_ev + ic);
         if (e.x != r) break;
         if ((e.y >> 1) != lane) continue;
-        const float v = __ldg(g.resid + ((long long)(grp * 64 + e.y) * g.nt + it) * g.nrx + e.w);
+        const float v = inj_value(g, ((long long)(grp * 64 + e.y) * g.nt + it) * g.nrx + e.w);
 #pragma unroll
         for (int k = 0; k <= W; ++k)
             if (j0 + k == e.z) set_comp(A.ez[k], e.y & 1, __fsub_rn(comp(A.ez[k], e.y & 1), v));
@@ -396,8 +421,8 @@ __global__ void __launch_bounds__(128, 3) k_adj2(const Dev g, const int it, cons
             if (bcore && i >= th + 1 && i <= nx - th - 1) {
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
-                    hx[w] = sub2(hxc[w + 1], mul2(bc2(ch[w]), sub2(ezc[w + 1], ezc[w])));
-                    hy[w] = add2(hyc[w], mul2(bc2(ch[w]), sub2(ezr[w], ezc[w])));
+                    hx[w] = sub2(hxc[w + 1], mulbc(ch[w], sub2(ezc[w + 1], ezc[w])));
+                    hy[w] = add2(hyc[w], mulbc(ch[w], sub2(ezr[w], ezc[w])));
                 }
             } else {
 #pragma unroll
@@ -420,13 +445,13 @@ __global__ void __launch_bounds__(128, 3) k_adj2(const Dev g, const int it, cons
             // imaging (compute.py:1167-1172), summed by parts as in k_adj: the two
             // shots of a lane first, then the lanes by a reduce-scatter
             float v[2 * W];
-            const f2 dt2 = bc2(g.dt);
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                const f2 a = mul2(f1[w], sub2(ezc[w], eoc[w]));
-                const f2 b = mul2(mul2(f1[w], ezc[w]), dt2);
-                v[w] = __fadd_rn(a.x, a.y);
-                v[W + w] = __fadd_rn(b.x, b.y);
+                // products that an add consumes: scalar multiplies (see the file comment)
+                const f2 d = sub2(ezc[w], eoc[w]);
+                v[w] = __fadd_rn(__fmul_rn(f1[w].x, d.x), __fmul_rn(f1[w].y, d.y));
+                v[W + w] = __fadd_rn(__fmul_rn(__fmul_rn(f1[w].x, ezc[w].x), g.dt),
+                                     __fmul_rn(__fmul_rn(f1[w].y, ezc[w].y), g.dt));
             }
             const long long go2 = (long long)i * ny + j0;
             {

@@ -510,7 +510,7 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
     const bool bcore = j0 >= th + 1 && j0 + W <= ny - th - 1;
     BandY by{};
     if constexpr (SHOT) by = band_adj<W>(g, j0);
-    const float* resid_s = g.resid + ((long long)s * g.nt + it) * g.nrx;
+    const long long resid_o = ((long long)s * g.nt + it) * g.nrx;
     const AdjCols<W, SHOT> C(lane);
 #define EZS(r, k) sEZ[((r) * G::AEZ + C.c0 + (k)) * CS + l]
 #define HXS(r, k) sHX[((r) * G::AHX + C.cx + (k)) * CS + l]
@@ -543,7 +543,7 @@ __device__ __forceinline__ void adj_tile_e(const Dev& g, const float* Rp, unsign
         const int ie = E.y;
         while (ic < ie && __ldg(g.inj_ev + ic).x < r) ++ic;
         float e[W + 1];
-        adj_e_row<W, CS>(g, Rp, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_s,
+        adj_e_row<W, CS>(g, Rp, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyu, e, resid_o,
                          ic, ie, rd, wr);
 #pragma unroll
         for (int k = 0; k <= W; ++k) ENS(rr, k) = e[k];

@@ -1,0 +1,123 @@
+"""The inversion loop of the reference's example (example.ipynb, the training
+cell): Adam on eps_r (and, after a first phase, sigma), an L1 misfit times a
+weight, gradients zeroed on the CPML columns, the TV term of the default
+gradient.  Each epoch is one forward solve and one adjoint solve; the plan is
+rebuilt only when the model's first row changes (the HORIPML profile
+averages it, grid.slab_average) -- the reference rebuilds its grid, PML
+profile and coefficient arrays in every compute() call -- and the L1
+misfit's derivative is formed
+inside the adjoint's injection (fg_adjoint_reference_l1), so the residual
+tensor torch's L1Loss backward would build is never materialised.
+
+With the same inputs an epoch produces the gradients the notebook's
+compute() + L1Loss + backward() produce (tests/test_gpu_fwi.py).
+"""
+from __future__ import annotations
+
+from typing import Optional, Sequence
+
+import torch
+
+from .compute import Solve
+from .grid import build_setup
+from .tv import total_variation
+
+
+class Inversion:
+    """Full-waveform inversion of (eps_r, sigma) from observed traces.
+
+    ``kwargs`` are compute()'s keyword arguments for the survey geometry
+    (dx, ny, nx, nz, source, source_apmlitudes, step, nsrc, nrx,
+    time_windows, source/receiver locations and steps, pmlthick, dt,
+    Fixedreceiver); er0/se0/mr are (nx, ny, 1) starting models.  The
+    notebook's settings are the defaults: phase 1 (eps_r alone, lr 0.2) for
+    50 epochs, then eps_r at lr 0.1 and sigma at lr 1e-4, loss weight 100.
+    """
+
+    def __init__(self, device, kwargs: dict, observed: torch.Tensor, er0: torch.Tensor, se0: torch.Tensor,
+                 mr: torch.Tensor, phase1_epochs: int = 50, lr: Sequence[float] = (0.2, 0.1, 1e-4),
+                 loss_weight: float = 100.0, tv: bool = True, tv_weight: float = 0.01,
+                 tuning: Optional[dict] = None):
+        self.device = torch.device(device)
+        kw = dict(kwargs)
+        self.pml = int(kw.get("pmlthick", 0))
+        self.er = er0.detach().clone().to(self.device).requires_grad_(True)
+        self.se = se0.detach().clone().to(self.device).requires_grad_(True)
+        self.mr = mr.detach().to(self.device)
+        self.observed = observed.detach().to(self.device, torch.float32).contiguous()
+        self.loss_weight = float(loss_weight)
+        self.phase1_epochs = int(phase1_epochs)
+        self.opt1 = torch.optim.Adam([{"params": self.er, "lr": lr[0]}])
+        self.opt2 = torch.optim.Adam([{"params": self.er, "lr": lr[1]}, {"params": self.se, "lr": lr[2]}])
+        self.kw = kw
+        self.solve_args = dict(tuning=tuning, tv=tv, tv_weight=tv_weight)
+        self._row0 = None
+        self._plan_for(torch.clamp(self.er.detach(), min=1))
+        setup = self.setup
+        if tuple(self.observed.shape) != (setup.shots, setup.nt, self.solve.plan.nrx):
+            raise ValueError("observed traces %s != (%d, %d, %d)" % (tuple(self.observed.shape), setup.shots,
+                                                                      setup.nt, self.solve.plan.nrx))
+        # torch's L1Loss(mean) * w backward: w / numel in float32, times sign(syn - obs)
+        n = torch.tensor(float(self.observed.numel()), dtype=torch.float32)
+        self.scale = float(torch.tensor(self.loss_weight, dtype=torch.float32) / n)
+        self.epochs = 0
+
+    def _plan_for(self, er_c: torch.Tensor) -> None:
+        """(Re)build the set-up and plan when the profile's input (row 0 of the
+        clamped eps_r) differs from the one the current plan was built on."""
+        row0 = er_c[0].detach()
+        if self._row0 is not None and torch.equal(row0, self._row0):
+            return
+        kw = self.kw
+        self.setup = build_setup(self.device, kw["dx"], kw["ny"], kw["nx"], kw.get("nz", 1), kw.get("time_windows"),
+                                 kw["source"], kw.get("source_location"), kw.get("source_step"),
+                                 kw.get("receiver_location"), kw.get("receiver_step"), kw.get("pmlthick", 0),
+                                 kw["source_apmlitudes"], kw["step"], er_c.detach(), self.mr, kw["nsrc"], kw["nrx"],
+                                 kw.get("dt"), kw.get("freq"), kw.get("total_step"), kw.get("Fixedreceiver", False),
+                                 kw.get("customsource"), kw.get("customreceiver"))
+        self.solve = Solve(self.device, self.setup, **self.solve_args)
+        self._row0 = row0.clone()
+
+    def epoch(self) -> float:
+        """One epoch: forward, loss, fused adjoint, border zeroing, Adam step.
+        Returns the loss (L1 mean times the weight)."""
+        phase2 = self.epochs >= self.phase1_epochs
+        opt = self.opt2 if phase2 else self.opt1
+        opt.zero_grad()
+        er_c = torch.clamp(self.er, min=1)          # compute() clamps its inputs (autograd keeps the mask)
+        se_c = torch.clamp(self.se, min=0)
+        self._plan_for(er_c)
+        s = self.setup
+        plan = self.solve.plan
+        e32, s32, m32 = self.solve.materials(er_c.detach(), se_c.detach(), self.mr)
+        traces = torch.empty((s.shots, s.nt, plan.nrx), dtype=torch.float32, device=self.device)
+        hist = plan.new_hist()
+        plan.forward(e32, s32, m32, traces, hist)
+        loss = (traces - self.observed).abs().mean() * self.loss_weight
+        ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
+        gs = torch.empty_like(ge) if phase2 else None
+        plan.adjoint_reference_l1(e32, s32, m32, hist, traces, self.observed, self.scale, ge, gs)
+        del hist
+        ge = ge.view(er_c.shape)
+        if self.solve.tv:
+            lam = self.solve.tv_weight
+            ge = ge + lam * (2 * (er_c.detach() - total_variation(er_c.detach().clone())))
+        grads = [ge]
+        outs = [er_c]
+        if phase2:
+            gs = gs.view(se_c.shape)
+            if self.solve.tv:
+                gs = gs + self.solve.tv_weight * (2 * (se_c.detach() - total_variation(se_c.detach().clone())))
+            grads.append(gs)
+            outs.append(se_c)
+        torch.autograd.backward(outs, grads)
+        p = self.pml
+        if p > 0:
+            self.er.grad[:, :p, :] = 0
+            self.er.grad[:, -p:, :] = 0
+            if phase2:
+                self.se.grad[:, :p, :] = 0
+                self.se.grad[:, -p:, :] = 0
+        opt.step()
+        self.epochs += 1
+        return float(loss)

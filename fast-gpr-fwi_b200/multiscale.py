@@ -38,9 +38,19 @@ def _fir_causal(series: torch.Tensor, taps: torch.Tensor) -> torch.Tensor:
 
 
 def apply_filter(data: torch.Tensor, fs: float, cutoff: float) -> torch.Tensor:
-    """Low-pass ``data`` (1-D, or (step, iterations, nrx)) at ``cutoff`` Hz."""
+    """Low-pass ``data`` (1-D, or (step, iterations, nrx)) at ``cutoff`` Hz.
+
+    float32 CUDA data runs on fg_fir_causal (libfastgpr.so), which filters
+    the (step, iterations, nrx) layout along axis 1 directly; other tensors
+    take the reference's tensor arithmetic below."""
     numtaps = int(1 * (fs / cutoff))
-    taps = design_fir_filter(cutoff, fs, numtaps).to(data.device)
+    taps = design_fir_filter(cutoff, fs, numtaps)
+    if data.is_cuda and data.dtype == torch.float32 and data.ndim in (1, 3):
+        from . import _native
+        if data.ndim == 1:
+            return _native.fir_causal(data.view(1, -1, 1), taps).view(-1)
+        return _native.fir_causal(data, taps)
+    taps = taps.to(data.device)
     if data.ndim == 1:
         return _fir_causal(data.view(1, 1, -1), taps).view(-1)
     if data.ndim == 3:

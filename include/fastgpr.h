@@ -145,6 +145,17 @@ int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const 
                          const float* hist, const float* resid, float* grad_eps, float* grad_sig,
                          int32_t normalize, double* norms, void* stream);
 
+/* fg_adjoint_reference for the L1 misfit of the multiscale inversion
+ * (example.ipynb's L1Loss feeding back.cu): instead of a residual tensor,
+ * the synthetic traces (fg_forward's) and the observed ones, both
+ * (shots, nt, nrx) float32; the value injected at receiver r of shot s at
+ * step t is scale * sign(traces - observed) with sign(0) = 0, formed inside
+ * the adjoint step -- the gradient of scale * sum |traces - observed|
+ * (scale = 1 / (shots * nt * nrx), rounded to float32, for the mean). */
+int fg_adjoint_reference_l1(fg_plan* plan, const float* er, const float* se, const float* mr, const float* hist,
+                            const float* traces, const float* observed, float scale, float* grad_eps,
+                            float* grad_sig, int32_t normalize, double* norms, void* stream);
+
 /* Checkpointed solve, for histories that do not fit in device memory (the
  * reference keeps the whole Ez history, src/compute.py:553, which limits it
  * to nt * shots * nx * ny * 4 bytes of HBM).  fg_forward_checkpointed runs the
@@ -199,6 +210,18 @@ int fg_adjoint_reference_checkpointed(fg_plan* plan, const float* er, const floa
 #define FG_STATIC_SCRATCH_BYTES (32LL * 1024 * 1024)
 int fg_forward_static(fg_plan* plan, const float* er, const float* se, const float* mr,
                       float* traces, float* hist, void* stream);
+
+/* Causal FIR filter of the multiscale inversion (reference
+ * src/multiscale.py:19-53, apply_filter): x is (batch, T, R) float32 with
+ * the time axis T in the middle and R innermost -- the layout of the traces
+ * fg_forward returns, (shots, nt, nrx); a single series is batch = R = 1.
+ * Each series is reflect-padded by k-1 samples on the left and
+ * cross-correlated with the k taps:
+ *   out[b][t][r] = sum_m taps[m] * x[b][|t + m - (k-1)|][r].
+ * taps: device float32[k], 1 <= k <= 8192 and k - 1 < T; out must not
+ * overlap x.  Float32 sum over m in order with fused multiply-adds. */
+int fg_fir_causal(const float* x, int64_t batch, int32_t T, int32_t R, const float* taps, int32_t k, float* out,
+                  void* stream);
 
 /* Total-variation denoising of an (M, N) float32 model (reference
  * src/tv.py:135-217, the regulariser of the default gradient,

@@ -74,3 +74,33 @@ def test_tv_drop_in_default_stop_matches_tensor_path(fg):
     cpu = fg.total_variation(torch.tensor(x)[:, :, None]).numpy()
     got = fg.total_variation(torch.tensor(x, device="cuda")[:, :, None]).cpu().numpy()
     np.testing.assert_allclose(got, cpu, rtol=1e-6, atol=1e-6 * np.abs(cpu).max())
+
+
+# --- multiscale FIR (fg_fir_causal) ---------------------------------------
+
+@gpu
+def test_fir_kernel_matches_reference_golden(fg):
+    got3 = fg.apply_filter(torch.tensor(GOLD["fir_data3"], device="cuda"), 1e10, 1e8)
+    assert got3.is_cuda and tuple(got3.shape) == GOLD["fir_out3"].shape
+    np.testing.assert_allclose(got3.cpu().numpy(), GOLD["fir_out3"], rtol=1e-6, atol=1e-6)
+    got1 = fg.apply_filter(torch.tensor(GOLD["fir_data1"], device="cuda"), 8e9, 1e8)
+    np.testing.assert_allclose(got1.cpu().numpy(), GOLD["fir_out1"], rtol=1e-6, atol=1e-6)
+
+
+@gpu
+@pytest.mark.parametrize("shape,fs,fc", [((64, 4000, 100), 1.78e10, 2e8), ((3, 257, 7), 1e10, 2.5e8),
+                                         ((2, 50, 1), 1e10, 2e8), ((1, 31, 33), 1e10, 3.3e8)])
+def test_fir_kernel_matches_tensor_path(fg, shape, fs, fc):
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(shape).astype(np.float32)
+    want = fg.apply_filter(torch.tensor(x), fs, fc).numpy()          # CPU: the reference's tensor arithmetic
+    got = fg.apply_filter(torch.tensor(x, device="cuda"), fs, fc).cpu().numpy()
+    scale = np.abs(want).max()
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6 * scale)
+
+
+@gpu
+def test_fir_kernel_rejects_padding_longer_than_series(fg):
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    with pytest.raises(nat.FastGprError):
+        nat.fir_causal(torch.zeros((1, 10, 2), device="cuda"), torch.ones(11))
