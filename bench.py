@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample length")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     return ap.parse_args()
 
 
@@ -353,6 +354,10 @@ def run_ours(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_e2e:
         per_shot = run_per_shot(args, fg, wl, dev)
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        serving = run_serving(fg, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(wl, setup, args.cpu_seconds)
@@ -378,6 +383,7 @@ def run_ours(args, rank, local, world):
             "clocks": clk,
             "e2e": e2e,
             "per_shot_path": per_shot,
+            "serving": serving,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -464,6 +470,57 @@ def run_per_shot(args, fg, wl, dev, shots=4):
     return {"value": round(wl.nx * wl.ny * shots * wl.nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
             "shots": shots, "ms_per_shot": round(ms / shots, 3),
             "api": "compute(..., step=1, tv=False) + traces.backward(resid), looped over shots"}
+
+
+def serving_stream(fg, n=24, seed=4004):
+    """A seeded stream in the spirit of the serving workload: grids from
+    100x60 to 256x256 plus a 20-cell CPML, 1-32 shots, nt 1000-2000,
+    100-200 MHz Ricker, layered models as the benchmark's; half forward,
+    half gradient requests."""
+    serve = importlib.import_module(PKG + ".serve")
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n):
+        nz_, nx_ = int(rng.integers(60, 257)), int(rng.integers(100, 257))
+        shots = int(rng.integers(1, 33))
+        nt = int(rng.integers(1000, 2001))
+        wl = fg.workloads.small(seed=seed + k, nx=nx_ + 40, ny=nz_ + 40, shots=shots, nt=nt, pml=20, dx=0.025,
+                                fixed=True, nrx=16)
+        wl.freq = float(rng.uniform(1e8, 2e8))
+        wl.source_step = [0.0, 0.0, 0.0]
+        kw = wl.kwargs("cuda")
+        for key in ("er", "se", "mr", "device", "tv"):
+            kw.pop(key)
+        resid = None
+        if k % 2:
+            resid = torch.tensor(rng.standard_normal((shots, nt, wl.nrx)).astype(np.float32) * 1e-3)
+        reqs.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid))
+    return serve, reqs
+
+
+def run_serving(fg, dev, rate_hz=40.0):
+    """Continuous batching against one request at a time, same stream and
+    arrivals (Poisson, seeded): p50 / p99 latency and throughput."""
+    serve, reqs = serving_stream(fg)
+    gaps = np.random.default_rng(7).exponential(1.0 / rate_hz, size=len(reqs))
+    out = {}
+    for name, active in (("continuous", 4), ("one_at_a_time", 1)):
+        srv = serve.Server(dev, max_active=active)
+        srv.submit(reqs[0]).result()          # warm-up (plan, kernels)
+        srv.results.clear()
+        futs = []
+        for r, gap in zip(reqs, gaps):
+            time.sleep(float(gap))
+            futs.append(srv.submit(r))
+        for f in futs:
+            f.result()
+        st = srv.stats()
+        srv.close()
+        out[name] = {"p50_ms": round(st["p50_s"] * 1e3, 2), "p99_ms": round(st["p99_s"] * 1e3, 2),
+                     "throughput_gcs": round(st["throughput_gcs"], 3), "peak_active": st["peak_active"]}
+    torch.cuda.empty_cache()
+    return {"requests": len(reqs), "arrivals": "Poisson %.0f/s" % rate_hz,
+            "unit": "Gcell-steps/s of solver steps (forward and adjoint steps each counted)", **out}
 
 
 # ---------------------------------------------------------------------------

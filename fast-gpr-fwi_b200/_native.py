@@ -147,7 +147,7 @@ class Plan:
     """A planned solve geometry with its bound device workspace."""
 
     def __init__(self, nx, ny, shots, nt, th, dx32, dt32, src: np.ndarray, rx: np.ndarray,
-                 srcw: np.ndarray, pml: Optional[np.ndarray], device, tuning=None):
+                 srcw: np.ndarray, pml: Optional[np.ndarray], device, tuning=None, bind: bool = True):
         L = lib()
         self.device = torch.device(device)
         self.nx, self.ny, self.shots, self.nt, self.th = int(nx), int(ny), int(shots), int(nt), int(th)
@@ -180,9 +180,17 @@ class Plan:
         check(L.fg_plan_hist_shape(handle, shape))
         self.hist_shape = tuple(int(v) for v in shape)   # (nt, groups, nx, pitch, slots)
         self.hist_floats = int(np.prod(self.hist_shape))
-        nbytes = int(L.fg_plan_workspace_bytes(handle))
-        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
-        check(L.fg_plan_bind(handle, self.workspace.data_ptr(), nbytes, stream_handle(self.device)))
+        self.workspace_bytes = int(L.fg_plan_workspace_bytes(handle))
+        self.workspace = None
+        if bind:
+            self.bind()
+
+    def bind(self):
+        """Allocate the device workspace and upload the plan's tables."""
+        if self.workspace is None:
+            self.workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=self.device)
+            check(lib().fg_plan_bind(self._h, self.workspace.data_ptr(), self.workspace_bytes,
+                                     stream_handle(self.device)))
 
     @property
     def handle(self):

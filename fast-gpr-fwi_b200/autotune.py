@@ -1,0 +1,102 @@
+"""Launch-shape autotuner.
+
+The step kernels come in several shapes (lane march or tensor-map tile
+pipeline; rows per tile, warps per block, pipeline stages), and which one is
+fastest depends on the grid, the shot count and the CPML thickness.  The
+autotuner plans the same geometry with a truncated run of `probe_steps`
+steps, times the forward step of every forward candidate and the adjoint
+step of every adjoint candidate with CUDA events, and returns the fastest
+pair as one fg_tuning dict (the adjoint runs on its own plan, so the two are
+chosen independently).  Results are cached per (device, grid, shots, CPML
+thickness).  Every shape computes the same bits, so tuning changes speed
+only.
+"""
+from __future__ import annotations
+
+import itertools
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _native
+
+_CACHE: Dict[Tuple, dict] = {}
+
+FWD_SHOT = [dict(kernel=1, rows_per_tile=ti) for ti in (2, 4, 6)] + \
+           [dict(kernel=0, rows_per_tile=8, warps_per_block=4, stages=s) for s in (2, 3)]
+ADJ_SHOT = [dict(adj_kernel=1, adj_rows_per_tile=ti, adj_warps_per_block=4, adj_stages=s)
+            for ti, s in ((8, 2), (8, 3), (4, 2))] + [dict(adj_kernel=2, adj_rows_per_tile=4)]
+FWD_COL = [dict(kernel=0, rows_per_tile=ti, warps_per_block=min(ti, 4)) for ti in (4, 8)] + \
+          [dict(kernel=1, rows_per_tile=4)]
+ADJ_COL = [dict(adj_kernel=1, adj_rows_per_tile=ti, adj_warps_per_block=min(ti, 4)) for ti in (4, 8)] + \
+          [dict(adj_kernel=2, adj_rows_per_tile=4)]
+
+
+def _probe_plan(setup, device, tuning, steps):
+    s = setup
+    pml = s.profile.packed() if s.profile is not None else None
+    return _native.Plan(s.nx, s.ny, s.shots, steps, s.th, s.dx, s.dt32, s.src.cpu().numpy(), s.rx.cpu().numpy(),
+                        np.ascontiguousarray(s.srcw[:, :steps]), pml, device, tuning)
+
+
+def _time_ms(fn, reps):
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    fn()
+    best = None
+    for _ in range(reps):
+        ev[0].record()
+        fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        t = ev[0].elapsed_time(ev[1])
+        best = t if best is None else min(best, t)
+    return best
+
+
+def autotune(device, setup, er, se, mr, probe_steps: int = 64, reps: int = 2, lanes: Optional[int] = None) -> dict:
+    """The fastest launch shape for this geometry (an fg_tuning dict).
+    er/se/mr: (nx, ny) float32 device models (any plausible model will do:
+    the kernels' speed does not depend on the values)."""
+    device = torch.device(device)
+    shot = setup.shots >= 8 if lanes is None else lanes == 1
+    key = (torch.cuda.get_device_name(device), setup.nx, setup.ny, setup.shots, setup.th, shot)
+    if key in _CACHE:
+        return dict(_CACHE[key])
+    steps = max(8, min(int(probe_steps), setup.nt))
+    base = dict(lanes=1 if shot else 2, cells_per_thread=4 if shot else 2)
+    S, nx, ny = setup.shots, setup.nx, setup.ny
+    fwd_c, adj_c = (FWD_SHOT, ADJ_SHOT) if shot else (FWD_COL, ADJ_COL)
+    best_f = best_a = None
+    for f, a in itertools.product(fwd_c, adj_c[:1]):
+        tu = dict(base, **f, **a)
+        try:
+            p = _probe_plan(setup, device, tu, steps)
+        except _native.FastGprError:
+            continue
+        tr = torch.empty((S, steps, p.nrx), device=device)
+        h = p.new_hist()
+        t = _time_ms(lambda: p.forward(er, se, mr, tr, h), reps)
+        if best_f is None or t < best_f[0]:
+            best_f = (t, f)
+        del p, h
+    resid = torch.zeros((S, steps, max(1, int(setup.rx.shape[1]))), device=device)
+    for a in adj_c:
+        tu = dict(base, **best_f[1], **a)
+        try:
+            p = _probe_plan(setup, device, tu, steps)
+        except _native.FastGprError:
+            continue
+        tr = torch.empty((S, steps, p.nrx), device=device)
+        h = p.new_hist()
+        p.forward(er, se, mr, tr, h)
+        ge = torch.empty((nx, ny), device=device)
+        gs = torch.empty_like(ge)
+        t = _time_ms(lambda: p.adjoint_reference(er, se, mr, h, resid[:, :, :p.nrx], ge, gs), reps)
+        if best_a is None or t < best_a[0]:
+            best_a = (t, a)
+        del p, h
+    torch.cuda.empty_cache()
+    tuning = dict(base, **best_f[1], **best_a[1])
+    _CACHE[key] = dict(tuning)
+    return tuning

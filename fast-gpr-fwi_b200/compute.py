@@ -78,7 +78,7 @@ class Solve:
     """One planned forward/adjoint solve: geometry, plan and workspace."""
 
     def __init__(self, device, setup: SolveSetup, tuning: Optional[dict] = None, tv: bool = True,
-                 tv_weight: float = 0.01, adjoint: str = "reference", checkpoint=None):
+                 tv_weight: float = 0.01, adjoint: str = "reference", checkpoint=None, bind: bool = True):
         if adjoint not in ("reference",):
             raise ValueError("adjoint must be 'reference'")
         self.device = torch.device(device)
@@ -89,9 +89,17 @@ class Solve:
         self.tv_weight = tv_weight
         self.adjoint = adjoint
         s = setup
+        if isinstance(tuning, str):
+            if tuning != "auto":
+                raise ValueError("tuning must be a dict, None or 'auto'")
+            from .autotune import autotune
+            ones = torch.ones((s.nx, s.ny), dtype=torch.float32, device=self.device)
+            tuning = autotune(self.device, s, 4 * ones, 1e-3 * ones, ones)
+        self.tuning = tuning
         pml = s.profile.packed() if s.profile is not None else None
         self.plan = _native.Plan(s.nx, s.ny, s.shots, s.nt, s.th, s.dx, s.dt32,
-                                 s.src.cpu().numpy(), s.rx.cpu().numpy(), s.srcw, pml, self.device, tuning)
+                                 s.src.cpu().numpy(), s.rx.cpu().numpy(), s.srcw, pml, self.device, tuning,
+                                 bind=bind)
         self.interval = checkpoint_interval(self.plan, checkpoint)
 
     def materials(self, er, se, mr):
@@ -184,6 +192,9 @@ def compute(device, dx, ny, nx, nz, source, source_apmlitudes, step, er, se, mr,
     reference does; an int K keeps the solver state every K steps instead and
     recomputes the history segment by segment during the backward pass (one
     extra forward solve, same results bit for bit); True picks K.
+    ``tuning`` (not in the reference): None = default launch shapes, a dict of
+    fg_tuning fields, or 'auto' = the fastest shapes for this geometry
+    measured on a truncated run (autotune.py, cached per geometry).
     """
     if pml_formulation != 'HORIPML':
         raise ValueError("only the HORIPML formulation is implemented (as in the reference)")

@@ -1,0 +1,227 @@
+"""Serving: continuous batching of forward and gradient solves on one GPU.
+
+Requests (a survey geometry as compute()'s keyword arguments, a model, and
+for a gradient the residual at the receivers) arrive at any time.  A request
+is admitted as soon as its device footprint fits in what is left of the HBM
+budget -- its plans' workspaces, its traces and gradients, and either the
+whole Ez history or, when that does not fit, checkpoints plus one history
+segment (the checkpointed solve, bit-identical results).  Admitted requests
+run side by side, each on a CUDA stream of its own driven by a worker
+thread (the library's launches release the GIL), so requests that arrive
+while others are on the GPU overlap with them on the device.  Every result
+is computed by the same kernels in the same order as the request alone, so
+it is the same alone and in the mix, bit for bit.
+
+The reference has no serving path (one compute() call at a time, each
+rebuilding its grid); this is the request loop north_star's serving
+configuration asks for.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+import torch
+
+from .compute import Solve, checkpoint_interval
+from .grid import build_setup
+
+
+@dataclass
+class Request:
+    """One solve.  kwargs: compute()'s geometry arguments (no er/se/mr);
+    er, se, mr: (nx, ny) or (nx, ny, 1) models; resid: (shots, nt, nrx) for a
+    gradient (None: forward only)."""
+    kwargs: dict
+    er: torch.Tensor
+    se: torch.Tensor
+    mr: torch.Tensor
+    resid: Optional[torch.Tensor] = None
+    tuning: Optional[dict] = None
+
+
+@dataclass
+class Result:
+    traces: torch.Tensor
+    grad_eps: Optional[torch.Tensor]
+    grad_sig: Optional[torch.Tensor]
+    cell_steps: int
+    bytes_reserved: int
+    checkpoint: Optional[int]
+    submitted: float = 0.0
+    started: float = 0.0
+    finished: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.submitted
+
+
+@dataclass
+class _Job:
+    req: Request
+    fut: cf.Future
+    submitted: float
+    solve: Optional[Solve] = None
+    need: int = 0
+    interval: Optional[int] = None
+
+
+def _setup(device, req: Request):
+    kw = req.kwargs
+    er = torch.clamp(torch.as_tensor(req.er, device=device, dtype=torch.float32), min=1)
+    if er.dim() == 2:
+        er = er[:, :, None]
+    mr = torch.as_tensor(req.mr, device=device, dtype=torch.float32)
+    if mr.dim() == 2:
+        mr = mr[:, :, None]
+    return build_setup(device, kw["dx"], kw["ny"], kw["nx"], kw.get("nz", 1), kw.get("time_windows"),
+                       kw.get("source", ["hertzian", "z"]), kw.get("source_location"), kw.get("source_step"),
+                       kw.get("receiver_location"), kw.get("receiver_step"), kw.get("pmlthick", 0),
+                       kw["source_apmlitudes"], kw["step"], er, mr, kw["nsrc"], kw["nrx"], kw.get("dt"),
+                       kw.get("freq"), kw.get("total_step"), kw.get("Fixedreceiver", False),
+                       kw.get("customsource"), kw.get("customreceiver"))
+
+
+class Server:
+    """Admits requests by an HBM budget and runs the admitted ones concurrently.
+
+    hbm_budget: bytes the server may hold on the device (default: 90% of the
+    free memory when the server starts); max_active: requests on the GPU at
+    once (streams / worker threads)."""
+
+    def __init__(self, device="cuda:0", hbm_budget: Optional[int] = None, max_active: int = 4):
+        self.device = torch.device(device)
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = int(free * 0.9)
+        self.budget = int(hbm_budget)
+        self.used = 0
+        self.max_active = int(max_active)
+        self.active = 0
+        self.peak_active = 0
+        self._queue: list = []
+        self._lock = threading.Condition()
+        self._pool = cf.ThreadPoolExecutor(max_workers=self.max_active)
+        self._closed = False
+        self.results: list = []
+
+    # -- admission ----------------------------------------------------------
+    def _plan(self, job: _Job) -> None:
+        """Host-side plan of a job (no device memory yet) and its footprint."""
+        req = job.req
+        setup = _setup(self.device, req)
+        solve = Solve(self.device, setup, tuning=req.tuning, tv=False, bind=False)
+        p = solve.plan
+        S, nt, nrx = setup.shots, setup.nt, p.nrx
+        fixed = p.workspace_bytes + 4 * S * nt * nrx + (8 * setup.nx * setup.ny if req.resid is not None else 0)
+        full = fixed + 4 * p.hist_floats
+        job.interval = None
+        if req.resid is not None and full > self.budget:
+            k = checkpoint_interval(p, True)
+            job.interval = k
+            full = fixed + max(0, p.checkpoint_bytes(k)) + 4 * k * (p.hist_floats // nt)
+        elif req.resid is None:
+            full = fixed                            # a forward alone keeps no history
+        job.solve = solve
+        job.need = full
+
+    def submit(self, req: Request) -> cf.Future:
+        """Queue a request; the future resolves to a Result."""
+        job = _Job(req, cf.Future(), time.perf_counter())
+        self._plan(job)
+        if job.need > self.budget:
+            job.fut.set_exception(MemoryError("request needs %d bytes, budget %d" % (job.need, self.budget)))
+            return job.fut
+        with self._lock:
+            if self._closed:
+                raise RuntimeError("server closed")
+            self._queue.append(job)
+            self._admit_locked()
+        return job.fut
+
+    def _admit_locked(self) -> None:
+        # first come, first served; a request waits until its bytes fit
+        while self._queue and self.active < self.max_active and self.used + self._queue[0].need <= self.budget:
+            job = self._queue.pop(0)
+            self.used += job.need
+            self.active += 1
+            self.peak_active = max(self.peak_active, self.active)
+            self._pool.submit(self._run, job)
+
+    def _release(self, job: _Job) -> None:
+        with self._lock:
+            self.used -= job.need
+            self.active -= 1
+            self._admit_locked()
+            self._lock.notify_all()
+
+    # -- execution ----------------------------------------------------------
+    def _run(self, job: _Job) -> None:
+        try:
+            started = time.perf_counter()
+            stream = torch.cuda.Stream(self.device)
+            with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                res = self._solve(job)
+                stream.synchronize()
+            res.submitted, res.started, res.finished = job.submitted, started, time.perf_counter()
+            job.solve = None
+            with self._lock:
+                self.results.append(res)
+            job.fut.set_result(res)
+        except Exception as e:   # delivered to the caller through the future
+            job.fut.set_exception(e)
+        finally:
+            self._release(job)
+
+    def _solve(self, job: _Job) -> Result:
+        req, solve = job.req, job.solve
+        p = solve.plan
+        p.bind()
+        s = solve.setup
+        er, se, mr = solve.materials(torch.clamp(torch.as_tensor(req.er, device=self.device), min=1),
+                                     torch.clamp(torch.as_tensor(req.se, device=self.device), min=0),
+                                     torch.as_tensor(req.mr, device=self.device))
+        S, nt, nrx = s.shots, s.nt, p.nrx
+        traces = torch.empty((S, nt, nrx), dtype=torch.float32, device=self.device)
+        ge = gs = None
+        if req.resid is None:
+            p.forward(er, se, mr, traces, None)
+        else:
+            resid = torch.as_tensor(req.resid, device=self.device, dtype=torch.float32).contiguous()
+            ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
+            gs = torch.empty_like(ge)
+            if job.interval is None:
+                hist = p.new_hist()
+                p.forward(er, se, mr, traces, hist)
+                p.adjoint_reference(er, se, mr, hist, resid, ge, gs)
+            else:
+                ck = p.new_checkpoints(job.interval)
+                seg = p.new_segment(job.interval)
+                p.forward_checkpointed(er, se, mr, traces, ck, job.interval)
+                p.adjoint_reference_checkpointed(er, se, mr, ck, job.interval, seg, resid, ge, gs)
+        cells = s.nx * s.ny * S * nt * (2 if req.resid is not None else 1)
+        return Result(traces, ge, gs, cells, job.need, job.interval)
+
+    # -- reporting ----------------------------------------------------------
+    def close(self, wait: bool = True) -> None:
+        with self._lock:
+            self._closed = True
+        self._pool.shutdown(wait=wait)
+
+    def stats(self) -> dict:
+        """p50 / p99 latency (s) and throughput (Gcell-steps/s) over the results so far."""
+        with self._lock:
+            res = list(self.results)
+        if not res:
+            return {}
+        lat = np.array([r.latency for r in res])
+        span = max(r.finished for r in res) - min(r.submitted for r in res)
+        cells = sum(r.cell_steps for r in res)
+        return {"requests": len(res), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "throughput_gcs": cells / span / 1e9 if span > 0 else float("nan"),
+                "peak_active": self.peak_active}

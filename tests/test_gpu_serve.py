@@ -1,0 +1,73 @@
+"""Serving (fast-gpr-fwi_b200/serve.py): a mixed stream of forward and
+gradient requests of different sizes, admitted by an HBM budget and run
+concurrently, gives every request the result it gets alone, bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(fg):
+    serve = __import__("importlib").import_module("fast-gpr-fwi_b200.serve")
+    out = []
+    shapes = [(48, 40, 3, 120, 6), (64, 56, 9, 90, 6), (40, 56, 2, 150, 5), (56, 48, 12, 100, 6),
+              (48, 40, 1, 200, 6), (72, 64, 5, 80, 8)]
+    for n, (nx, ny, shots, nt, pml) in enumerate(shapes):
+        wl = fg.workloads.small(seed=10 + n, nx=nx, ny=ny, shots=shots, nt=nt, pml=pml, fixed=True)
+        wl.source_step = [0.03, 0.01, 0.0]
+        kw = wl.kwargs("cuda")
+        for k in ("er", "se", "mr", "device", "tv"):
+            kw.pop(k)
+        rng = np.random.default_rng(n)
+        resid = None
+        if n % 2 == 0:
+            resid = torch.tensor(rng.standard_normal((shots, nt, wl.nrx)).astype(np.float32) * 1e-3)
+        out.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid))
+    return serve, out
+
+
+def _arrays(res):
+    return [None if t is None else t.cpu().numpy() for t in (res.traces, res.grad_eps, res.grad_sig)]
+
+
+def test_results_same_alone_and_in_the_mix(fg):
+    serve, reqs = _requests(fg)
+    alone = []
+    for r in reqs:
+        srv = serve.Server("cuda:0", max_active=1)
+        alone.append(_arrays(srv.submit(r).result()))
+        srv.close()
+    srv = serve.Server("cuda:0", max_active=4)
+    futs = [srv.submit(r) for r in reqs + reqs]
+    mixed = [f.result() for f in futs]
+    st = srv.stats()
+    srv.close()
+    assert st["requests"] == 2 * len(reqs) and st["peak_active"] >= 2
+    assert st["p99_s"] >= st["p50_s"] > 0
+    for k, res in enumerate(mixed):
+        for a, b in zip(alone[k % len(reqs)], _arrays(res)):
+            if a is None:
+                assert b is None
+            else:
+                assert np.array_equal(a, b)
+
+
+def test_budget_admission_and_checkpoint_fallback(fg):
+    serve, reqs = _requests(fg)
+    grad = reqs[2]                    # a gradient request
+    srv = serve.Server("cuda:0", max_active=2)
+    full = srv.submit(grad).result()
+    srv.close()
+    # a budget below the full-history footprint: the gradient takes the checkpointed solve, same bits
+    tight = serve.Server("cuda:0", hbm_budget=int(full.bytes_reserved * 0.6), max_active=2)
+    ck = tight.submit(grad).result()
+    tight.close()
+    assert full.checkpoint is None and ck.checkpoint is not None and ck.bytes_reserved < full.bytes_reserved
+    for a, b in zip(_arrays(full), _arrays(ck)):
+        assert np.array_equal(a, b)
+    # a budget too small for any form of the request is refused
+    tiny = serve.Server("cuda:0", hbm_budget=1 << 20, max_active=1)
+    with pytest.raises(MemoryError):
+        tiny.submit(grad).result()
+    tiny.close()
