@@ -11,6 +11,12 @@ tensor torch's L1Loss backward would build is never materialised.
 
 With the same inputs an epoch produces the gradients the notebook's
 compute() + L1Loss + backward() produce (tests/test_gpu_fwi.py).
+
+graph=True captures an epoch's solve -- the coefficient kernels, state
+resets, 2 nt - 1 step launches and the gradient reductions -- in a CUDA graph
+with static model, trace and gradient buffers, and replays it every epoch
+after copying the current models in; the graph is captured again when the
+plan is rebuilt.  Replays compute the eager solve's bits.
 """
 from __future__ import annotations
 
@@ -37,7 +43,7 @@ class Inversion:
     def __init__(self, device, kwargs: dict, observed: torch.Tensor, er0: torch.Tensor, se0: torch.Tensor,
                  mr: torch.Tensor, phase1_epochs: int = 50, lr: Sequence[float] = (0.2, 0.1, 1e-4),
                  loss_weight: float = 100.0, tv: bool = True, tv_weight: float = 0.01,
-                 tuning: Optional[dict] = None):
+                 tuning: Optional[dict] = None, graph: bool = False):
         self.device = torch.device(device)
         kw = dict(kwargs)
         self.pml = int(kw.get("pmlthick", 0))
@@ -51,6 +57,8 @@ class Inversion:
         self.opt2 = torch.optim.Adam([{"params": self.er, "lr": lr[1]}, {"params": self.se, "lr": lr[2]}])
         self.kw = kw
         self.solve_args = dict(tuning=tuning, tv=tv, tv_weight=tv_weight)
+        self.use_graph = bool(graph)
+        self._graph = None
         self._row0 = None
         self._plan_for(torch.clamp(self.er.detach(), min=1))
         setup = self.setup
@@ -77,6 +85,40 @@ class Inversion:
                                  kw.get("customsource"), kw.get("customreceiver"))
         self.solve = Solve(self.device, self.setup, **self.solve_args)
         self._row0 = row0.clone()
+        self._graph = None
+        s, p = self.setup, self.solve.plan
+        # static buffers of the solve (the graph's inputs and outputs)
+        self._e32 = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
+        self._s32 = torch.empty_like(self._e32)
+        self._m32 = self.solve.materials(self.mr, self.mr, self.mr)[2]
+        self._traces = torch.empty((s.shots, s.nt, p.nrx), dtype=torch.float32, device=self.device)
+        self._hist = p.new_hist()
+        self._ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
+        self._gs = torch.empty_like(self._ge)
+
+    def _solve_into_static(self) -> None:
+        """Forward + fused L1 adjoint on the static buffers (eagerly or as a graph replay)."""
+        p = self.solve.plan
+
+        def run():
+            p.forward(self._e32, self._s32, self._m32, self._traces, self._hist)
+            p.adjoint_reference_l1(self._e32, self._s32, self._m32, self._hist, self._traces, self.observed,
+                                   self.scale, self._ge, self._gs)
+
+        if not self.use_graph:
+            run()
+            return
+        if self._graph is None:
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(side):
+                run()                                  # warm-up: launch shapes and occupancy are cached here
+            torch.cuda.current_stream(self.device).wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                run()
+            self._graph = g
+        self._graph.replay()
 
     def epoch(self) -> float:
         """One epoch: forward, loss, fused adjoint, border zeroing, Adam step.
@@ -87,18 +129,13 @@ class Inversion:
         er_c = torch.clamp(self.er, min=1)          # compute() clamps its inputs (autograd keeps the mask)
         se_c = torch.clamp(self.se, min=0)
         self._plan_for(er_c)
-        s = self.setup
-        plan = self.solve.plan
-        e32, s32, m32 = self.solve.materials(er_c.detach(), se_c.detach(), self.mr)
-        traces = torch.empty((s.shots, s.nt, plan.nrx), dtype=torch.float32, device=self.device)
-        hist = plan.new_hist()
-        plan.forward(e32, s32, m32, traces, hist)
-        loss = (traces - self.observed).abs().mean() * self.loss_weight
-        ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
-        gs = torch.empty_like(ge) if phase2 else None
-        plan.adjoint_reference_l1(e32, s32, m32, hist, traces, self.observed, self.scale, ge, gs)
-        del hist
-        ge = ge.view(er_c.shape)
+        e32, s32, _ = self.solve.materials(er_c.detach(), se_c.detach(), self.mr)
+        self._e32.copy_(e32)
+        self._s32.copy_(s32)
+        self._solve_into_static()
+        loss = (self._traces - self.observed).abs().mean() * self.loss_weight
+        ge = self._ge.clone().view(er_c.shape)
+        gs = self._gs.clone() if phase2 else None
         if self.solve.tv:
             lam = self.solve.tv_weight
             ge = ge + lam * (2 * (er_c.detach() - total_variation(er_c.detach().clone())))

@@ -12,16 +12,15 @@ while others are on the GPU overlap with them on the device.  Every result
 is computed by the same kernels in the same order as the request alone, so
 it is the same alone and in the mix, bit for bit.
 
-The reference has no serving path (one compute() call at a time, each
-rebuilding its grid); this is the request loop north_star's serving
-configuration asks for.
+The reference has no serving path: one compute() call at a time, each
+rebuilding its grid.
 """
 from __future__ import annotations
 
 import concurrent.futures as cf
 import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Optional
 
 import numpy as np

@@ -71,3 +71,19 @@ def test_inversion_reduces_misfit(fg):
     inv = fg.Inversion(dev, kw, obs, er0, se0, mr, phase1_epochs=3)
     losses = [inv.epoch() for _ in range(6)]
     assert losses[-1] < losses[0]
+
+
+def test_inversion_graph_replay_equals_eager(fg):
+    """The epoch's solve captured in a CUDA graph and replayed gives the eager bits."""
+    wl, dev, obs, er0, se0, mr = _problem(fg)
+    kw = wl.kwargs(dev, tv=True)
+    for k in ("er", "se", "mr", "tv", "device"):
+        kw.pop(k)
+    runs = []
+    for graph in (False, True):
+        inv = fg.Inversion(dev, kw, obs, er0, se0, mr, phase1_epochs=2, graph=graph)
+        losses = [inv.epoch() for _ in range(4)]
+        runs.append((losses, inv.er.detach().cpu().numpy(), inv.se.detach().cpu().numpy(), inv._graph is not None))
+    assert runs[0][0] == runs[1][0]
+    assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][2], runs[1][2])
+    assert runs[1][3] and not runs[0][3]
