@@ -879,6 +879,40 @@ int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
     return FG_OK;
 }
 
+// The division check depends only on the divisor (and the device's
+// arithmetic), so each (device, divisor) is checked once per process; the
+// result (*dinv_out) is RN(1/d) when div_d may use its reciprocal step, else 0.
+static int div_check(float d, cudaStream_t st, int* bad, float* dinv_out) {
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<int, unsigned>, float>> cache;
+    int dev = 0;
+    FG_CUDA(cudaGetDevice(&dev));
+    unsigned bits;
+    std::memcpy(&bits, &d, 4);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (auto& e : cache)
+            if (e.first.first == dev && e.first.second == bits) {
+                *dinv_out = e.second;
+                return FG_OK;
+            }
+    }
+    const float dinv = 1.0f / d;
+    float c = 0.f;
+    if (d >= 0x1p-30f && d <= 0x1p30f && std::fabs((double)d * (double)dinv - 1.0) < 0x1p-25) {
+        int nbad = -1;
+        fg::k_div_check<<<512, 256, 0, st>>>(d, dinv, bad);
+        FG_CUDA(cudaGetLastError());
+        FG_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        FG_CUDA(cudaStreamSynchronize(st));
+        if (nbad == 0) c = dinv;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    cache.push_back({{dev, bits}, c});
+    *dinv_out = c;
+    return FG_OK;
+}
+
 static int bind_one(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     if (!p) return fail(FG_ERR_INVALID, "fg_plan_bind: NULL plan");
     if (!workspace || bytes < (int64_t)p->total) return fail(FG_ERR_WORKSPACE, "workspace missing or too small");
@@ -908,19 +942,10 @@ static int bind_one(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     // division by the cell size: the reciprocal step of div_d is enabled when
     // it returns __fdiv_rn's bits for every significand (one binade decides all)
     {
-        const float d = p->dx, dinv = 1.0f / p->dx;
-        p->dinv = 0.f;
-        if (d >= 0x1p-30f && d <= 0x1p30f && std::fabs((double)d * (double)dinv - 1.0) < 0x1p-25) {
-            int* bad = (int*)(p->ws + p->o_err) + 2;
-            fg::k_div_check<<<512, 256, 0, st>>>(d, dinv, bad);
-            FG_CUDA(cudaGetLastError());
-            int nbad = -1;
-            FG_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-            FG_CUDA(cudaStreamSynchronize(st));
-            if (nbad == 0) p->dinv = dinv;
-        }
-        p->g.dinv = p->dinv;
+        const int rc = div_check(p->dx, st, (int*)(p->ws + p->o_err) + 2, &p->dinv);
+        if (rc) return rc;
     }
+    p->g.dinv = p->dinv;
     if (p->kernel == 0) {
         const int rc = encode_tile_maps(p);
         if (rc) return rc;
