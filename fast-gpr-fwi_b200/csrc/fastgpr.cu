@@ -70,6 +70,7 @@ struct fg_plan {
     int fwd_blocks = 0, adj_blocks = 0;
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
     float dinv = 0.f;
+    int div_scaled = 0;   // the scaled step matches __fdiv_rn for every |x| < 2^31 (checked at bind)
     // the adjoint's own plan (own state, coefficients, accumulators and launch
     // shape); its workspace follows this plan's in the caller's workspace
     fg_plan* adj = nullptr;
@@ -242,7 +243,7 @@ void fill_grid(fg_plan* p) {
     char* w = p->ws;
     g.nx = p->nx; g.ny = p->ny; g.P = p->P; g.th = p->th; g.TY = p->TY;
     g.S = p->S; g.nt = p->nt; g.nrx = p->nrx; g.Ph = p->Ph; g.ngroups = p->ngroups;
-    g.d = p->dx; g.dt = p->dt; g.dinv = p->dinv;
+    g.d = p->dx; g.dt = p->dt; g.dinv = p->dinv; g.div_scaled = p->div_scaled;
     g.plane = p->plane; g.pxs = p->pxs; g.pys = p->pys;
     const long long cplane = (long long)(p->nx + 1) * p->P;
     float* coef = (float*)(w + p->o_coef);
@@ -879,12 +880,15 @@ int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
     return FG_OK;
 }
 
-// The division check depends only on the divisor (and the device's
-// arithmetic), so each (device, divisor) is checked once per process; the
-// result (*dinv_out) is RN(1/d) when div_d may use its reciprocal step, else 0.
-static int div_check(float d, cudaStream_t st, int* bad, float* dinv_out) {
+// The division checks depend only on the divisor (and the device's
+// arithmetic), so each (device, divisor) is checked once per process.
+//   dinv:   RN(1/d) when div_d may use its reciprocal step (every significand
+//           of one binade matches __fdiv_rn), else 0
+//   scaled: div_d_scaled matches __fdiv_rn for every |x| < 2^31
+struct DivCheck { float dinv; int scaled; };
+static int div_check(float d, cudaStream_t st, int* bad, DivCheck* out) {
     static std::mutex mu;
-    static std::vector<std::pair<std::pair<int, unsigned>, float>> cache;
+    static std::vector<std::pair<std::pair<int, unsigned>, DivCheck>> cache;
     int dev = 0;
     FG_CUDA(cudaGetDevice(&dev));
     unsigned bits;
@@ -893,23 +897,30 @@ static int div_check(float d, cudaStream_t st, int* bad, float* dinv_out) {
         std::lock_guard<std::mutex> lk(mu);
         for (auto& e : cache)
             if (e.first.first == dev && e.first.second == bits) {
-                *dinv_out = e.second;
+                *out = e.second;
                 return FG_OK;
             }
     }
     const float dinv = 1.0f / d;
-    float c = 0.f;
+    DivCheck c{0.f, 0};
     if (d >= 0x1p-30f && d <= 0x1p30f && std::fabs((double)d * (double)dinv - 1.0) < 0x1p-25) {
-        int nbad = -1;
+        int nbad[2] = {-1, -1};
+        int sms = 0;
+        FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         fg::k_div_check<<<512, 256, 0, st>>>(d, dinv, bad);
         FG_CUDA(cudaGetLastError());
-        FG_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
+        fg::k_div_check_scaled<<<sms * 8, 256, 0, st>>>(d, dinv, bad + 1);
+        FG_CUDA(cudaGetLastError());
+        FG_CUDA(cudaMemcpyAsync(nbad, bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
         FG_CUDA(cudaStreamSynchronize(st));
-        if (nbad == 0) c = dinv;
+        if (nbad[0] == 0) {
+            c.dinv = dinv;
+            c.scaled = nbad[1] == 0;
+        }
     }
     std::lock_guard<std::mutex> lk(mu);
     cache.push_back({{dev, bits}, c});
-    *dinv_out = c;
+    *out = c;
     return FG_OK;
 }
 
@@ -941,11 +952,17 @@ static int bind_one(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_err, 0, sizeof(int) * 4, st));
     // division by the cell size: the reciprocal step of div_d is enabled when
     // it returns __fdiv_rn's bits for every significand (one binade decides all)
+    // The scaled step of the shot-lane CPML rows is enabled when it returns
+    // __fdiv_rn's bits for every |x| < 2^31.
     {
-        const int rc = div_check(p->dx, st, (int*)(p->ws + p->o_err) + 2, &p->dinv);
+        DivCheck c;
+        const int rc = div_check(p->dx, st, (int*)(p->ws + p->o_err) + 2, &c);
         if (rc) return rc;
+        p->dinv = c.dinv;
+        p->div_scaled = c.scaled;
     }
     p->g.dinv = p->dinv;
+    p->g.div_scaled = p->div_scaled;
     if (p->kernel == 0) {
         const int rc = encode_tile_maps(p);
         if (rc) return rc;

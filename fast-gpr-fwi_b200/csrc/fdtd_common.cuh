@@ -49,6 +49,7 @@ struct Dev {
     int ngroups;         // shot groups
     float d;             // cell size (CPML derivative divisor)
     float dinv;          // RN(1/d) when div_d may use it (checked at bind), else 0
+    int div_scaled;      // div_d_scaled is __fdiv_rn for every |x| < 2^31 (checked at bind)
     float dt;            // time step (sigma imaging factor)
     long long plane;     // floats of one group's plane of one field
     long long pxs, pys;  // floats of one group's x-slab / y-slab auxiliaries
@@ -239,6 +240,16 @@ __device__ __forceinline__ float div_d_step(float x, float d, float dinv) {
     const float q = __fmul_rn(x, dinv);
     const float r = __fmaf_rn(-q, d, x);
     return __fmaf_rn(r, dinv, q);
+}
+// The step on x * 2^59, scaled back by 2^-59.  For |x| < 2^31 the scaled
+// argument is zero or lies in [2^-90, 2^90), where the step is the correctly
+// rounded quotient, so no test of x is needed below 2^31; scaling back is
+// exact unless the quotient is subnormal, where the two roundings may differ
+// from one (the bind-time check, k_div_check_scaled, decides per divisor).
+// For x = -0 the step gives +0: the sign of x goes back on (a no-op for every
+// other x, as d > 0).
+__device__ __forceinline__ float div_d_scaled(float x, float d, float dinv) {
+    return copysignf(__fmul_rn(div_d_step(__fmul_rn(x, 0x1p59f), d, dinv), 0x1p-59f), x);
 }
 __device__ __forceinline__ float div_d(const Dev& g, float x) {
     if (g.dinv != 0.f) {
@@ -587,6 +598,21 @@ __global__ void k_div_check(float d, float dinv, int* bad) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < (1 << 23); m += gridDim.x * blockDim.x) {
         const float x = __int_as_float(0x3f800000 | m);
         n += __float_as_int(div_d_step(x, d, dinv)) != __float_as_int(__fdiv_rn(x, d));
+    }
+    if (n) atomicAdd(bad, n);
+}
+
+// Check of div_d_scaled against __fdiv_rn for every x with |x| < 2^31 (bit
+// patterns 0 .. 0x4effffff and their negatives): bad[0] counts the
+// mismatches.
+__global__ void k_div_check_scaled(float d, float dinv, int* bad) {
+    int n = 0;
+    const long long total = 0x4f000000ll;
+    for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < total;
+         m += (long long)gridDim.x * blockDim.x) {
+        const float x = __int_as_float((int)m);
+        n += __float_as_int(div_d_scaled(x, d, dinv)) != __float_as_int(__fdiv_rn(x, d));
+        n += __float_as_int(div_d_scaled(-x, d, dinv)) != __float_as_int(__fdiv_rn(-x, d));
     }
     if (n) atomicAdd(bad, n);
 }

@@ -141,13 +141,35 @@ __device__ __forceinline__ void st_xrun(const Dev& g, float* a, int r, int c0, u
         if (bit(own, n)) st1(g, b + n * 32, p[n]);
 }
 
+// Division of a row by the cell size, decided once per row.  div_d tests the
+// range of every x and branches per lane to __fdiv_rn; inside the unrolled
+// CPML rows those tests and branches cost more than the arithmetic.  Where
+// the plan's divisor passed k_div_check_scaled, div_d_scaled is __fdiv_rn's
+// quotient for every |x| < 2^31: one warp vote per row asks whether every
+// input the row divides is below that (NaN is not), and the row then runs
+// straight-line with div_d_scaled, or with div_d throughout.  All 32 lanes
+// are active: they are 32 shots of the same cells.
+template <int N>
+__device__ __forceinline__ bool div_row_fast(const Dev& g, uint32_t m, const float (&x)[N]) {
+    bool bad = false;
+#pragma unroll
+    for (int n = 0; n < N; ++n)
+        if (bit(m, n)) bad |= !(fabsf(x[n]) < 0x1p31f);
+    return g.div_scaled && !__any_sync(0xffffffffu, bad);
+}
+template <bool FAST>
+__device__ __forceinline__ float div_row(const Dev& g, float x) {
+    if constexpr (FAST) return div_d_scaled(x, g.d, g.dinv);
+    else return div_d(g, x);
+}
+
 // E of cells j0 .. j0+N-1 of row i from dhy / dhx (old E in ez, updated in
 // place): interior (i >= 1, j >= 1), then the CPML corrections in slab order.
 // cd / px / py are the row's loaded uE4 and auxiliaries (px, py updated).
-template <int N>
-__device__ __forceinline__ void e_shot(const Dev& g, const float* R, int i, int j0, const XRow& xe, const YRun& ye,
-                                       float (&ez)[N], const float (&dhy)[N], const float (&dhx)[N], const float* ca,
-                                       const float* cb, const float (&cd)[N], float (&px)[N], float (&py)[N]) {
+template <int N, bool FAST>
+__device__ __forceinline__ void e_shot_k(const Dev& g, const float* R, int i, int j0, const XRow& xe, const YRun& ye,
+                                         float (&ez)[N], const float (&dhy)[N], const float (&dhx)[N], const float* ca,
+                                         const float* cb, const float (&cd)[N], float (&px)[N], float (&py)[N]) {
     const int th = g.th;
     float xa = 0.f, xb = 0.f, xc = 0.f, xf = 0.f;
     if (xe.on) {
@@ -165,42 +187,59 @@ __device__ __forceinline__ void e_shot(const Dev& g, const float* R, int i, int 
         // x0 and xmax come before and after y0 in the slab order; ymax is last
         const bool late_x = xe.maxside && fy && ye.off == 0;
         if (xe.on && !late_x) {
-            const float dd = div_d(g, dhy[n]);
+            const float dd = div_row<FAST>(g, dhy[n]);
             e = __fmaf_rn(cd[n], madd2(xa, dd, xb, px[n]), e);
             px[n] = msub2(xc, px[n], xf, dd);
         }
-        if (fy) e = cpml<false>(g, e, div_d(g, dhx[n]), cd[n], py[n], R, ye.k0 + ye.dk * n);
+        if (fy) e = cpml<false>(g, e, div_row<FAST>(g, dhx[n]), cd[n], py[n], R, ye.k0 + ye.dk * n);
         if (late_x) {
-            const float dd = div_d(g, dhy[n]);
+            const float dd = div_row<FAST>(g, dhy[n]);
             e = __fmaf_rn(cd[n], madd2(xa, dd, xb, px[n]), e);
             px[n] = msub2(xc, px[n], xf, dd);
         }
         ez[n] = e;
     }
 }
+template <int N>
+__device__ __forceinline__ void e_shot(const Dev& g, const float* R, int i, int j0, const XRow& xe, const YRun& ye,
+                                       float (&ez)[N], const float (&dhy)[N], const float (&dhx)[N], const float* ca,
+                                       const float* cb, const float (&cd)[N], float (&px)[N], float (&py)[N]) {
+    if (div_row_fast<N>(g, xe.on ? ye.in : 0u, dhy) && div_row_fast<N>(g, ye.m & ye.in, dhx))
+        e_shot_k<N, true>(g, R, i, j0, xe, ye, ez, dhy, dhx, ca, cb, cd, px, py);
+    else
+        e_shot_k<N, false>(g, R, i, j0, xe, ye, ez, dhy, dhx, ca, cb, cd, px, py);
+}
 
 // Hx of cells c0 .. c0+N-1 of row i (old Hx in h, updated in place):
 // interior (i >= 1), then the y-slab correction.
-template <int N>
-__device__ __forceinline__ void hx_shot(const Dev& g, const float* R, int i, const YRun& yh, float (&h)[N],
-                                        const float (&dz)[N], const float* ch, const float (&ci)[N], float (&py)[N]) {
+template <int N, bool FAST>
+__device__ __forceinline__ void hx_shot_k(const Dev& g, const float* R, int i, const YRun& yh, float (&h)[N],
+                                          const float (&dz)[N], const float* ch, const float (&ci)[N], float (&py)[N]) {
     const float* HR = R + 4 * g.th;
 #pragma unroll
     for (int n = 0; n < N; ++n) {
         if (!bit(yh.in, n)) continue;
         float v = h[n];
         if (i >= 1) v = msub2(1.0f, v, ch[n], dz[n]);
-        if (bit(yh.m, n)) v = cpml<false>(g, v, div_d(g, dz[n]), ci[n], py[n], HR, yh.k0 + yh.dk * n);
+        if (bit(yh.m, n)) v = cpml<false>(g, v, div_row<FAST>(g, dz[n]), ci[n], py[n], HR, yh.k0 + yh.dk * n);
         h[n] = v;
     }
+}
+template <int N>
+__device__ __forceinline__ void hx_shot(const Dev& g, const float* R, int i, const YRun& yh, float (&h)[N],
+                                        const float (&dz)[N], const float* ch, const float (&ci)[N], float (&py)[N]) {
+    if (div_row_fast<N>(g, yh.m & yh.in, dz))
+        hx_shot_k<N, true>(g, R, i, yh, h, dz, ch, ci, py);
+    else
+        hx_shot_k<N, false>(g, R, i, yh, h, dz, ch, ci, py);
 }
 
 // Hy of cells j0 .. j0+N-1 of row i (validity mask `in`): interior (j >= 1),
 // then the x-slab correction (row-uniform profile index).
-template <int N>
-__device__ __forceinline__ void hy_shot(const Dev& g, const float* R, int j0, const XRow& xh, uint32_t in,
-                                        float (&h)[N], const float (&dz)[N], const float* ch, const float* ci,
-                                        float (&px)[N]) {
+template <int N, bool FAST>
+__device__ __forceinline__ void hy_shot_k(const Dev& g, const float* R, int j0, const XRow& xh, uint32_t in,
+                                          float (&h)[N], const float (&dz)[N], const float* ch, const float* ci,
+                                          float (&px)[N]) {
     const int th = g.th;
     const float* HR = R + 4 * th;
     float xa = 0.f, xb = 0.f, xc = 0.f, xf = 0.f;
@@ -216,12 +255,21 @@ __device__ __forceinline__ void hy_shot(const Dev& g, const float* R, int j0, co
         float v = h[n];
         if (j0 + n >= 1) v = madd2(1.0f, v, ch[n], dz[n]);
         if (xh.on) {
-            const float dd = div_d(g, dz[n]);
+            const float dd = div_row<FAST>(g, dz[n]);
             v = __fmaf_rn(ci[n], madd2(xa, dd, xb, px[n]), v);
             px[n] = msub2(xc, px[n], xf, dd);
         }
         h[n] = v;
     }
+}
+template <int N>
+__device__ __forceinline__ void hy_shot(const Dev& g, const float* R, int j0, const XRow& xh, uint32_t in,
+                                        float (&h)[N], const float (&dz)[N], const float* ch, const float* ci,
+                                        float (&px)[N]) {
+    if (div_row_fast<N>(g, xh.on ? in : 0u, dz))
+        hy_shot_k<N, true>(g, R, j0, xh, in, h, dz, ch, ci, px);
+    else
+        hy_shot_k<N, false>(g, R, j0, xh, in, h, dz, ch, ci, px);
 }
 
 // uE4 / uH4 of cells c0 .. c0+N-1 of row i that `need` them.

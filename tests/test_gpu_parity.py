@@ -254,3 +254,38 @@ def test_two_shot_groups_vs_oracle(fg, orc, dev, shots, tuning):
     oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
     assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
     assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
+
+
+@pytest.mark.parametrize("scale,dx", [(1e13, 0.05), (1e-20, 0.05), (1.0, 0.03)])
+@pytest.mark.parametrize("tuning", [
+    None,
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 1, "adj_rows_per_tile": 8,
+     "adj_warps_per_block": 4, "adj_stages": 2},
+])
+def test_division_ranges_vs_oracle(fg, orc, dev, scale, dx, tuning):
+    """Field values that take each branch of the CPML rows' division by the
+    cell size: derivatives of 2^31 and above (amplitude 1e13: the per-division
+    path of the shot-lane rows), fields around 1e-18 with tens of thousands of
+    subnormal values at the wavefront (the scaled step, whose double rounding
+    the bind-time check rules out for dx = 0.05), and dx = 0.03, whose scaled
+    step fails that check (subnormal quotients round differently), so its
+    rows divide per cell throughout."""
+    wl = fg.workloads.small(shots=3, nt=120, dx=dx, nx=64)
+    prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+    prob.srcw = setup.srcw = np.ascontiguousarray(setup.srcw * np.float32(scale), dtype=np.float32)
+    solve = fg.Solve(dev, setup, tv=False, tuning=tuning)
+    er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+    traces, hist = solve.forward(er, se, mr)
+    o_tr, o_hist = orc.forward(prob, np.float32)
+    assert np.isfinite(o_tr).all() and np.abs(o_tr).max() > 0
+    np.testing.assert_array_equal(traces.cpu().numpy(), o_tr)
+    np.testing.assert_array_equal(solve.plan.hist_view(hist).cpu().numpy(), o_hist)
+    # the residual scales up with a large source, never down, so that the
+    # gradients stay inside float32's normal range
+    rng = np.random.default_rng(9)
+    resid = (rng.standard_normal(traces.shape) * max(scale, 1.0)).astype(np.float32)
+    ge, gs = solve.gradient(er, se, mr, hist, torch.tensor(resid, device=dev), normalize=False)
+    oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
+    assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
+    assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
