@@ -64,7 +64,7 @@ UNIT = "Gcell-steps/s"
 # dram__bytes_write.sum of one launch on the 64-shot 440x340 grid, summarised
 # under profiles/): forward 262.0 MB, adjoint 280.5 MB per launch over
 # 64 x 440 x 340 shot-cells.
-NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 262.0e6 / (64 * 440 * 340), "adjoint": 280.5e6 / (64 * 440 * 340)}
+NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 259.6e6 / (64 * 440 * 340), "adjoint": 281.5e6 / (64 * 440 * 340)}
 
 
 def _fg():
