@@ -845,6 +845,7 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
                                                                : (at.kernel == 0 ? std::min(at.rows_per_tile, 4) : 4);
         at.stages = tune && tune->adj_stages ? tune->adj_stages : (at.kernel == 0 ? 2 : 0);
     }
+    if (tune && tune->adj_cells_per_thread) at.cells_per_thread = tune->adj_cells_per_thread;
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {

@@ -90,11 +90,14 @@ typedef struct fg_tuning {
      * name one, else the default adjoint shape (shot lanes: tile pipeline,
      * 8 rows over 4 consumer warps, 2 stages; column lanes: the forward's);
      * 1 = tile pipeline, 2 = lane march, shaped by the three fields below
-     * (0 = their defaults).  cells_per_thread and lanes are shared. */
+     * (0 = their defaults).  lanes is shared; adj_cells_per_thread (0 = the
+     * forward's cells_per_thread) sets the adjoint's own.  The Ez history
+     * layout does not depend on cells_per_thread, so the two may differ. */
     int32_t adj_kernel;
     int32_t adj_rows_per_tile;
     int32_t adj_warps_per_block;
     int32_t adj_stages;
+    int32_t adj_cells_per_thread;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;

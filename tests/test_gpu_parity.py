@@ -136,6 +136,12 @@ TUNINGS = [
     {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 1, "adj_rows_per_tile": 8,
      "adj_warps_per_block": 4, "adj_stages": 2},
     {"kernel": 0, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 8, "adj_kernel": 2, "adj_rows_per_tile": 3},
+    # the adjoint on its own cells per thread
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 2, "adj_rows_per_tile": 4,
+     "adj_cells_per_thread": 8},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 1, "adj_rows_per_tile": 4,
+     "adj_warps_per_block": 4, "adj_stages": 2, "adj_cells_per_thread": 8},
+    {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 4, "adj_kernel": 2, "adj_cells_per_thread": 4},
 ]
 
 
