@@ -64,7 +64,9 @@ UNIT = "Gcell-steps/s"
 # dram__bytes_write.sum of one launch on the 64-shot 440x340 grid, summarised
 # under profiles/): forward 262.0 MB, adjoint 280.5 MB per launch over
 # 64 x 440 x 340 shot-cells.
-NCU_BYTES_PER_SHOT_CELL_STEP = {"forward": 259.6e6 / (64 * 440 * 340), "adjoint": 281.5e6 / (64 * 440 * 340)}
+# DRAM bytes per shot-cell-step of each step kernel, from one ncu capture on the 440 x 340 grid with 64 shots
+# (read + write); a kernel with no capture reports null traffic
+NCU_BYTES_PER_SHOT_CELL_STEP = {"fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340)}
 
 
 def _fg():
@@ -124,7 +126,7 @@ def kernel_name(tuning, direction):
         k = t.get("kernel", 1)
     else:
         ak = t.get("adj_kernel", 0)
-        k = (t.get("kernel", 1) if t else 0) if ak == 0 else (0 if ak == 1 else 1)
+        k = (t.get("kernel", 1) if t else 1) if ak == 0 else (0 if ak == 1 else 1)
     pair = t.get("lanes") == 3
     if k == 0:
         return "fg::k_%s_pipe (tensor-map tile pipeline, %s step)" % ("fwd" if direction == "forward" else "adj",
@@ -331,7 +333,7 @@ def run_ours(args, rank, local, world):
     bytes_launch = adj_b if dom == "adjoint" else fwd_b
     launch_ms = adj_launch_ms if dom == "adjoint" else fwd_launch_ms
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
-    ncu = NCU_BYTES_PER_SHOT_CELL_STEP[dom]
+    ncu = next((v for k, v in NCU_BYTES_PER_SHOT_CELL_STEP.items() if kernel_name(tuning, dom).startswith(k)), None)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None if ncu is None else int(ncu * S * nx * ny),

@@ -25,8 +25,9 @@ _CACHE: Dict[Tuple, dict] = {}
 
 FWD_SHOT = [dict(kernel=1, rows_per_tile=ti) for ti in (2, 4, 6)] + \
            [dict(kernel=0, rows_per_tile=8, warps_per_block=4, stages=s) for s in (2, 3)]
-ADJ_SHOT = [dict(adj_kernel=1, adj_rows_per_tile=ti, adj_warps_per_block=4, adj_stages=s)
-            for ti, s in ((8, 2), (8, 3), (4, 2))] + [dict(adj_kernel=2, adj_rows_per_tile=4)]
+ADJ_SHOT = [dict(adj_kernel=2, adj_rows_per_tile=ti, adj_cells_per_thread=8) for ti in (3, 4, 8)] + \
+           [dict(adj_kernel=1, adj_rows_per_tile=8, adj_warps_per_block=4, adj_stages=2, adj_cells_per_thread=4),
+            dict(adj_kernel=2, adj_rows_per_tile=4, adj_cells_per_thread=4)]
 FWD_COL = [dict(kernel=0, rows_per_tile=ti, warps_per_block=min(ti, 4)) for ti in (4, 8)] + \
           [dict(kernel=1, rows_per_tile=4)]
 ADJ_COL = [dict(adj_kernel=1, adj_rows_per_tile=ti, adj_warps_per_block=min(ti, 4)) for ti in (4, 8)] + \

@@ -87,8 +87,8 @@ typedef struct fg_tuning {
                                   march and column lanes the tile pipeline. */
     /* The adjoint runs on a plan of its own (own state and accumulators); its
      * launch shape: adj_kernel 0 = the forward's shape when the fields above
-     * name one, else the default adjoint shape (shot lanes: tile pipeline,
-     * 8 rows over 4 consumer warps, 2 stages; column lanes: the forward's);
+     * name one, else the default adjoint shape (shot lanes: lane march with
+     * 8 cells per thread over 4 rows; column lanes: the forward's);
      * 1 = tile pipeline, 2 = lane march, shaped by the three fields below
      * (0 = their defaults).  lanes is shared; adj_cells_per_thread (0 = the
      * forward's cells_per_thread) sets the adjoint's own.  The Ez history
