@@ -27,5 +27,5 @@ def test_autotune_picks_a_valid_shape_with_identical_results(fg, shots):
         assert np.array_equal(a, b)
     assert len(at._CACHE) >= 1
     tuned = next(iter(at._CACHE.values()))
-    assert set(tuned) <= {"lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel",
-                          "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages"}
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    assert set(tuned) <= set(nat.FgTuning.KEYS)
