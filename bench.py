@@ -66,7 +66,8 @@ UNIT = "Gcell-steps/s"
 # 64 x 440 x 340 shot-cells.
 # DRAM bytes per shot-cell-step of each step kernel, from one ncu capture on the 440 x 340 grid with 64 shots
 # (read + write); a kernel with no capture reports null traffic
-NCU_BYTES_PER_SHOT_CELL_STEP = {"fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340)}
+NCU_BYTES_PER_SHOT_CELL_STEP = {"fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340),
+                                "fg::k_adj (": 293.9e6 / (64 * 440 * 340)}
 
 
 def _fg():
