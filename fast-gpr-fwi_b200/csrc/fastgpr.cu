@@ -11,15 +11,12 @@
 #include <cudaTypedefs.h>
 
 #include "../../include/fastgpr.h"
-#include "fdtd_common.cuh"
-#include "fdtd_lanes.cuh"
-#include "fdtd_tile.cuh"
+#include "plan.h"
+#include "fdtd_setup.cuh"
 #include "tv.cuh"
-#include "fdtd_pairs.cuh"
 #include "fir.cuh"
 
-using fg::Dev;
-using fg::Ev;
+using namespace fgk;
 
 namespace {
 
@@ -43,44 +40,6 @@ int cuda_fail(cudaError_t e, const char* what) {
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
-
-struct fg_plan {
-    // problem
-    int nx, ny, S, nt, th, nsrc, nrx;
-    float dx, dt;
-    std::vector<int32_t> src, rx;
-    std::vector<float> srcw, pml;
-    // launch shape
-    int kernel;         // 0 = tensor-map tiles, 1 = lane march
-    bool shot;          // shot lanes (CS = 32 or, with pair, 64) or column lanes (CS = 1)
-    bool pair = false;  // two shots per lane (CS = 64, lane march only)
-    int W, TI, WPB, D;  // cells per thread, rows per tile, warps per block, ring stages (0 = direct loads)
-    // tensor maps of the tile kernels (encoded when a workspace is bound)
-    CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
-    int CS, SL;         // floats per cell in a group plane, shots per group
-    int P, TY, Ph, BW, nb, nc, ngroups, ntiles;
-    std::vector<int> chunk_row, order;
-    std::vector<int4> tiles;   // (b0, i0, group, id) per position of `order`
-    std::vector<Ev> src_ev, rx_ev, inj_ev;
-    std::vector<int> src_off, rx_off, inj_off;
-    // workspace layout (byte offsets)
-    size_t o_coef, o_state, o_psi, o_chunk, o_order, o_tiles, o_ctr, o_srcev, o_rxev, o_injev, o_offs, o_srcw, o_pml, o_gacc,
-        o_sums, o_partial, o_norms, o_err, total;
-    // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
-    int fwd_blocks = 0, adj_blocks = 0;
-    // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
-    float dinv = 0.f;
-    int div_scaled = 0;   // the scaled step matches __fdiv_rn for every |x| < 2^31 (checked at bind)
-    // the adjoint's own plan (own state, coefficients, accumulators and launch
-    // shape); its workspace follows this plan's in the caller's workspace
-    fg_plan* adj = nullptr;
-    ~fg_plan() { delete adj; }
-    long long plane, pxs, pys;
-    size_t state_bytes, psi_bytes;
-    char* ws = nullptr;
-    int64_t ws_bytes = 0;
-    Dev g;
-};
 
 namespace {
 
@@ -277,132 +236,6 @@ void fill_grid(fg_plan* p) {
     g.err = (int*)(w + p->o_err);
 }
 
-using FwdFn = cudaError_t (*)(const Dev&, int, int, int, int*, cudaStream_t);
-using AdjFn = cudaError_t (*)(const Dev&, int, int, int, int, int*, cudaStream_t);
-
-template <int W, bool SHOT>
-size_t ring_smem(int wpb, int D, bool adjoint) {
-    using RG = fg::RingGeom<W, SHOT>;
-    return fg::ring_bar_bytes(wpb, D) + (size_t)wpb * D * (adjoint ? RG::ADJ : RG::FWD) * sizeof(float);
-}
-
-template <class K>
-cudaError_t allow_smem(K kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-}
-
-// Blocks of a persistent launch: as many as are resident on the device at
-// once, at most one warp per tile.
-template <class K>
-cudaError_t persistent_blocks(K kernel, int wpb, size_t smem, int ntiles, int* blocks) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * wpb, smem);
-    if (e != cudaSuccess) return e;
-    const int need = (ntiles + wpb - 1) / wpb;
-    *blocks = std::max(1, std::min(need, std::max(per_sm, 1) * sms));
-    return cudaSuccess;
-}
-
-template <int W, bool SHOT, bool RING>
-cudaError_t launch_fwd_k(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
-    const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, false) : 0);
-    auto kernel = fg::k_fwd<W, SHOT, RING>;
-    if (*blocks == 0) {
-        cudaError_t e = allow_smem(kernel, smem);
-        if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
-        if (e != cudaSuccess) return e;
-    }
-    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, t, D);
-    return cudaSuccess;
-}
-template <int W, bool SHOT, bool RING>
-cudaError_t launch_adj_k(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
-    const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, true) : 0);
-    auto kernel = fg::k_adj<W, SHOT, RING>;
-    if (*blocks == 0) {
-        cudaError_t e = allow_smem(kernel, smem);
-        if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
-        if (e != cudaSuccess) return e;
-    }
-    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, it, rp, D);
-    return cudaSuccess;
-}
-template <int W, bool SHOT>
-cudaError_t launch_fwd(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
-    return D == 0 ? launch_fwd_k<W, SHOT, false>(g, t, wpb, D, blocks, st)
-                  : launch_fwd_k<W, SHOT, true>(g, t, wpb, D, blocks, st);
-}
-template <int W, bool SHOT>
-cudaError_t launch_adj(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
-    return D == 0 ? launch_adj_k<W, SHOT, false>(g, it, rp, wpb, D, blocks, st)
-                  : launch_adj_k<W, SHOT, true>(g, it, rp, wpb, D, blocks, st);
-}
-
-template <bool SHOT>
-FwdFn pick_fwd_w(int W) {
-    switch (W) {
-        case 2: return launch_fwd<2, SHOT>;
-        case 4: return launch_fwd<4, SHOT>;
-        case 8: return launch_fwd<8, SHOT>;
-    }
-    return nullptr;
-}
-FwdFn pick_fwd(bool shot, int W) { return shot ? pick_fwd_w<true>(W) : pick_fwd_w<false>(W); }
-template <bool SHOT>
-AdjFn pick_adj_w(int W) {
-    switch (W) {
-        case 2: return launch_adj<2, SHOT>;
-        case 4: return launch_adj<4, SHOT>;
-        case 8: return launch_adj<8, SHOT>;
-    }
-    return nullptr;
-}
-AdjFn pick_adj(bool shot, int W) { return shot ? pick_adj_w<true>(W) : pick_adj_w<false>(W); }
-
-template <int W>
-cudaError_t launch_fwd2(const Dev& g, int t, int, int, int* blocks, cudaStream_t st) {
-    const size_t smem = fg::prof_bytes(g.th);
-    auto kernel = fg::k_fwd2<W>;
-    if (*blocks == 0) {
-        cudaError_t e = allow_smem(kernel, smem);
-        if (e == cudaSuccess) e = persistent_blocks(kernel, 4, smem, g.ntiles, blocks);
-        if (e != cudaSuccess) return e;
-    }
-    kernel<<<*blocks, 128, smem, st>>>(g, t);
-    return cudaSuccess;
-}
-template <int W>
-cudaError_t launch_adj2(const Dev& g, int it, int rp, int, int, int* blocks, cudaStream_t st) {
-    const size_t smem = fg::prof_bytes(g.th);
-    auto kernel = fg::k_adj2<W>;
-    if (*blocks == 0) {
-        cudaError_t e = allow_smem(kernel, smem);
-        if (e == cudaSuccess) e = persistent_blocks(kernel, 4, smem, g.ntiles, blocks);
-        if (e != cudaSuccess) return e;
-    }
-    kernel<<<*blocks, 128, smem, st>>>(g, it, rp);
-    return cudaSuccess;
-}
-FwdFn pick_fwd2(int W) { return W == 2 ? launch_fwd2<2> : W == 4 ? launch_fwd2<4> : nullptr; }
-AdjFn pick_adj2(int W) { return W == 2 ? launch_adj2<2> : W == 4 ? launch_adj2<4> : nullptr; }
-
-// Shared memory of the larger (adjoint) ring, or 0 for direct loads.
-size_t plan_ring_smem(const fg_plan* p) {
-    if (p->D == 0) return 0;
-    switch ((p->shot ? 10 : 0) + p->W) {
-        case 12: return ring_smem<2, true>(p->WPB, p->D, true);
-        case 14: return ring_smem<4, true>(p->WPB, p->D, true);
-        case 18: return ring_smem<8, true>(p->WPB, p->D, true);
-        case 2: return ring_smem<2, false>(p->WPB, p->D, true);
-        case 4: return ring_smem<4, false>(p->WPB, p->D, true);
-        case 8: return ring_smem<8, false>(p->WPB, p->D, true);
-    }
-    return 0;
-}
-
 int coefficients(const float* er, const float* se, const float* mr, int nx, int ny, float dt, float dx, int adjoint,
                  float* out, int P, int col0, cudaStream_t st) {
     const long long n = (long long)(nx + 1) * P;
@@ -508,66 +341,6 @@ int encode_hist_map(const fg_plan* p, CUtensorMap* m, const float* hist, int nst
     const uint64_t st[2] = {(uint64_t)p->Ph * f4, (uint64_t)p->nx * p->Ph * f4};
     const uint32_t box[3] = {(uint32_t)p->BW, (uint32_t)p->TI, 1};
     return encode_map(m, hist, 3, dims, st, box);
-}
-
-// Persistent pipeline launches: WPB consumer warps (TI / WPB rows each) + 1
-// producer warp per CTA,
-// as many CTAs as are resident on the device (at most one per tile).
-template <class K>
-cudaError_t pipe_blocks(K kernel, int threads, size_t smem, int ntiles, int* blocks) {
-    if (*blocks) return cudaSuccess;
-    cudaError_t e = allow_smem(kernel, smem);
-    int dev = 0, sms = 0, per_sm = 0;
-    if (e == cudaSuccess) e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-    if (e != cudaSuccess) return e;
-    *blocks = std::max(1, std::min(ntiles, std::max(per_sm, 1) * sms));
-    return cudaSuccess;
-}
-template <int W, bool SHOT>
-cudaError_t launch_fwd_tile(fg_plan* p, const Dev& g, int t, cudaStream_t st) {
-    const fg::TileSmem<W, SHOT> L(p->TI, false);
-    const fg::PipeSmem M(p->th, p->D, L.total);
-    auto kernel = fg::k_fwd_pipe<W, SHOT>;
-    const int threads = 32 * (p->WPB + 1);
-    const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->fwd_blocks);
-    if (e != cudaSuccess) return e;
-    kernel<<<p->fwd_blocks, threads, M.total, st>>>(g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t, p->D, p->TI);
-    return cudaSuccess;
-}
-template <int W, bool SHOT>
-cudaError_t launch_adj_tile(fg_plan* p, const Dev& g, const CUtensorMap& tmh, int it, int rp, cudaStream_t st) {
-    const fg::TileSmem<W, SHOT> L(p->TI, true);
-    const fg::PipeSmem M(p->th, p->D, L.total);
-    auto kernel = fg::k_adj_pipe<W, SHOT>;
-    const int threads = 32 * (p->WPB + 1);
-    const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->adj_blocks);
-    if (e != cudaSuccess) return e;
-    kernel<<<p->adj_blocks, threads, M.total, st>>>(g, p->tm_aez, p->tm_ahx, p->tm_ahy, p->tm_co, tmh, it, rp,
-                                                     p->D, p->TI);
-    return cudaSuccess;
-}
-using FwdTileFn = cudaError_t (*)(fg_plan*, const Dev&, int, cudaStream_t);
-using AdjTileFn = cudaError_t (*)(fg_plan*, const Dev&, const CUtensorMap&, int, int, cudaStream_t);
-FwdTileFn pick_fwd_tile(bool shot, int W) {
-    if (shot) return W == 4 ? launch_fwd_tile<4, true> : W == 8 ? launch_fwd_tile<8, true> : nullptr;
-    return W == 2 ? launch_fwd_tile<2, false> : W == 4 ? launch_fwd_tile<4, false> : nullptr;
-}
-AdjTileFn pick_adj_tile(bool shot, int W) {
-    if (shot) return W == 4 ? launch_adj_tile<4, true> : W == 8 ? launch_adj_tile<8, true> : nullptr;
-    return W == 2 ? launch_adj_tile<2, false> : W == 4 ? launch_adj_tile<4, false> : nullptr;
-}
-// Shared memory of the larger (adjoint) pipeline CTA.
-size_t plan_tile_smem(const fg_plan* p) {
-    size_t stage = 0;
-    switch ((p->shot ? 10 : 0) + p->W) {
-        case 14: stage = fg::TileSmem<4, true>(p->TI, true).total; break;
-        case 18: stage = fg::TileSmem<8, true>(p->TI, true).total; break;
-        case 2: stage = fg::TileSmem<2, false>(p->TI, true).total; break;
-        case 4: stage = fg::TileSmem<4, false>(p->TI, true).total; break;
-    }
-    return fg::PipeSmem(p->th, p->D, stage).total;
 }
 
 // Device scratch of fg_forward_static: one array per GPU that loads the
