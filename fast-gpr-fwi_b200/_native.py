@@ -30,7 +30,7 @@ EXPORTS = (
     "fg_coefficients", "fg_forward", "fg_adjoint_reference", "fg_plan_check", "fg_last_error",
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
     "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
-    "fg_fir_causal", "fg_adjoint_reference_l1",
+    "fg_fir_causal", "fg_adjoint_reference_l1", "fg_adjoint_exact",
 )
 
 
@@ -51,11 +51,12 @@ class FgTuning(ctypes.Structure):
         ("warps_per_block", ctypes.c_int32), ("stages", ctypes.c_int32), ("kernel", ctypes.c_int32),
         ("adj_kernel", ctypes.c_int32), ("adj_rows_per_tile", ctypes.c_int32),
         ("adj_warps_per_block", ctypes.c_int32), ("adj_stages", ctypes.c_int32),
-        ("adj_cells_per_thread", ctypes.c_int32),
+        ("adj_cells_per_thread", ctypes.c_int32), ("prefetch", ctypes.c_int32),
     ]
 
     KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel",
-            "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages", "adj_cells_per_thread")
+            "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages", "adj_cells_per_thread",
+            "prefetch")
 
 
 class FastGprError(RuntimeError):
@@ -116,6 +117,8 @@ def lib() -> ctypes.CDLL:
     L.fg_adjoint_reference_checkpointed.restype = ctypes.c_int
     L.fg_adjoint_reference_l1.argtypes = [vp, vp, vp, vp, vp, vp, vp, f32, vp, vp, i32, vp, vp]
     L.fg_adjoint_reference_l1.restype = ctypes.c_int
+    L.fg_adjoint_exact.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.fg_adjoint_exact.restype = ctypes.c_int
     L.fg_fir_causal.argtypes = [vp, i64, i32, i32, vp, i32, vp, vp]
     L.fg_fir_causal.restype = ctypes.c_int
     L.fg_tv_workspace_bytes.argtypes = [i32, i32]
@@ -236,6 +239,13 @@ class Plan:
         check(lib().fg_adjoint_reference_l1(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(hist), ptr(traces),
                                             ptr(observed), float(scale), ptr(grad_eps), ptr(grad_sig),
                                             1 if normalize else 0, ptr(norms), stream_handle(self.device)))
+        if checked_build():
+            self.device_check()
+
+    def adjoint_exact(self, er32, se32, mr32, hist, weights, grad_eps, grad_sig):
+        """Exact gradient of sum(weights * traces) (fg_adjoint_exact), not normalised."""
+        check(lib().fg_adjoint_exact(self._h, ptr(er32), ptr(se32), ptr(mr32), ptr(hist), ptr(weights),
+                                     ptr(grad_eps), ptr(grad_sig), stream_handle(self.device)))
         if checked_build():
             self.device_check()
 

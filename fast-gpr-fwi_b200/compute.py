@@ -17,6 +17,11 @@ geometry (grid.py) and owns the tensors.  There is no CPU path.
 New keywords (after the reference's own, all defaulting to the reference's
 behaviour): ``adjoint`` ('reference'), ``tv_weight`` (0.01, the constant of
 src/compute.py:920,928) and ``tuning`` (launch shape, see autotune).
+
+``adjoint='exact'`` swaps the reference's gradient for the exact discrete
+adjoint of the forward loop (fg_adjoint_exact): the true derivative of the
+loss with respect to ``er`` and ``se`` (CPML profile held fixed), not
+normalised; the TV term is still added when ``tv`` is set.
 """
 from __future__ import annotations
 
@@ -79,8 +84,8 @@ class Solve:
 
     def __init__(self, device, setup: SolveSetup, tuning: Optional[dict] = None, tv: bool = True,
                  tv_weight: float = 0.01, adjoint: str = "reference", checkpoint=None, bind: bool = True):
-        if adjoint not in ("reference",):
-            raise ValueError("adjoint must be 'reference'")
+        if adjoint not in ("reference", "exact"):
+            raise ValueError("adjoint must be 'reference' or 'exact'")
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise RuntimeError("the FDTD solver runs on CUDA devices only (got %s)" % self.device)
@@ -101,6 +106,8 @@ class Solve:
                                  s.src.cpu().numpy(), s.rx.cpu().numpy(), s.srcw, pml, self.device, tuning,
                                  bind=bind)
         self.interval = checkpoint_interval(self.plan, checkpoint)
+        if adjoint == "exact" and self.interval is not None:
+            raise ValueError("adjoint='exact' keeps the whole Ez history (checkpoint=None)")
 
     def materials(self, er, se, mr):
         s = self.setup
@@ -127,7 +134,9 @@ class Solve:
             raise ValueError("residual shape %s != (%d, %d, %d)" % (tuple(resid.shape), s.shots, s.nt, self.plan.nrx))
         ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device) if need_eps else None
         gs = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device) if need_sig else None
-        if isinstance(hist, Checkpoints):
+        if self.adjoint == "exact":
+            self.plan.adjoint_exact(er32, se32, mr32, hist, resid, ge, gs)
+        elif isinstance(hist, Checkpoints):
             seg = self.plan.new_segment(hist.interval)
             self.plan.adjoint_reference_checkpointed(er32, se32, mr32, hist.buf, hist.interval, seg, resid, ge, gs,
                                                      normalize=normalize)

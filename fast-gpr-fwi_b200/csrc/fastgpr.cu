@@ -56,7 +56,7 @@ int classify(const fg_plan* p, int i, int j, int k) {
 void build_tiles(fg_plan* p) {
     p->SL = p->pair ? 64 : (p->shot ? 32 : 1);
     p->CS = p->SL;
-    p->BW = p->shot ? p->W : 32 * p->W;
+    p->BW = p->kernel == 2 ? p->WPB * p->W : (p->shot ? p->W : 32 * p->W);
     p->nb = (p->ny + p->BW - 1) / p->BW;
     // PADC leading zero columns, then columns up to nb*BW + 3 (halo column and
     // the 16-byte-aligned stage segments of the last band); rows of 16 bytes
@@ -193,6 +193,7 @@ void layout(fg_plan* p) {
     p->o_partial = take(2 * kRedBlocks * sizeof(double));
     p->o_norms = take(2 * sizeof(double));
     p->o_err = take(sizeof(int) * 4);
+    p->o_rxpos = take((size_t)p->S * p->nrx * sizeof(int2));
     p->total = o;
 }
 
@@ -224,6 +225,7 @@ void fill_grid(fg_plan* p) {
     g.tiles = (const int4*)(w + p->o_tiles);
     g.tile_ctr = (int*)(w + p->o_ctr);
     g.fast_cpml = 2 * p->th < p->nx && 2 * p->th < p->ny;
+    g.pf = p->pf;
     g.src_ev = (const Ev*)(w + p->o_srcev);
     g.rx_ev = (const Ev*)(w + p->o_rxev);
     g.inj_ev = (const Ev*)(w + p->o_injev);
@@ -535,19 +537,37 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // rows) for column lanes
     const bool tuned_kernel = tune && (tune->kernel || tune->stages || tune->rows_per_tile || tune->cells_per_thread);
     p->kernel = tuned_kernel ? tune->kernel : (p->shot ? 1 : 0);
-    if (p->kernel < 0 || p->kernel > 1) {
+    if (p->kernel < 0 || p->kernel > 2) {
         delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning: kernel must be 0 (tiles) or 1 (lane march)");
+        return fail(FG_ERR_INVALID, "unsupported tuning: kernel must be 0 (tiles), 1 (lane march) or 2 (band pipeline)");
     }
     p->W = tune && tune->cells_per_thread ? tune->cells_per_thread : (p->shot ? 4 : 2);
-    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : 4;
+    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : (p->kernel == 2 ? 32 : 4);
     p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : (p->kernel == 0 ? std::min(p->TI, 4) : 4);
     p->D = tune ? tune->stages : 0;
     if (p->kernel == 0 && p->pair) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: shot pairs (lanes 3) take the lane march (kernel 1)");
     }
-    if (p->kernel == 0) {
+    if (p->kernel == 2) {
+        if (p->D == 0) p->D = 6;   // ring stages of the band pipeline
+        if (!p->shot || p->pair) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: the band pipeline (kernel 2) takes shot lanes");
+        }
+        if (!pick_fwd_band(p->W, p->WPB) || p->TI < 1 || p->D < 2 || p->D > 16) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: the band pipeline takes (cells_per_thread, "
+                                        "warps_per_block) in (2,4) (2,8) (4,2) (4,4), "
+                                        "rows_per_tile >= 1 and stages 2..16");
+        }
+        if (std::max(band_smem(p->W, p->WPB, p->th, p->D, false), band_smem(p->W, p->WPB, p->th, p->D, true)) >
+            227 * 1024) {
+            delete p;
+            return fail(FG_ERR_INVALID, "unsupported tuning: the band pipeline's stages need more than 227 KB of "
+                                        "shared memory");
+        }
+    } else if (p->kernel == 0) {
         if (p->D == 0) p->D = 3;   // pipeline stages of the tile kernels
         const bool okw = p->shot ? (p->W == 4 || p->W == 8) : (p->W == 2 || p->W == 4);
         if (!okw || !(p->TI == 2 || p->TI == 4 || p->TI == 8 || p->TI == 16) || p->D < 2 || p->D > fg::MAX_STAGES ||
@@ -575,6 +595,15 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
             return fail(FG_ERR_INVALID, "unsupported tuning: shot lanes with stages need cells_per_thread 4 or 8");
         }
     }
+    const int pf = tune ? tune->prefetch : 0;
+    if (pf < -1 || pf > 2) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: prefetch must be -1, 0, 1 or 2");
+    }
+    // the next-tile prefetch serves the shot-lane lane march with direct loads;
+    // the band pipeline prefetches the CPML auxiliaries of the rows it streams
+    p->pf = ((p->kernel == 1 && p->shot && !p->pair && p->D == 0) || p->kernel == 2) ? (pf == 0 ? 1 : std::max(pf, 0))
+                                                                                      : 0;
     if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: the ring needs more than 227 KB of shared memory");
@@ -599,9 +628,10 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     // 440 x 340 benchmark grid, 119 us against 139 us for the tile pipeline)
     const bool tuned = tune && (tune->kernel || tune->stages || tune->rows_per_tile || tune->cells_per_thread);
     const int ak = tune ? tune->adj_kernel : 0;
-    if (ak < 0 || ak > 2) {
+    if (ak < 0 || ak > 3) {
         delete p;
-        return fail(FG_ERR_INVALID, "unsupported tuning: adj_kernel must be 0, 1 (tiles) or 2 (lane march)");
+        return fail(FG_ERR_INVALID,
+                    "unsupported tuning: adj_kernel must be 0, 1 (tiles), 2 (lane march) or 3 (band pipeline)");
     }
     fg_tuning at = {};
     at.lanes = p->pair ? 3 : (p->shot ? 1 : 2);
@@ -618,13 +648,16 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
         at.warps_per_block = tune && tune->adj_warps_per_block ? tune->adj_warps_per_block : 4;
         at.stages = tune && tune->adj_stages ? tune->adj_stages : 0;
     } else {
-        at.kernel = ak == 2 ? 1 : 0;
-        at.rows_per_tile = tune && tune->adj_rows_per_tile ? tune->adj_rows_per_tile : (at.kernel == 0 ? 8 : 4);
+        at.kernel = ak == 3 ? 2 : (ak == 2 ? 1 : 0);
+        at.rows_per_tile = tune && tune->adj_rows_per_tile ? tune->adj_rows_per_tile
+                                                           : (at.kernel == 0 ? 8 : (at.kernel == 2 ? 32 : 4));
         at.warps_per_block = tune && tune->adj_warps_per_block ? tune->adj_warps_per_block
                                                                : (at.kernel == 0 ? std::min(at.rows_per_tile, 4) : 4);
-        at.stages = tune && tune->adj_stages ? tune->adj_stages : (at.kernel == 0 ? 2 : 0);
+        at.stages = tune && tune->adj_stages ? tune->adj_stages : (at.kernel == 0 ? 2 : (at.kernel == 2 ? 6 : 0));
+        if (at.kernel == 2 && !(tune && tune->adj_cells_per_thread)) at.cells_per_thread = 4;
     }
     if (tune && tune->adj_cells_per_thread) at.cells_per_thread = tune->adj_cells_per_thread;
+    at.prefetch = tune ? tune->prefetch : 0;
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {
@@ -728,6 +761,13 @@ static int bind_one(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     offs.insert(offs.end(), p->inj_off.begin(), p->inj_off.end());
     FG_CUDA(up(p->o_offs, offs.data(), offs.size() * sizeof(int)));
     FG_CUDA(up(p->o_srcw, p->srcw.data(), p->srcw.size() * sizeof(float)));
+    // receiver cells per shot for the exact adjoint's injection, (-1, -1) when inert
+    std::vector<int2> rxpos((size_t)p->S * p->nrx);
+    for (size_t k = 0; k < rxpos.size(); ++k) {
+        const int i = p->rx[3 * k], j = p->rx[3 * k + 1], kk = p->rx[3 * k + 2];
+        rxpos[k] = classify(p, i, j, kk) == 1 ? make_int2(i, j) : make_int2(-1, -1);
+    }
+    FG_CUDA(up(p->o_rxpos, rxpos.data(), rxpos.size() * sizeof(int2)));
     FG_CUDA(up(p->o_pml, p->pml.data(), p->pml.size() * sizeof(float)));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_err, 0, sizeof(int) * 4, st));
     // division by the cell size: the reciprocal step of div_d is enabled when
@@ -778,6 +818,10 @@ int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
         FwdTileFn tfn = pick_fwd_tile(p->shot, p->W);
         if (!tfn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int t = t0; t < t1; ++t) FG_CUDA(tfn(p, g, t, st));
+    } else if (p->kernel == 2) {
+        FwdFn fn = pick_fwd_band(p->W, p->WPB);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int t = t0; t < t1; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
     } else {
         FwdFn fn = p->pair ? pick_fwd2(p->W) : pick_fwd(p->shot, p->W);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
@@ -797,6 +841,10 @@ int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t
         const int rc = encode_hist_map(a, &tmh, g.hist, nsteps);
         if (rc) return rc;
         for (int it = hi; it >= lo; --it) FG_CUDA(tfn(a, g, tmh, it, (a->nt - 1 - it) & 1, st));
+    } else if (a->kernel == 2) {
+        AdjFn fn = pick_adj_band(a->W, a->WPB);
+        if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        for (int it = hi; it >= lo; --it) FG_CUDA(fn(g, it, (a->nt - 1 - it) & 1, a->WPB, a->D, &a->adj_blocks, st));
     } else {
         AdjFn fn = a->pair ? pick_adj2(a->W) : pick_adj(a->shot, a->W);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
@@ -930,6 +978,43 @@ int fg_adjoint_reference_l1(fg_plan* p, const float* er, const float* se, const 
     if (p && p->nrx > 0 && !observed) return fail(FG_ERR_INVALID, "fg_adjoint_reference_l1: NULL observed traces");
     return adjoint_full(p, er, se, mr, hist, traces, observed, scale, grad_eps, grad_sig, normalize, norms, stream,
                         "fg_adjoint_reference_l1");
+}
+
+int fg_adjoint_exact(fg_plan* p, const float* er, const float* se, const float* mr, const float* hist,
+                     const float* weights, float* grad_eps, float* grad_sig, void* stream) {
+    if (!p || !er || !se || !mr || !hist || (!weights && p->nrx > 0))
+        return fail(FG_ERR_INVALID, "fg_adjoint_exact: NULL argument");
+    fg_plan* a = p->adj ? p->adj : p;
+    if (!a->ws) return fail(FG_ERR_WORKSPACE, "fg_adjoint_exact: plan has no workspace");
+    cudaStream_t st = (cudaStream_t)stream;
+    // the forward's coefficients (Ucget): the adjoint of the forward operator itself
+    int rc = coefficients(er, se, mr, a->nx, a->ny, a->dt, a->dx, 0, (float*)(a->ws + a->o_coef), a->P, fg::PADC, st);
+    if (rc) return rc;
+    if ((rc = reset_state(a, st))) return rc;
+    const size_t n = (size_t)a->nx * a->ny;
+    FG_CUDA(cudaMemsetAsync(a->ws + a->o_gacc, 0, (size_t)a->ngroups * 2 * n * sizeof(double), st));
+    Dev g = a->g;
+    g.hist = const_cast<float*>(hist);
+    g.out_lo = (const char*)hist;
+    g.out_hi = (const char*)(hist + (size_t)a->nt * hist_step_floats(a));
+    const int2* rxpos = (const int2*)(a->ws + a->o_rxpos);
+    const int nt = a->nt;
+    if (nt >= 2) {
+        // lambda_{nt-1} = R^T w_{nt-1} in parity 0; iteration it reads parity (nt-1-it) & 1
+        if (a->nrx > 0) FG_CUDA(launch_inject_exact(g, rxpos, weights, nt - 1, 0, a->CS, st));
+        for (int it = nt - 1; it >= 1; --it) {
+            const int rp = (nt - 1 - it) & 1;
+            FG_CUDA(launch_adj_exact(g, it, rp, a->CS, st));
+            if (it >= 2 && a->nrx > 0) FG_CUDA(launch_inject_exact(g, rxpos, weights, it - 1, rp ^ 1, a->CS, st));
+        }
+    }
+    double* sums = (double*)(a->ws + a->o_sums);
+    double* partial = (double*)(a->ws + a->o_partial);
+    fg::k_grad_sum<<<kRedBlocks, 256, 0, st>>>(g.gacc, a->ngroups, (long long)n, sums, partial);
+    FG_CUDA(cudaGetLastError());
+    const double e0 = (double)8.8541878128e-12f;   // the float constant of uc.cu:8
+    FG_CUDA(launch_grad_exact(sums, er, se, a->nx, a->ny, e0 / (double)a->dt, grad_eps, grad_sig, st));
+    return FG_OK;
 }
 
 int64_t fg_plan_checkpoint_bytes(const fg_plan* p, int32_t interval) {

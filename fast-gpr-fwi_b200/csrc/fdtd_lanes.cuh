@@ -143,6 +143,89 @@ __device__ __forceinline__ const float* stage_profile(const Dev& g, unsigned cha
     return R;
 }
 
+// Bulk prefetch of [p, p + bytes) into L2 (no data returned).
+__device__ __forceinline__ void prefetch_l2(const float* p, long long first, long long last) {
+    // [first, last] in floats, widened to 16-byte boundaries
+    const long long a = first & ~3LL, b = (last | 3LL) + 1;
+    if (b <= a) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + a), "r"((uint32_t)((b - a) * 4)) : "memory");
+}
+
+// Prefetch into L2 the CPML auxiliaries (read parity) a tile of rows
+// [r0, r1] and columns [jlo, jhi] touches, so that the consumers' gather
+// loads of a CPML tile hit L2.  Issued by the producer, S tiles ahead.
+template <int CS>
+__device__ __forceinline__ void prefetch_tile_psi(const Dev& g, int grp, int rp, int r0, int r1, int jlo, int jhi) {
+    const int th = g.th, nx = g.nx, ny = g.ny, P = g.P, TY = g.TY;
+    if (th <= 0) return;
+    r0 = max(r0, 0);
+    r1 = min(r1, nx - 1);
+    jlo = max(jlo, 0);
+    jhi = min(jhi, ny - 1);
+    if (r0 > r1 || jlo > jhi) return;
+    const PsiG rd = psi_group(g, rp, grp);
+    // x slabs: E rows 1..th (k = th-i), H rows 0..th-1 (k = th-1-i), both nx-th.. (k = th+i-(nx-th))
+    for (int i = r0; i <= r1; ++i) {
+        const int ke = (i >= 1 && i <= th) ? th - i : (i >= nx - th ? th + i - (nx - th) : -1);
+        const int kh = (i <= th - 1) ? th - 1 - i : (i >= nx - th ? th + i - (nx - th) : -1);
+        if (ke >= 0) prefetch_l2(rd.ex, ((long long)ke * P + jlo) * CS, ((long long)ke * P + jhi) * CS + CS - 1);
+        if (kh >= 0) prefetch_l2(rd.hx, ((long long)kh * P + jlo) * CS, ((long long)kh * P + jhi) * CS + CS - 1);
+    }
+    // y slabs: y0 columns 0..th (k = th-j for E, th-1-j for H), ymax columns ny-th.. (k = j-(ny-th))
+    const bool y0 = jlo <= th, ym = jhi >= ny - th;
+    if (!y0 && !ym) return;
+    const int k0lo = max(0, th - 1 - jhi), k0hi = min(th - 1, th - jlo);
+    const int kmlo = max(jlo, ny - th) - (ny - th), kmhi = jhi - (ny - th);
+    for (int i = r0; i <= r1; ++i) {
+        if (y0 && k0lo <= k0hi) {
+            const long long o = (long long)i * TY;
+            prefetch_l2(rd.ey, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
+            prefetch_l2(rd.hy, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
+        }
+        if (ym && kmlo <= kmhi) {
+            const long long o = (long long)(nx + 1 + i) * TY;
+            prefetch_l2(rd.ey, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
+            prefetch_l2(rd.hy, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
+        }
+    }
+}
+
+// Prefetch into L2 what the shot-lane tile at fetch position `pos` will read
+// from the state of parity rp -- Ez, Hx and Hy of rows [i0-1, i1] (clamped to
+// the plane), columns j0-1 .. j0+W -- and, when hist is set (adjoint), its
+// Ez history rows [i0, i1) of step `it`, plus the CPML auxiliaries of a
+// boundary tile.  One bulk prefetch per lane; issued a tile ahead, so the
+// tile's own loads find their lines in L2.
+template <int W>
+__device__ __forceinline__ void prefetch_tile_shot(const Dev& g, int pos, int rp, int lane, const float* hist, int it) {
+    if (pos >= g.ntiles) return;
+    const int id = __ldg(g.order + pos);
+    const int band = id % g.nb, rest = id / g.nb, chunk = rest % g.nc, grp = rest / g.nc;
+    const int i0 = __ldg(g.chunk_row + chunk), i1 = __ldg(g.chunk_row + chunk + 1);
+    const int j0 = band * W;
+    const int r0 = max(i0 - 1, 0), r1 = min(i1, g.nx), nr = r1 - r0 + 1;
+    const int nh = hist && j0 < g.Ph ? i1 - i0 : 0;
+    const long long go = (long long)grp * g.plane + ((long long)r0 * g.P + j0 - 1 + PADC) * 32;
+    const long long rowS = (long long)g.P * 32;
+    for (int k = lane; k < 3 * nr + nh; k += 32) {
+        const float* p;
+        uint32_t bytes;
+        if (k < 3 * nr) {
+            const int f = k / nr, r = k - f * nr;
+            const float* base = f == 0 ? g.ez[rp] : (f == 1 ? g.hx[rp] : g.hy[rp]);
+            p = base + go + r * rowS;
+            bytes = (W + 2) * 128;
+        } else {
+            const int i = i0 + (k - 3 * nr);
+            p = hist + ((((long long)(it - g.hist_t0) * g.ngroups + grp) * g.nx + i) * g.Ph + j0) * 32;
+            bytes = (uint32_t)min(W, g.Ph - j0) * 128;
+        }
+        if (!FG_OK_PTR(g, p, (int)bytes)) continue;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+    }
+    if (lane == 0 && g.th > 0) prefetch_tile_psi<32>(g, grp, rp, r0, r1, j0 - 1, j0 + W);
+}
+
 // ---------------------------------------------------------------------------
 // Tiles
 // ---------------------------------------------------------------------------
@@ -236,6 +319,56 @@ struct FwdIn {                 // operands of row i
     float ch[W + 1];           // uH1 (i, j0-1 ..)
 };
 
+// Interior forward row (every cell of H at columns j0-1 .. j0+W-1 and of E
+// at j0 .. j0+W-1 away from the CPML and the frame): the leapfrog of
+// fields_updates_gpu.cu:47-78 then :8-33.
+template <int W>
+__device__ __forceinline__ void fwd_core(const FwdIn<W>& B, const float (&ezc)[W + 2], const float (&hyu)[W],
+                                         float (&hxn)[W + 1], float (&hyn)[W], float (&ezn)[W]) {
+#pragma unroll
+    for (int k = 0; k <= W; ++k) hxn[k] = __fsub_rn(B.hxo[k], __fmul_rn(B.ch[k], __fsub_rn(ezc[k + 1], ezc[k])));
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+        hyn[w] = __fadd_rn(B.hyo[w], __fmul_rn(B.ch[w + 1], __fsub_rn(B.en[w + 1], ezc[w + 1])));
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+        ezn[w] = __fmaf_rn(-B.cb[w], __fsub_rn(hxn[w + 1], hxn[w]),
+                           madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
+}
+
+// Hertzian dipole (sourcereceiver.cu:84) on the new Ez of row i, in list
+// order: the tile's source events of the row from sc on.
+template <int W>
+__device__ __forceinline__ void fwd_sources(const Dev& g, int i, int t, int j0, int slot, float (&ezn)[W], int& sc,
+                                            int se) {
+    for (; sc < se; ++sc) {
+        const Ev e = __ldg(g.src_ev + sc);
+        if (e.x != i) break;
+        if (e.y != slot) continue;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (j0 + w == e.z) {
+                const float cd = ldro(g, g.cd + coef_at(g, i, e.z));
+                ezn[w] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezn[w]);
+            }
+    }
+}
+
+// Receiver samples of row i (store_outputs, sourcereceiver.cu:11-56, reads
+// Ez at the start of step t+1 = after step t).
+template <int W>
+__device__ __forceinline__ void fwd_receivers(const Dev& g, int i, int t, int j0, int slot, int s, const float (&ezn)[W],
+                                              int& rc, int re) {
+    for (; rc < re; ++rc) {
+        const Ev e = __ldg(g.rx_ev + rc);
+        if (e.x != i) break;
+        if (e.y != slot || t + 1 >= g.nt) continue;
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (j0 + w == e.z && g.traces) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezn[w];
+    }
+}
+
 // Row i of the forward step from its operands; carries ezc (Ez_old of row i,
 // columns j0-1 .. j0+W) and hyu (Hy_new of row i-1) to the next row.
 template <int W, int CS>
@@ -247,15 +380,7 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
     const int nx = g.nx, ny = g.ny, th = g.th;
     float hxn[W + 1], hyn[W], ezn[W];
     if (bcore && i >= th + 1 && i <= nx - th - 1) {
-#pragma unroll
-        for (int k = 0; k <= W; ++k) hxn[k] = __fsub_rn(B.hxo[k], __fmul_rn(B.ch[k], __fsub_rn(ezc[k + 1], ezc[k])));
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-            hyn[w] = __fadd_rn(B.hyo[w], __fmul_rn(B.ch[w + 1], __fsub_rn(B.en[w + 1], ezc[w + 1])));
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-            ezn[w] = __fmaf_rn(-B.cb[w], __fsub_rn(hxn[w + 1], hxn[w]),
-                               madd2(B.ca[w], ezc[w + 1], B.cb[w], __fsub_rn(hyn[w], hyu[w])));
+        fwd_core<W>(B, ezc, hyu, hxn, hyn, ezn);
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
             fwd_row_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn, ezn);
@@ -308,31 +433,13 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
                                           __fsub_rn(hxn[w + 1], hxn[w]), B.ca[w], B.cb[w], rd, wr);
         }
     }
-    // Hertzian dipole (sourcereceiver.cu:84), in list order
-    for (; sc < se; ++sc) {
-        const Ev e = __ldg(g.src_ev + sc);
-        if (e.x != i) break;
-        if (e.y != slot) continue;
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-            if (j0 + w == e.z) {
-                const float cd = ldro(g, g.cd + coef_at(g, i, e.z));
-                ezn[w] = __fmaf_rn(-cd, __ldg(g.srcw + (long long)e.w * g.nt + t), ezn[w]);
-            }
-    }
+    fwd_sources<W>(g, i, t, j0, slot, ezn, sc, se);
     const long long o = ((long long)i * g.P + j0 + PADC) * CS + l;
     st_cells<W, CS>(g, ezW + o, ezn);
     st_cells<W, CS>(g, hxW + o, hxn + 1);
     st_cells<W, CS>(g, hyW + o, hyn);
     if (hist && j0 < g.Ph) st_cells<W, CS, true>(g, hist + (long long)i * hrow, ezn);
-    for (; rc < re; ++rc) {
-        const Ev e = __ldg(g.rx_ev + rc);
-        if (e.x != i) break;
-        if (e.y != slot || t + 1 >= g.nt) continue;
-#pragma unroll
-        for (int w = 0; w < W; ++w)
-            if (j0 + w == e.z && g.traces) g.traces[((long long)s * g.nt + t + 1) * g.nrx + e.w] = ezn[w];
-    }
+    fwd_receivers<W>(g, i, t, j0, slot, s, ezn, rc, re);
 #pragma unroll
     for (int k = 0; k < W + 2; ++k) ezc[k] = B.en[k];
 #pragma unroll
@@ -420,6 +527,7 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
     while (cur < nt_) {
         const LaneTile<SHOT> T = decode_tile<W, SHOT>(g, __ldg(g.order + cur), lane);
         if (RING && lane == 0) produce();
+        if (SHOT && !RING && g.pf == 1) prefetch_tile_shot<W>(g, nxt, rp, lane, nullptr, 0);
         const int l = T.l, j0 = T.j0, slot = SHOT ? l : 0;
         const long long go = (long long)T.grp * g.plane;
         const float* ezR = g.ez[rp] + go;
@@ -491,6 +599,7 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
         const int nrow = T.i1 - T.i0;
         for (int n = 0; n < nrow; ++n) {
             const int i = T.i0 + n;
+            if (SHOT && !RING && g.pf == 2 && n == nrow / 2) prefetch_tile_shot<W>(g, nxt, rp, lane, nullptr, 0);
             if (RING) {
                 const bool ok = wait_stage(bars + cslot, cpar);
                 if (!__all_sync(FULL, ok)) {
@@ -575,6 +684,31 @@ __device__ __forceinline__ void adj_e_load(const Dev& g, AdjEIn<W>& A, int r, in
     ld_coef<W + 1, CALIGN<W>>(g, A.cb, g.cb + rb);
 }
 
+// back_source (back.cu:34): Ez -= residual at the receivers of row r, no
+// scaling, in list order: the tile's injection events of the row from ic on.
+template <int W>
+__device__ __forceinline__ void adj_inject(const Dev& g, float (&ez)[W + 1], int r, int j0, int slot, long long resid_o,
+                                           int& ic, int ie) {
+    for (; ic < ie; ++ic) {
+        const Ev e = __ldg(g.inj_ev + ic);
+        if (e.x != r) break;
+        if (e.y != slot) continue;
+#pragma unroll
+        for (int k = 0; k <= W; ++k)
+            if (j0 + k == e.z) ez[k] = __fsub_rn(ez[k], inj_value(g, resid_o + e.w));
+    }
+}
+
+// Interior E of row r, columns j0 .. j0+W, from the old state (hyu = old Hy
+// of row r-1): the E leapfrog of fields_updates_gpu.cu:8-33 with Ucgeta's uE0.
+template <int W>
+__device__ __forceinline__ void adj_e_core(const AdjEIn<W>& A, const float (&hyu)[W + 1], float (&out)[W + 1]) {
+#pragma unroll
+    for (int k = 0; k <= W; ++k)
+        out[k] = __fmaf_rn(-A.cb[k], __fsub_rn(A.hxo[k + 1], A.hxo[k]),
+                           madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
+}
+
 // New E of row r, columns j0 .. j0+W (column j0+W is the halo), from the old
 // state: residuals injected first (list order), then the E update with the
 // old H (hyu = Hy_old of row r-1).  Auxiliaries are stored for the thread's
@@ -584,20 +718,9 @@ template <int W, int CS>
 __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A, int r, int j0,
                                           int l, int slot, bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
                                           long long resid_o, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
-    // back_source (back.cu:34): Ez -= residual, no scaling
-    for (; ic < ie; ++ic) {
-        const Ev e = __ldg(g.inj_ev + ic);
-        if (e.x != r) break;
-        if (e.y != slot) continue;
-#pragma unroll
-        for (int k = 0; k <= W; ++k)
-            if (j0 + k == e.z) A.ez[k] = __fsub_rn(A.ez[k], inj_value(g, resid_o + e.w));
-    }
+    adj_inject<W>(g, A.ez, r, j0, slot, resid_o, ic, ie);
     if (core) {
-#pragma unroll
-        for (int k = 0; k <= W; ++k)
-            out[k] = __fmaf_rn(-A.cb[k], __fsub_rn(A.hxo[k + 1], A.hxo[k]),
-                               madd2(A.ca[k], A.ez[k], A.cb[k], __fsub_rn(A.hyo[k], hyu[k])));
+        adj_e_core<W>(A, hyu, out);
     } else if (CS == 32 && by.lean) {
         if constexpr (CS == 32)
             adj_e_row_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
@@ -649,6 +772,138 @@ __device__ __forceinline__ float lane_reduce_scatter(float (&v)[M], int lane) {
 #pragma unroll
     for (int m = (1 << s) >> 1; m >= 1; m >>= 1) x = __fadd_rn(x, __shfl_xor_sync(FULL, x, m));
     return x;
+}
+
+// Interior H of row i from the new E (ezc: row i, columns j0 .. j0+W; ezr:
+// row i+1) and the old H (hxc from column j0-1, hyc from j0).
+template <int W>
+__device__ __forceinline__ void adj_h_core(const float (&ch)[W], const float (&ezc)[W + 1], const float (&ezr)[W + 1],
+                                           const float (&hxc)[W + 2], const float (&hyc)[W + 1], float (&hx)[W],
+                                           float (&hy)[W]) {
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        hx[w] = __fsub_rn(hxc[w + 1], __fmul_rn(ch[w], __fsub_rn(ezc[w + 1], ezc[w])));
+        hy[w] = __fadd_rn(hyc[w], __fmul_rn(ch[w], __fsub_rn(ezr[w], ezc[w])));
+    }
+}
+
+// Imaging (compute.py:1167-1172) of row i, cells j0 .. j0+W-1, into the fp64
+// accumulators at ge / gs (the row's cell j0).  sum_t (Ez_f[t] - Ez_f[t-1])
+// lambda_t is summed by parts as sum_t Ez_f[t] (lambda_t - lambda_{t+1}) -
+// Ez_f[0] lambda_1: lambda_{t+1} is this step's old Ez (eoc), so the history
+// (f1) is read once per step; k_imaging_tail subtracts the last term.  The
+// sigma sum is sum_t Ez_f[t] lambda_t dt.  Shot lanes sum the warp's 32 shots
+// by a reduce-scatter first, so each cell gets one addition per launch.
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_image(const Dev& g, const float (&f1)[W], const float (&ezc)[W + 1],
+                                          const float (&eoc)[W], double* ge, double* gs, int j0, int lane) {
+    float v[2 * W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+        v[w] = __fmul_rn(f1[w], __fsub_rn(ezc[w], eoc[w]));
+        v[W + w] = __fmul_rn(__fmul_rn(f1[w], ezc[w]), g.dt);
+    }
+    if (SHOT) {
+        constexpr int s = (2 * W) == 4 ? 3 : ((2 * W) == 8 ? 2 : 1);
+        const float x = lane_reduce_scatter<2 * W>(v, lane);
+        if ((lane & ((1 << s) - 1)) == 0) {
+            const int e = lane >> s;   // element index 0 .. 2W-1
+            const int w = e < W ? e : e - W;
+            if (j0 + w < g.ny) acc_add(g, (e < W ? ge : gs) + w, (double)x);
+        }
+    } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+            if (j0 + w < g.ny) {
+                acc_add(g, ge + w, (double)v[w]);
+                acc_add(g, gs + w, (double)v[W + w]);
+            }
+    }
+}
+
+// One iteration of the reference-mode adjoint march for a thread's W cells:
+// the new E of row r = i + 1 from its old operands A (own if r is inside the
+// chunk [.., i1), else the halo row below; nothing when r is the frame row),
+// H of row i from the new E, the imaging sums and the stores; then the
+// carried rows (new E, old H and old Ez of row i) move on to row r.
+template <int W, bool SHOT>
+__device__ __forceinline__ void adj_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A,
+                                        const float (&ch)[W], const float (&f1)[W], float (&ezc)[W + 1],
+                                        float (&hxc)[W + 2], float (&hyc)[W + 1], float (&eoc)[W], int i, int i1,
+                                        int j0, int l, int slot, int lane, bool bcore, long long resid_o, int& ic,
+                                        int ie, const PsiG& rd, const PsiG& wr, float* ezW, float* hxW, float* hyW,
+                                        double* gae, double* gas) {
+    constexpr int CS = SHOT ? 32 : 1;
+    const int r = i + 1;
+    const int P = g.P, nx = g.nx, ny = g.ny, th = g.th;
+    // new E of row r (own if inside the chunk, else the halo row below)
+    float ezr[W + 1], eor[W];
+    if (r < nx) {
+#pragma unroll
+        for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
+        adj_e_row<W, CS>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyc, ezr,
+                         resid_o, ic, ie, rd, wr);
+    } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w) eor[w] = 0.f;
+#pragma unroll
+        for (int k = 0; k <= W; ++k) ezr[k] = A.hyo[k] = 0.f;
+#pragma unroll
+        for (int k = 0; k < W + 2; ++k) A.hxo[k] = 0.f;
+    }
+    // H of row i from the new E
+    float hx[W], hy[W];
+    if (bcore && i >= th + 1 && i <= nx - th - 1) {
+        adj_h_core<W>(ch, ezc, ezr, hxc, hyc, hx, hy);
+    } else if (SHOT && by.lean) {
+        float dzx[W], dzy[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            hx[w] = hxc[w + 1];
+            hy[w] = hyc[w];
+            dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
+            dzy[w] = __fsub_rn(ezr[w], ezc[w]);
+        }
+        if constexpr (SHOT) adj_h_row_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
+    } else if (g.fast_cpml) {
+        float dzx[W], dzy[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            hx[w] = hxc[w + 1];
+            hy[w] = hyc[w];
+            dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
+            dzy[w] = __fsub_rn(ezr[w], ezc[w]);
+        }
+        hx_cells<W, CS>(g, R, i, j0, l, hx, dzx, ch, 0, rd, wr);
+        hy_cells<W, CS, true>(g, R, i, j0, l, hy, dzy, ch, rd, wr);
+    } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const int j = j0 + w;
+            hx[w] = hxc[w + 1];
+            hy[w] = hyc[w];
+            if (j < ny) {
+                hx[w] = hx_cell<CS, true>(g, R, i, j, l, hxc[w + 1], __fsub_rn(ezc[w + 1], ezc[w]), ch[w], rd,
+                                          wr);
+                hy[w] = hy_cell<CS, true>(g, R, i, j, l, hyc[w], __fsub_rn(ezr[w], ezc[w]), ch[w], rd, wr);
+            }
+        }
+    }
+    const long long go2 = (long long)i * ny + j0;
+    adj_image<W, SHOT>(g, f1, ezc, eoc, gae + go2, gas + go2, j0, lane);
+    const long long o = ((long long)i * P + j0 + PADC) * CS + l;
+    st_cells<W, CS>(g, ezW + o, ezc);
+    st_cells<W, CS>(g, hxW + o, hx);
+    st_cells<W, CS>(g, hyW + o, hy);
+#pragma unroll
+    for (int k = 0; k <= W; ++k) {
+        ezc[k] = ezr[k];
+        hyc[k] = A.hyo[k];
+    }
+#pragma unroll
+    for (int w = 0; w < W; ++w) eoc[w] = eor[w];
+#pragma unroll
+    for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
 }
 
 // Stage of adjoint iteration i of tile Q: E operands of row r = i+1 (Ez_old,
@@ -738,6 +993,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
     while (cur < nt_) {
         const LaneTile<SHOT> T = decode_tile<W, SHOT>(g, __ldg(g.order + cur), lane);
         if (RING && lane == 0) produce();
+        if (SHOT && !RING && g.pf == 1) prefetch_tile_shot<W>(g, nxt, rp, lane, g.hist, it);
         const int l = T.l, j0 = T.j0, slot = SHOT ? l : 0;
         // column lanes without cells only take part in the warp's stage protocol
         const bool work = SHOT || T.live;
@@ -788,6 +1044,7 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
         const int nrow = T.i1 - T.i0;
         for (int n = 0; n < nrow; ++n) {
             const int i = T.i0 + n, r = i + 1;
+            if (SHOT && !RING && g.pf == 2 && n == nrow / 2) prefetch_tile_shot<W>(g, nxt, rp, lane, g.hist, it);
             AdjEIn<W> A;
             float ch[W], f1[W];
             if (RING) {
@@ -844,107 +1101,8 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
                     for (int w = 0; w < W; ++w) f1[w] = 0.f;
                 }
             }
-            // new E of row r (own if inside the chunk, else the halo row below)
-            float ezr[W + 1], eor[W];
-            if (r < nx) {
-#pragma unroll
-                for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
-                adj_e_row<W, CS>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < T.i1, hyc, ezr,
-                                 resid_o, ic, ie, rd, wr);
-            } else {
-#pragma unroll
-                for (int w = 0; w < W; ++w) eor[w] = 0.f;
-#pragma unroll
-                for (int k = 0; k <= W; ++k) ezr[k] = A.hyo[k] = 0.f;
-#pragma unroll
-                for (int k = 0; k < W + 2; ++k) A.hxo[k] = 0.f;
-            }
-            // H of row i from the new E
-            float hx[W], hy[W];
-            if (bcore && i >= th + 1 && i <= nx - th - 1) {
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    hx[w] = __fsub_rn(hxc[w + 1], __fmul_rn(ch[w], __fsub_rn(ezc[w + 1], ezc[w])));
-                    hy[w] = __fadd_rn(hyc[w], __fmul_rn(ch[w], __fsub_rn(ezr[w], ezc[w])));
-                }
-            } else if (SHOT && by.lean) {
-                float dzx[W], dzy[W];
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    hx[w] = hxc[w + 1];
-                    hy[w] = hyc[w];
-                    dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
-                    dzy[w] = __fsub_rn(ezr[w], ezc[w]);
-                }
-                if constexpr (SHOT) adj_h_row_shot<W>(g, R, by, i, j0, l, hx, hy, dzx, dzy, ch, rd, wr);
-            } else if (g.fast_cpml) {
-                float dzx[W], dzy[W];
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    hx[w] = hxc[w + 1];
-                    hy[w] = hyc[w];
-                    dzx[w] = __fsub_rn(ezc[w + 1], ezc[w]);
-                    dzy[w] = __fsub_rn(ezr[w], ezc[w]);
-                }
-                hx_cells<W, CS>(g, R, i, j0, l, hx, dzx, ch, 0, rd, wr);
-                hy_cells<W, CS, true>(g, R, i, j0, l, hy, dzy, ch, rd, wr);
-            } else {
-#pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    const int j = j0 + w;
-                    hx[w] = hxc[w + 1];
-                    hy[w] = hyc[w];
-                    if (j < ny) {
-                        hx[w] = hx_cell<CS, true>(g, R, i, j, l, hxc[w + 1], __fsub_rn(ezc[w + 1], ezc[w]), ch[w], rd,
-                                                  wr);
-                        hy[w] = hy_cell<CS, true>(g, R, i, j, l, hyc[w], __fsub_rn(ezr[w], ezc[w]), ch[w], rd, wr);
-                    }
-                }
-            }
-            // imaging (compute.py:1167-1172).  sum_t (Ez_f[t] - Ez_f[t-1]) lambda_t is
-            // summed by parts as sum_t Ez_f[t] (lambda_t - lambda_{t+1}) - Ez_f[0] lambda_1:
-            // lambda_{t+1} is this step's old Ez, so the history is read once
-            // per step; k_imaging_tail subtracts the last term.  The sigma sum is
-            // sum_t Ez_f[t] lambda_t dt.
-            float v[2 * W];
-#pragma unroll
-            for (int w = 0; w < W; ++w) {
-                v[w] = __fmul_rn(f1[w], __fsub_rn(ezc[w], eoc[w]));
-                v[W + w] = __fmul_rn(__fmul_rn(f1[w], ezc[w]), g.dt);
-            }
-            const long long go2 = (long long)i * ny + j0;
-            if (SHOT) {
-                constexpr int s = (2 * W) == 4 ? 3 : ((2 * W) == 8 ? 2 : 1);
-                const float x = lane_reduce_scatter<2 * W>(v, lane);
-                if ((lane & ((1 << s) - 1)) == 0) {
-                    const int e = lane >> s;   // element index 0 .. 2W-1
-                    const int w = e < W ? e : e - W;
-                    if (j0 + w < ny) {
-                        double* a = (e < W ? gae : gas) + go2 + w;
-                        acc_add(g, a, (double)x);
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int w = 0; w < W; ++w)
-                    if (j0 + w < ny) {
-                        acc_add(g, gae + go2 + w, (double)v[w]);
-                        acc_add(g, gas + go2 + w, (double)v[W + w]);
-                    }
-            }
-            const long long o = ((long long)i * P + j0 + PADC) * CS + l;
-            st_cells<W, CS>(g, ezW + o, ezc);
-            st_cells<W, CS>(g, hxW + o, hx);
-            st_cells<W, CS>(g, hyW + o, hy);
-#pragma unroll
-            for (int k = 0; k <= W; ++k) {
-                ezc[k] = ezr[k];
-                hyc[k] = A.hyo[k];
-            }
-#pragma unroll
-            for (int w = 0; w < W; ++w) eoc[w] = eor[w];
-#pragma unroll
-            for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
+            adj_row<W, SHOT>(g, R, by, A, ch, f1, ezc, hxc, hyc, eoc, i, T.i1, j0, l, slot, lane, bcore, resid_o, ic, ie, rd,
+                             wr, ezW, hxW, hyW, gae, gas);
         }
         cur = nxt;
         nxt = cur < nt_ ? fetch_tile(ctr, lane) : nt_;

@@ -214,53 +214,6 @@ __device__ __forceinline__ void produce_tiles(const Dev& g, uint64_t* full, uint
     for (int m = k - S < 0 ? 0 : k - S; m < k; ++m) wait_stage(full + (m % S), (uint32_t)(m / S) & 1u);
 }
 
-// Bulk prefetch of [p, p + bytes) into L2 (no data returned).
-__device__ __forceinline__ void prefetch_l2(const float* p, long long first, long long last) {
-    // [first, last] in floats, widened to 16-byte boundaries
-    const long long a = first & ~3LL, b = (last | 3LL) + 1;
-    if (b <= a) return;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p + a), "r"((uint32_t)((b - a) * 4)) : "memory");
-}
-
-// Prefetch into L2 the CPML auxiliaries (read parity) a tile of rows
-// [r0, r1] and columns [jlo, jhi] touches, so that the consumers' gather
-// loads of a CPML tile hit L2.  Issued by the producer, S tiles ahead.
-template <int CS>
-__device__ __forceinline__ void prefetch_tile_psi(const Dev& g, int grp, int rp, int r0, int r1, int jlo, int jhi) {
-    const int th = g.th, nx = g.nx, ny = g.ny, P = g.P, TY = g.TY;
-    if (th <= 0) return;
-    r0 = max(r0, 0);
-    r1 = min(r1, nx - 1);
-    jlo = max(jlo, 0);
-    jhi = min(jhi, ny - 1);
-    if (r0 > r1 || jlo > jhi) return;
-    const PsiG rd = psi_group(g, rp, grp);
-    // x slabs: E rows 1..th (k = th-i), H rows 0..th-1 (k = th-1-i), both nx-th.. (k = th+i-(nx-th))
-    for (int i = r0; i <= r1; ++i) {
-        const int ke = (i >= 1 && i <= th) ? th - i : (i >= nx - th ? th + i - (nx - th) : -1);
-        const int kh = (i <= th - 1) ? th - 1 - i : (i >= nx - th ? th + i - (nx - th) : -1);
-        if (ke >= 0) prefetch_l2(rd.ex, ((long long)ke * P + jlo) * CS, ((long long)ke * P + jhi) * CS + CS - 1);
-        if (kh >= 0) prefetch_l2(rd.hx, ((long long)kh * P + jlo) * CS, ((long long)kh * P + jhi) * CS + CS - 1);
-    }
-    // y slabs: y0 columns 0..th (k = th-j for E, th-1-j for H), ymax columns ny-th.. (k = j-(ny-th))
-    const bool y0 = jlo <= th, ym = jhi >= ny - th;
-    if (!y0 && !ym) return;
-    const int k0lo = max(0, th - 1 - jhi), k0hi = min(th - 1, th - jlo);
-    const int kmlo = max(jlo, ny - th) - (ny - th), kmhi = jhi - (ny - th);
-    for (int i = r0; i <= r1; ++i) {
-        if (y0 && k0lo <= k0hi) {
-            const long long o = (long long)i * TY;
-            prefetch_l2(rd.ey, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
-            prefetch_l2(rd.hy, (o + k0lo) * CS, (o + k0hi) * CS + CS - 1);
-        }
-        if (ym && kmlo <= kmhi) {
-            const long long o = (long long)(nx + 1 + i) * TY;
-            prefetch_l2(rd.ey, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
-            prefetch_l2(rd.hy, (o + kmlo) * CS, (o + kmhi) * CS + CS - 1);
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Forward step
 // ---------------------------------------------------------------------------

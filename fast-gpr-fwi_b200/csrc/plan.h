@@ -5,6 +5,8 @@
 //   steps_lanes_adj.cu  lane-march adjoint   (fdtd_lanes.cuh)
 //   steps_tiles.cu      tensor-map tile pipelines (fdtd_tile.cuh)
 //   steps_pairs.cu      shot-pair lane march (fdtd_pairs.cuh)
+//   steps_band.cu       band pipelines       (fdtd_band.cuh)
+//   steps_exact.cu      exact adjoint        (fdtd_exact.cuh)
 // Not part of the C ABI (include/fastgpr.h).
 #pragma once
 
@@ -30,10 +32,11 @@ struct fg_plan {
     std::vector<int32_t> src, rx;
     std::vector<float> srcw, pml;
     // launch shape
-    int kernel;         // 0 = tensor-map tiles, 1 = lane march
+    int kernel;         // 0 = tensor-map tiles, 1 = lane march, 2 = band pipeline
     bool shot;          // shot lanes (CS = 32 or, with pair, 64) or column lanes (CS = 1)
     bool pair = false;  // two shots per lane (CS = 64, lane march only)
     int W, TI, WPB, D;  // cells per thread, rows per tile, warps per block, ring stages (0 = direct loads)
+    int pf = 0;         // next-tile L2 prefetch of the lane march (Dev::pf)
     // tensor maps of the tile kernels (encoded when a workspace is bound)
     CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
     int CS, SL;         // floats per cell in a group plane, shots per group
@@ -44,7 +47,7 @@ struct fg_plan {
     std::vector<int> src_off, rx_off, inj_off;
     // workspace layout (byte offsets)
     size_t o_coef, o_state, o_psi, o_chunk, o_order, o_tiles, o_ctr, o_srcev, o_rxev, o_injev, o_offs, o_srcw, o_pml, o_gacc,
-        o_sums, o_partial, o_norms, o_err, total;
+        o_sums, o_partial, o_norms, o_err, o_rxpos, total;
     // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
     int fwd_blocks = 0, adj_blocks = 0;
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
@@ -119,6 +122,17 @@ FwdFn pick_fwd2(int W);                  // shot pairs, forward
 AdjFn pick_adj2(int W);                  // shot pairs, adjoint
 FwdTileFn pick_fwd_tile(bool shot, int W);
 AdjTileFn pick_adj_tile(bool shot, int W);
+FwdFn pick_fwd_band(int W, int C);       // band pipeline (C consumer warps), forward
+AdjFn pick_adj_band(int W, int C);       // band pipeline, adjoint
+// Shared memory of a band-pipeline CTA (0: no kernel of that shape).
+size_t band_smem(int W, int C, int th, int D, bool adjoint);
+// Exact adjoint (steps_exact.cu): one transposed step of every cell and its
+// imaging sums; the receiver injection; the gradient from the sums.
+cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, cudaStream_t st);
+cudaError_t launch_inject_exact(const Dev& g, const int2* rxpos, const float* w, int t, int par, int CS,
+                                cudaStream_t st);
+cudaError_t launch_grad_exact(const double* sums, const float* er, const float* se, int nx, int ny, double a,
+                              float* ge, float* gs, cudaStream_t st);
 // Shared memory of the larger (adjoint) ring of a lane-march plan, or 0 for
 // direct loads; of the larger (adjoint) CTA of a tile-pipeline plan.
 size_t plan_ring_smem(const fg_plan* p);

@@ -98,6 +98,12 @@ typedef struct fg_tuning {
     int32_t adj_warps_per_block;
     int32_t adj_stages;
     int32_t adj_cells_per_thread;
+    /* Lane march with shot lanes and no stages (forward and adjoint): each
+     * warp prefetches into L2 the rows of the tile it will take next, so the
+     * loads of that tile find their lines in L2 instead of waiting for HBM.
+     * 0 = default (1), -1 = off, 1 = when the warp starts its current tile,
+     * 2 = at the current tile's middle row. */
+    int32_t prefetch;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
@@ -158,6 +164,24 @@ int fg_adjoint_reference(fg_plan* plan, const float* er, const float* se, const 
 int fg_adjoint_reference_l1(fg_plan* plan, const float* er, const float* se, const float* mr, const float* hist,
                             const float* traces, const float* observed, float scale, float* grad_eps,
                             float* grad_sig, int32_t normalize, double* norms, void* stream);
+
+/* Exact discrete adjoint of fg_forward: the gradient of
+ * J = sum_{s,t,r} weights[s][t][r] * traces[s][t][r] with respect to the
+ * relative permittivity and the conductivity of every cell, for traces as
+ * fg_forward returns them (the CPML profile held fixed).  No counterpart in
+ * the reference, whose gradient (compute.py:1020-1180, back.cu:8-37) runs the
+ * forward operator in reverse time with Ucgeta's coefficients and the raw
+ * residual, and so is not the derivative of anything: this call transposes
+ * every step of the forward loop (H and E leapfrog, both CPML phases), runs
+ * the transposed steps from the last step back to the first with the weights
+ * injected at the receivers, and forms dJ/d eps_r and dJ/d sigma from the
+ * derivatives of Ucget's E coefficients.  er, se, mr and hist as for
+ * fg_adjoint_reference (hist from fg_forward); weights: (shots, nt, nrx)
+ * float32 (a loss's gradient with respect to the traces); grad_eps /
+ * grad_sig: (nx, ny) float32, either may be NULL.  Not normalised.  Runs on
+ * the plan's adjoint state (like fg_adjoint_reference). */
+int fg_adjoint_exact(fg_plan* plan, const float* er, const float* se, const float* mr, const float* hist,
+                     const float* weights, float* grad_eps, float* grad_sig, void* stream);
 
 /* Checkpointed solve, for histories that do not fit in device memory (the
  * reference keeps the whole Ez history, src/compute.py:553, which limits it

@@ -15,6 +15,13 @@
 //   Forward loop             src/compute.py:574-712
 //   Backward loop + imaging  src/compute.py:1048-1172
 //
+// It also holds the exact discrete adjoint of that forward loop (the
+// transpose of each time step, h_phase_T / e_phase_T below), which the
+// reference does not have: its gradient (compute.py:1020-1180) re-runs the
+// forward operator in reverse time instead.  The exact adjoint is checked by
+// the dot-product test of one step and its transpose and by centred finite
+// differences of the forward loop (tests/test_exact_adjoint.py).
+//
 // Only the TMz components are kept (Ez, Hx, Hy and the Ez/Hx/Hy CPML
 // auxiliaries); Ex, Ey, Hz and their PHI arrays stay identically zero in the
 // reference for a TMz source.  The dead k=1 plane of the reference layout is
@@ -278,6 +285,138 @@ void e_phase(State<T>& st, const Coeffs<T>& k, const T* uE0) {
         }
 }
 
+// ---- Transposes of the two phases (the exact discrete adjoint of a step).
+// A phase is linear in the state; written as F' = F + sum of terms, its
+// transpose maps the adjoint state after the phase (bars) to the one before.
+// Derivative buffers: dzx(s,i,j) / dzy(s,i,j) hold the adjoint of the
+// differences Ez[i][j+1]-Ez[i][j] / Ez[i+1][j]-Ez[i][j] (H phase), and
+// dhx / dhy those of Hx[i][j]-Hx[i][j-1] / Hy[i][j]-Hy[i-1][j] (E phase).
+template <typename T>
+void h_phase_T(State<T>& L, const Coeffs<T>& k) {
+    const int nx = L.nx, ny = L.ny, th = L.th, S = L.S;
+    const size_t N = (size_t)nx * ny;
+    std::vector<T> dzx(N * S, T(0)), dzy(N * S, T(0));
+    auto at = [&](int s, int i, int j) { return (size_t)s * N + (size_t)i * ny + j; };
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                const T u1 = k.uH1[k.c(i, j)];
+                const size_t a = L.at(s, i, j);
+                if (i >= 1) dzx[at(s, i, j)] = -u1 * L.hx[a];   // Hx' = Hx - u1 dzx
+                if (j >= 1) dzy[at(s, i, j)] = u1 * L.hy[a];    // Hy' = Hy + u1 dzy
+            }
+    if (th > 0) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int s = 0; s < S; ++s)
+            for (int j = 0; j < ny; ++j)
+                for (int i1 = 0; i1 < th; ++i1) {
+                    // Hy' += uH4 (ra1 dz/d + RB phi), phi' = RE phi - RF dz/d  (x0 then xmax rows)
+                    for (int side = 0; side < 2; ++side) {
+                        const int ii = side == 0 ? th - 1 - i1 : nx - th + i1;
+                        T& phi = (side == 0 ? L.ph_x0 : L.ph_xm)[((size_t)s * th + i1) * ny + j];
+                        const T hb = L.hy[L.at(s, ii, j)], u4 = k.uH4[k.c(ii, j)];
+                        const T dd = u4 * (k.HRA[i1] - T(1)) * hb - k.HRF[i1] * phi;
+                        phi = k.HRE[i1] * phi + u4 * k.HRB[i1] * hb;
+#pragma omp atomic
+                        dzy[at(s, ii, j)] += dd / k.d;
+                    }
+                }
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int s = 0; s < S; ++s)
+            for (int i = 0; i < nx; ++i)
+                for (int j1 = 0; j1 < th; ++j1) {
+                    // Hx' -= uH4 (ra1 dz/d + RB phi), phi' = RE phi - RF dz/d  (y0 then ymax columns)
+                    for (int side = 0; side < 2; ++side) {
+                        const int jj = side == 0 ? th - 1 - j1 : ny - th + j1;
+                        T& phi = (side == 0 ? L.ph_y0 : L.ph_ym)[((size_t)s * nx + i) * th + j1];
+                        const T hb = L.hx[L.at(s, i, jj)], u4 = k.uH4[k.c(i, jj)];
+                        const T dd = -u4 * (k.HRA[j1] - T(1)) * hb - k.HRF[j1] * phi;
+                        phi = k.HRE[j1] * phi - u4 * k.HRB[j1] * hb;
+#pragma omp atomic
+                        dzx[at(s, i, jj)] += dd / k.d;
+                    }
+                }
+    }
+    // Ez[i][j+1] - Ez[i][j] and Ez[i+1][j] - Ez[i][j]; the zero frame (i == nx,
+    // j == ny) is not part of the state, so its adjoint is dropped
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                T e = L.ez[L.at(s, i, j)] - dzx[at(s, i, j)] - dzy[at(s, i, j)];
+                if (j >= 1) e += dzx[at(s, i, j - 1)];
+                if (i >= 1) e += dzy[at(s, i - 1, j)];
+                L.ez[L.at(s, i, j)] = e;
+            }
+}
+
+template <typename T>
+void e_phase_T(State<T>& L, const Coeffs<T>& k) {
+    const int nx = L.nx, ny = L.ny, th = L.th, S = L.S;
+    const size_t N = (size_t)nx * ny;
+    std::vector<T> dhx(N * S, T(0)), dhy(N * S, T(0)), eb(N * S);
+    auto at = [&](int s, int i, int j) { return (size_t)s * N + (size_t)i * ny + j; };
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                const T e = L.ez[L.at(s, i, j)];
+                eb[at(s, i, j)] = e;
+                if (i >= 1 && j >= 1) {
+                    // Ez' = uE0 Ez + uE1 dHy - uE1 dHx
+                    const size_t c = k.c(i, j);
+                    dhy[at(s, i, j)] = k.uE1[c] * e;
+                    dhx[at(s, i, j)] = -k.uE1[c] * e;
+                    L.ez[L.at(s, i, j)] = k.uE0[c] * e;
+                }
+            }
+    if (th > 0) {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int s = 0; s < S; ++s)
+            for (int j = 0; j < ny; ++j)
+                for (int i2 = 0; i2 < th; ++i2) {
+                    // Ez' += uE4 (ra1 dHy/d + RB phi), phi' = RE phi - RF dHy/d  (x0 then xmax rows)
+                    for (int side = 0; side < 2; ++side) {
+                        const int ii = side == 0 ? th - i2 : nx - th + i2;
+                        T& phi = (side == 0 ? L.pe_x0 : L.pe_xm)[((size_t)s * th + i2) * ny + j];
+                        const T e = eb[at(s, ii, j)], u4 = k.uE4[k.c(ii, j)];
+                        const T dd = u4 * (k.ERA[i2] - T(1)) * e - k.ERF[i2] * phi;
+                        phi = k.ERE[i2] * phi + u4 * k.ERB[i2] * e;
+#pragma omp atomic
+                        dhy[at(s, ii, j)] += dd / k.d;
+                    }
+                }
+#pragma omp parallel for collapse(2) schedule(static)
+        for (int s = 0; s < S; ++s)
+            for (int i = 0; i < nx; ++i)
+                for (int j2 = 0; j2 < th; ++j2) {
+                    // Ez' -= uE4 (ra1 dHx/d + RB phi), phi' = RE phi - RF dHx/d  (y0 then ymax columns)
+                    for (int side = 0; side < 2; ++side) {
+                        const int jj = side == 0 ? th - j2 : ny - th + j2;
+                        T& phi = (side == 0 ? L.pe_y0 : L.pe_ym)[((size_t)s * nx + i) * th + j2];
+                        const T e = eb[at(s, i, jj)], u4 = k.uE4[k.c(i, jj)];
+                        const T dd = -u4 * (k.ERA[j2] - T(1)) * e - k.ERF[j2] * phi;
+                        phi = k.ERE[j2] * phi - u4 * k.ERB[j2] * e;
+#pragma omp atomic
+                        dhx[at(s, i, jj)] += dd / k.d;
+                    }
+                }
+    }
+    // Hy[i][j] - Hy[i-1][j] and Hx[i][j] - Hx[i][j-1]
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int s = 0; s < S; ++s)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                const size_t a = L.at(s, i, j);
+                T hy = L.hy[a] + dhy[at(s, i, j)], hx = L.hx[a] + dhx[at(s, i, j)];
+                if (i + 1 < nx) hy -= dhy[at(s, i + 1, j)];
+                if (j + 1 < ny) hx -= dhx[at(s, i, j + 1)];
+                L.hy[a] = hy;
+                L.hx[a] = hx;
+            }
+}
+
 template <typename T>
 Coeffs<T> make_coeffs(const OracleProblem* p) {
     Coeffs<T> k;
@@ -371,6 +510,86 @@ int adjoint_ref_impl(const OracleProblem* p, const T* hist, const T* g, T* ge, T
     return 0;
 }
 
+// Exact discrete adjoint of forward_impl for the functional
+// J = sum_{s,t,r} w[s][t][r] traces[s][t][r].  traces[t] reads Ez of x_t, the
+// state after t steps (x_0 = 0), and step t maps x_t to x_{t+1} = E(H(x_t)) +
+// source.  The adjoint runs lambda_{nt-1} = R^T w_{nt-1}, lambda_{t-1} =
+// S^T lambda_t + R^T w_{t-1}; the model enters step t-1 only through the E
+// coefficients of x_t's Ez, so the sums
+//   s1 = sum_{t>=1} sum_s lambda_t Ez(x_{t-1}),  s2 = sum_{t>=1} sum_s lambda_t Ez(x_t)
+// (per cell) give the gradient (oracle.adjoint_exact forms it).  hist: the
+// forward's (nt, S, nx, ny) Ez history, hist[t] = Ez of x_{t+1}.
+template <typename T>
+int adjoint_exact_impl(const OracleProblem* p, const T* hist, const T* w, T* s1, T* s2) {
+    const int nx = p->nx, ny = p->ny, S = p->S, nt = p->nt, nrx = p->nrx;
+    State<T> L(nx, ny, p->th, S);
+    Coeffs<T> k = make_coeffs<T>(p);
+    const size_t N = (size_t)nx * ny;
+    for (size_t c = 0; c < N; ++c) { s1[c] = T(0); s2[c] = T(0); }
+    auto inject = [&](int t) {
+        for (int s = 0; s < S; ++s)
+            for (int r = 0; r < nrx; ++r) {
+                const int i = p->rx[((size_t)s * nrx + r) * 2], j = p->rx[((size_t)s * nrx + r) * 2 + 1];
+                if (i < 0) continue;
+                L.ez[L.at(s, i, j)] += w[((size_t)s * nt + t) * nrx + r];
+            }
+    };
+    if (nt < 2) return 0;
+    inject(nt - 1);
+    for (int t = nt - 1; t >= 1; --t) {
+        const T* xt = hist + (size_t)(t - 1) * S * N;
+        const T* xp = t >= 2 ? hist + (size_t)(t - 2) * S * N : nullptr;
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j) {
+                T a = T(0), b = T(0);
+                for (int s = 0; s < S; ++s) {
+                    const size_t h = (size_t)s * N + (size_t)i * ny + j;
+                    const T lam = L.ez[L.at(s, i, j)];
+                    if (xp) a += lam * xp[h];
+                    b += lam * xt[h];
+                }
+                s1[(size_t)i * ny + j] += a;
+                s2[(size_t)i * ny + j] += b;
+            }
+        if (t >= 2) {
+            e_phase_T<T>(L, k);
+            h_phase_T<T>(L, k);
+            inject(t - 1);
+        }
+    }
+    return 0;
+}
+
+// One homogeneous step (no source) of a packed state, or its transpose.
+// Packing: ez, hx, hy (S (nx+1) (ny+1) each), then pe_x0, pe_xm (S th ny),
+// pe_y0, pe_ym (S nx th), ph_x0, ph_xm, ph_y0, ph_ym likewise.
+template <typename T>
+void state_io(State<T>& st, T* buf, bool load) {
+    std::vector<T>* parts[11] = {&st.ez, &st.hx, &st.hy, &st.pe_x0, &st.pe_xm, &st.pe_y0, &st.pe_ym,
+                                 &st.ph_x0, &st.ph_xm, &st.ph_y0, &st.ph_ym};
+    for (auto* v : parts) {
+        if (load) std::memcpy(v->data(), buf, v->size() * sizeof(T));
+        else std::memcpy(buf, v->data(), v->size() * sizeof(T));
+        buf += v->size();
+    }
+}
+template <typename T>
+int step_impl(const OracleProblem* p, const T* in, T* out, int transpose) {
+    State<T> st(p->nx, p->ny, p->th, p->S);
+    Coeffs<T> k = make_coeffs<T>(p);
+    state_io<T>(st, const_cast<T*>(in), true);
+    if (transpose) {
+        e_phase_T<T>(st, k);
+        h_phase_T<T>(st, k);
+    } else {
+        h_phase<T>(st, k);
+        e_phase<T>(st, k, k.uE0);
+    }
+    state_io<T>(st, out, false);
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -389,6 +608,21 @@ int oracle_forward(const OracleProblem* p, void* traces, void* hist) {
     if (!p || !traces) return -1;
     if (p->dtype == 0) return forward_impl<float>(p, (float*)traces, (float*)hist);
     if (p->dtype == 1) return forward_impl<double>(p, (double*)traces, (double*)hist);
+    return -2;
+}
+
+int oracle_adjoint_exact(const OracleProblem* p, const void* hist, const void* w, void* s1, void* s2) {
+    if (!p || !hist || !w || !s1 || !s2) return -1;
+    if (p->dtype == 0) return adjoint_exact_impl<float>(p, (const float*)hist, (const float*)w, (float*)s1, (float*)s2);
+    if (p->dtype == 1)
+        return adjoint_exact_impl<double>(p, (const double*)hist, (const double*)w, (double*)s1, (double*)s2);
+    return -2;
+}
+
+int oracle_step(const OracleProblem* p, const void* in, void* out, int transpose) {
+    if (!p || !in || !out) return -1;
+    if (p->dtype == 0) return step_impl<float>(p, (const float*)in, (float*)out, transpose);
+    if (p->dtype == 1) return step_impl<double>(p, (const double*)in, (double*)out, transpose);
     return -2;
 }
 

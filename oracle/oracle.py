@@ -66,6 +66,11 @@ def _lib(variant: str = "") -> ctypes.CDLL:
         L.oracle_adjoint_ref.argtypes = [ctypes.POINTER(_OracleProblem), ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_adjoint_ref.restype = ctypes.c_int
+        L.oracle_adjoint_exact.argtypes = [ctypes.POINTER(_OracleProblem), ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_adjoint_exact.restype = ctypes.c_int
+        L.oracle_step.argtypes = [ctypes.POINTER(_OracleProblem), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.oracle_step.restype = ctypes.c_int
         L.oracle_set_threads.argtypes = [ctypes.c_int]
         L.oracle_set_threads.restype = ctypes.c_int
         _libs[name] = L
@@ -156,6 +161,77 @@ def adjoint_reference(p: Problem, hist: np.ndarray, resid: np.ndarray, dtype=np.
     if rc:
         raise RuntimeError("oracle_adjoint_ref failed: %d" % rc)
     return ge, gs
+
+
+def exact_sums(p: Problem, hist: np.ndarray, w: np.ndarray, dtype=np.float64):
+    """Imaging sums of the exact discrete adjoint for J = sum w * traces:
+    s1 = sum_t lambda_t Ez(x_{t-1}), s2 = sum_t lambda_t Ez(x_t), each (nx, ny)."""
+    q = p.cast(dtype)
+    s, keep = _struct(q, dtype)
+    h = np.ascontiguousarray(hist, dtype=dtype)
+    g = np.ascontiguousarray(w, dtype=dtype)
+    s1 = np.zeros((q.nx, q.ny), dtype=dtype)
+    s2 = np.zeros((q.nx, q.ny), dtype=dtype)
+    rc = _lib().oracle_adjoint_exact(ctypes.byref(s), h.ctypes.data, g.ctypes.data, s1.ctypes.data, s2.ctypes.data)
+    if rc:
+        raise RuntimeError("oracle_adjoint_exact failed: %d" % rc)
+    return s1, s2
+
+
+def exact_gradient(s1, s2, er, se, dt):
+    """Gradient of J with respect to (eps_r, sigma) from the exact sums.
+
+    Step t-1 makes Ez_t = c0 Ez_{t-1} + uE4 q on a cell whose E is updated by
+    the leapfrog (i, j >= 1; c0 = uE0 = EB/EA) and Ez_t = Ez_{t-1} + uE4 q on
+    the CPML-only cells of rows / columns 0 (c0 = 1), with EA = a er + se/2,
+    EB = a er - se/2, a = e0/dt (e0 the float32 constant of uc.cu:8) and uE4 =
+    1/EA.  Differentiating the coefficients with q fixed:
+      d/der: (a/EA) (Ez_{t-1} - Ez_t)
+      d/dse: -(Ez_{t-1} + Ez_t) / (2 EA)  (leapfrog cells), -(Ez_t - Ez_{t-1}) / (2 EA) (row/column 0)
+    times lambda_t, summed over t and shots.  PEC cells (se > 100) get 0."""
+    er = np.asarray(er, dtype=np.float64)
+    se = np.asarray(se, dtype=np.float64)
+    a = float(np.float32(EPS0)) / dt
+    EA = a * er + 0.5 * se
+    ge = (a / EA) * (s1 - s2)
+    gs = -(s1 + s2) / (2 * EA)
+    edge = np.zeros(er.shape, dtype=bool)
+    edge[0, :] = True
+    edge[:, 0] = True
+    gs[edge] = (-(s2 - s1) / (2 * EA))[edge]
+    pec = se > 100
+    ge[pec] = 0.0
+    gs[pec] = 0.0
+    return ge, gs
+
+
+def state_size(p: Problem) -> int:
+    """Length of a packed state vector (oracle_step's packing)."""
+    F = (p.nx + 1) * (p.ny + 1)
+    return p.shots * (3 * F + 4 * p.th * p.ny + 4 * p.nx * p.th)
+
+
+def frame_mask(p: Problem) -> np.ndarray:
+    """1 on the packed state's entries that are part of the solution space
+    (fields on i < nx, j < ny; every CPML auxiliary), 0 on the zero frame."""
+    F = (p.nx + 1) * (p.ny + 1)
+    f = np.zeros((p.nx + 1, p.ny + 1))
+    f[:p.nx, :p.ny] = 1.0
+    field = np.tile(f.reshape(-1), p.shots)
+    rest = np.ones(state_size(p) - 3 * p.shots * F)
+    return np.concatenate([field, field, field, rest])
+
+
+def step(p: Problem, state: np.ndarray, transpose: bool = False, dtype=np.float64) -> np.ndarray:
+    """One source-free time step of a packed state (or its transpose)."""
+    q = p.cast(dtype)
+    s, keep = _struct(q, dtype)
+    x = np.ascontiguousarray(state, dtype=dtype)
+    out = np.zeros_like(x)
+    rc = _lib().oracle_step(ctypes.byref(s), x.ctypes.data, out.ctypes.data, 1 if transpose else 0)
+    if rc:
+        raise RuntimeError("oracle_step failed: %d" % rc)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -94,3 +94,27 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+def fp64_problem(prob, setup, wl, er=None, se=None):
+    """The oracle problem in double precision with the set-up restated in FP64
+    (coefficients, CPML profile, Ricker) -- the FP64 oracle of the same update
+    equations.  er / se override the workload's model (the CPML profile keeps
+    the workload's, so that it stays fixed under a model perturbation)."""
+    er = np.maximum(wl.er, 1) if er is None else er
+    se = np.maximum(wl.se, 0) if se is None else se
+    f64 = orc.coefficients_fp64(er, se, wl.mr, setup.dt32, setup.dx)
+    p64 = prob.cast(np.float64)
+    for k, v in f64.items():
+        setattr(p64, k, v)
+    er_avg = float(np.mean(np.maximum(wl.er, 1)[0, :].astype(np.float64)))
+    p64.pml = orc.cpml_fp64(setup.th, setup.dx, er_avg, 1.0, setup.dt32)
+    p64.srcw = np.zeros_like(prob.srcw, dtype=np.float64)
+    p64.srcw[0] = orc.ricker_fp64(setup.nt, setup.dt32, (wl.nt - 1.5) * wl.dt, 1.0, wl.freq, setup.dx)
+    return p64
+
+
+def bump(nx, ny, ci, cj, width):
+    """Smooth (nx, ny) perturbation: a Gaussian of the given width (cells)."""
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    return np.exp(-(((i - ci) / width) ** 2 + ((j - cj) / width) ** 2))

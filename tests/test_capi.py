@@ -96,7 +96,7 @@ def test_checkpoint_sizes_and_adjoint_tuning_without_gpu(fg):
     assert L.fg_plan_checkpoint_bytes(h, 1) == (nt - 1) * one
     assert L.fg_plan_checkpoint_bytes(h, 0) == -1
     L.fg_plan_destroy(h)
-    bad = nat.FgTuning(*([0] * 6 + [3, 0, 0, 0]))     # adj_kernel 3 does not exist
+    bad = nat.FgTuning(*([0] * 6 + [4, 0, 0, 0]))     # adj_kernel 4 does not exist
     assert L.fg_plan_create(ctypes.byref(prob), ctypes.byref(bad), ctypes.byref(h)) == nat.FG_ERR_INVALID
     assert b"adj_kernel" in L.fg_last_error()
     ok = nat.FgTuning(*([0] * 6 + [2, 3, 2, 0]))      # lane-march adjoint

@@ -142,6 +142,15 @@ TUNINGS = [
     {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 1, "adj_rows_per_tile": 4,
      "adj_warps_per_block": 4, "adj_stages": 2, "adj_cells_per_thread": 8},
     {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 4, "adj_kernel": 2, "adj_cells_per_thread": 4},
+    # band pipeline (the adjoint follows the forward's shape)
+    {"kernel": 2, "lanes": 1, "cells_per_thread": 4, "warps_per_block": 4, "rows_per_tile": 7, "stages": 3},
+    {"kernel": 2, "lanes": 1, "cells_per_thread": 2, "warps_per_block": 4, "rows_per_tile": 16},
+    {"kernel": 2, "lanes": 1, "cells_per_thread": 4, "warps_per_block": 2, "rows_per_tile": 1, "stages": 2},
+    {"kernel": 2, "lanes": 1, "cells_per_thread": 2, "warps_per_block": 8, "rows_per_tile": 64, "stages": 8},
+    # band-pipeline adjoint behind other forwards
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "adj_kernel": 3, "adj_rows_per_tile": 9,
+     "adj_cells_per_thread": 4, "adj_warps_per_block": 4, "adj_stages": 4},
+    {"lanes": 1, "adj_kernel": 3, "adj_cells_per_thread": 2, "adj_warps_per_block": 8},
 ]
 
 
