@@ -59,11 +59,6 @@ PKG = "fast-gpr-fwi_b200"
 METRIC = "Gcell-steps/s fwd+adjoint"
 UNIT = "Gcell-steps/s"
 
-# DRAM bytes per shot-cell-step of the default step kernels (forward: lane
-# march, adjoint: tile pipeline), from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch on the 64-shot 440x340 grid, summarised
-# under profiles/): forward 262.0 MB, adjoint 280.5 MB per launch over
-# 64 x 440 x 340 shot-cells.
 # DRAM bytes per shot-cell-step of each step kernel, from one ncu capture on the 440 x 340 grid with 64 shots
 # (read + write); a kernel with no capture reports null traffic
 NCU_BYTES_PER_SHOT_CELL_STEP = {"fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340),
@@ -365,6 +360,10 @@ def run_ours(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(wl, setup, args.cpu_seconds)
 
+    fp64 = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        fp64 = fp64_error(fg, wl, dev, tuning)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -388,6 +387,7 @@ def run_ours(args, rank, local, world):
             "per_shot_path": per_shot,
             "serving": serving,
             "cpu_baseline": cpu,
+            "fp64_err": fp64,
         }
         print(json.dumps(line), flush=True)
 
@@ -590,6 +590,44 @@ def cpu_baseline(wl, setup, seconds):
     return {"value": round(cells / t / 1e9, 4), "unit": UNIT, "cores": threads, "kind": "port",
             "sample": _sample_text(wl, shots, nt, batches) + ", FP32 C++/OpenMP oracle, %.1f s" % t,
             "cpu": _cpu_model()}
+
+
+def fp64_error(fg, wl, dev, tuning, shots=8, nt=300):
+    """Relative L2 error of the benchmark's FP32 solve against the FP64 oracle
+    of the same update equations, on a bounded sample of the workload: its
+    first `shots` shots over its first `nt` steps, solved on the GPU with the
+    benchmark's launch shape and on the host in double precision (FP64
+    coefficients, CPML profile and Ricker).  Traces, the reference-mode
+    gradient (unit norm, as the step returns it) and the exact adjoint's
+    gradient of the same weights."""
+    from oracle import oracle as orc
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers
+    if wl.name != "config2":
+        return None
+    sample = fg.workloads.config2(shots=shots, nt=nt)
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(64)
+    w = rng.standard_normal((shots, nt, sample.nrx)).astype(np.float32)
+    prob, setup = helpers.oracle_problem_from_gpu(fg, sample, dev)
+    p64 = helpers.fp64_problem(prob, setup, sample)
+    o_tr, o_hist = orc.forward(p64, np.float64)
+    oe, os_ = orc.adjoint_reference(p64, o_hist, w, np.float64)
+    oe /= np.linalg.norm(oe)
+    os_ /= np.linalg.norm(os_)
+    s1, s2 = orc.exact_sums(p64, o_hist, w.astype(np.float64))
+    xe, xs = orc.exact_gradient(s1, s2, np.maximum(sample.er, 1), np.maximum(sample.se, 0), setup.dt32)
+    del o_hist
+    wt = torch.tensor(w, device=dev)
+    tr, ge, gs = helpers.run_package(fg, sample, dev, wt, tuning=tuning)
+    _, ee, es = helpers.run_package(fg, sample, dev, wt, adjoint="exact")
+    r = lambda a, b: round(helpers.rel_l2(a.cpu().numpy(), b), 9)
+    out = {"sample": "%s grid %dx%d, shots 0-%d, first %d of %d steps; FP32 GPU solve vs FP64 oracle"
+                     % (wl.name, sample.nx, sample.ny, shots - 1, nt, wl.nt),
+           "traces": r(tr, o_tr), "g_eps": r(ge, oe), "g_sig": r(gs, os_),
+           "exact_g_eps": r(ee, xe), "exact_g_sig": r(es, xs), "seconds": round(time.perf_counter() - t0, 1)}
+    torch.cuda.empty_cache()
+    return out
 
 
 def _cpu_model():

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdint>
 #include <vector>
 
 #include <cuda.h>
@@ -53,6 +54,7 @@ struct fg_plan {
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
     float dinv = 0.f;
     int div_scaled = 0;   // the scaled step matches __fdiv_rn for every |x| < 2^31 (checked at bind)
+    uint64_t id = 0;    // unique per plan in the process (which plan last filled the static scratch)
     // the adjoint's own plan (own state, coefficients, accumulators and launch
     // shape); its workspace follows this plan's in the caller's workspace
     fg_plan* adj = nullptr;

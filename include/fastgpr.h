@@ -9,9 +9,9 @@
  *   fg_coefficients       replaces Ucget / Ucgeta          (src/lib/uc.cu:48, :94)
  *   fg_forward            replaces, per time step, launch_store_outputs
  *                         (sourcereceiver.cu:40), h_fields_updates
- *                         (fields_updates_gpu.cu:183), order1_* H
+ *                         (fields_updates_gpu.cu:80), order1_* H
  *                         (pml_updates_h.cu:84-661), e_fields_updates
- *                         (fields_updates_gpu.cu:138), order1_* E
+ *                         (fields_updates_gpu.cu:35), order1_* E
  *                         (pml_updates_e.cu:80-633), update_hertzian_dipole
  *                         (sourcereceiver.cu:89) and the Ez history copy
  *                         (src/compute.py:712) -- the loop of compute.py:574-712
@@ -21,10 +21,15 @@
  *
  * Conventions
  *   - All array arguments are device pointers unless marked HOST.
- *   - Every call is asynchronous on the given stream (cudaStream_t passed as
- *     void*; NULL = legacy default stream) and returns an FG_* status; no call
- *     synchronises the device.  fg_last_error() gives the message of the most
- *     recent failure on the calling thread.
+ *   - Every call is queued on the given stream (cudaStream_t passed as
+ *     void*; NULL = legacy default stream) and returns an FG_* status.  The
+ *     solves return without waiting; the calls that wait for their stream are
+ *     fg_plan_bind (the plan's tables must stay valid until uploaded),
+ *     fg_total_variation (it returns the iteration count), fg_plan_check and
+ *     fg_forward_static when it uploads a plan's tables (see there); the first
+ *     bind of a cell size on a device also runs its division check and waits
+ *     for it.  fg_last_error() gives the message of the most recent failure
+ *     on the calling thread.
  *   - The caller owns every buffer.  A plan owns only host-side tables; its
  *     device scratch (fields, CPML auxiliaries, event tables, gradient
  *     accumulators) lives in a caller-allocated workspace of
@@ -221,13 +226,18 @@ int fg_adjoint_reference_checkpointed(fg_plan* plan, const float* er, const floa
  * process exits.  The plan's own workspace binding (fg_plan_bind), if any,
  * is left as it was.
  *
- *   - A plan whose fg_plan_workspace_bytes exceeds FG_STATIC_SCRATCH_BYTES
- *     is rejected with FG_ERR_WORKSPACE before any device work.
+ *   - A plan whose forward scratch exceeds FG_STATIC_SCRATCH_BYTES is
+ *     rejected with FG_ERR_WORKSPACE before any device work.  That is the
+ *     forward plan's own share of fg_plan_workspace_bytes (which also counts
+ *     the adjoint plan's scratch), so a plan whose workspace bytes exceed the
+ *     array may still fit.
  *   - The first call on a device looks up the array's device address (with
  *     that device current) and keeps it; make that first call before any
  *     stream capture.
- *   - The call waits for `stream` once, after uploading the plan's tables
- *     (as fg_plan_bind does), then queues the solve asynchronously.
+ *   - When the array of the device does not hold this plan's tables (the
+ *     plan's first call there, or another plan called in between), the call
+ *     uploads them and waits for `stream` (as fg_plan_bind does); otherwise
+ *     it only queues the solve.
  *   - Every call on a device shares the one array and the array keeps what
  *     the last call left in it; each call clears the field state it needs.
  *     Calls whose work overlaps on the GPU (other streams, other threads)

@@ -130,12 +130,12 @@ void h_phase(State<T>& st, const Coeffs<T>& k) {
             for (int j = 0; j < ny; ++j) {
                 const size_t a = st.at(s, i, j);
                 const T u1 = k.uH1[k.c(i, j)];
-                // Hx: i in [1, nx), j in [0, ny)   (fields_updates_gpu.cu:162-170)
+                // Hx: i in [1, nx), j in [0, ny)   (fields_updates_gpu.cu:57-64)
                 if (i >= 1) {
                     const T dz = st.ez[st.at(s, i, j + 1)] - st.ez[a];
                     st.hx[a] = msub2<T>(T(1), st.hx[a], u1, dz);
                 }
-                // Hy: i in [0, nx), j in [1, ny)   (fields_updates_gpu.cu:172-180)
+                // Hy: i in [0, nx), j in [1, ny)   (fields_updates_gpu.cu:67-76)
                 if (j >= 1) {
                     const T dz = st.ez[st.at(s, i + 1, j)] - st.ez[a];
                     st.hy[a] = madd2<T>(T(1), st.hy[a], u1, dz);
@@ -214,7 +214,7 @@ void e_phase(State<T>& st, const Coeffs<T>& k, const T* uE0) {
     for (int s = 0; s < S; ++s)
         for (int i = 1; i < nx; ++i)
             for (int j = 1; j < ny; ++j) {
-                // fields_updates_gpu.cu:124-134
+                // fields_updates_gpu.cu:21-32
                 const size_t a = st.at(s, i, j);
                 const size_t c = k.c(i, j);
                 const T dHy = st.hy[a] - st.hy[st.at(s, i - 1, j)];
@@ -480,7 +480,7 @@ int adjoint_ref_impl(const OracleProblem* p, const T* hist, const T* g, T* ge, T
     const size_t N = (size_t)nx * ny;
     for (size_t c = 0; c < N; ++c) { ge[c] = T(0); gs[c] = T(0); }
     for (int it = nt - 1; it >= 1; --it) {
-        // Back_source (back.cu:124-143): raw residual, no scaling
+        // Back_source (back.cu:8-37, the subtraction at :33-34): raw residual, no scaling
         for (int s = 0; s < S; ++s)
             for (int r = 0; r < nrx; ++r) {
                 const int i = p->rx[((size_t)s * nrx + r) * 2], j = p->rx[((size_t)s * nrx + r) * 2 + 1];

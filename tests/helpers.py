@@ -118,3 +118,42 @@ def bump(nx, ny, ci, cj, width):
     """Smooth (nx, ny) perturbation: a Gaussian of the given width (cells)."""
     i, j = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
     return np.exp(-(((i - ci) / width) ** 2 + ((j - cj) / width) ** 2))
+
+
+def run_package(fg, wl, dev, w, tuning=None, tv=False, adjoint="reference"):
+    """compute() + backward of sum(w * traces): (traces, g_eps, g_sig) on the device."""
+    er = torch.tensor(np.ascontiguousarray(wl.er[:, :, None]), device=dev, requires_grad=True)
+    se = torch.tensor(np.ascontiguousarray(wl.se[:, :, None]), device=dev, requires_grad=True)
+    traces, dt = fg.compute(**wl.kwargs(dev, er=er, se=se, tv=tv, tuning=tuning, adjoint=adjoint))
+    (traces * w).sum().backward()
+    torch.cuda.synchronize()
+    return traces.detach(), er.grad[:, :, 0].detach(), se.grad[:, :, 0].detach()
+
+
+def run_reference(refdrv, wl, dev, w):
+    """The reference's CUDA kernels driven as its Python driver drives them
+    (oracle/ref_driver.py): (grid, traces, g_eps, g_sig)."""
+    kw = wl.kwargs(dev)
+    er = torch.clamp(kw["er"], min=1)
+    se = torch.clamp(kw["se"], min=0)
+    G = refdrv.setup(dev, kw["dx"], kw["ny"], kw["nx"], 1, kw["time_windows"], kw["source_location"],
+                     kw["source_step"], kw["receiver_location"], kw["receiver_step"], kw["pmlthick"],
+                     kw["source_apmlitudes"], kw["step"], er, se, kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"],
+                     kw["Fixedreceiver"])
+    rxs, hist = refdrv.forward(G)
+    ge, gs = refdrv.backward(G, er, se, kw["mr"], hist, w)
+    return G, rxs[:, 2].contiguous(), ge[:, :, 0], gs[:, :, 0]
+
+
+def edge_workload(fg, nx, ny, pml, shots=3, nt=60):
+    """A small seeded case on an nx x ny grid with `pml` CPML cells, the
+    source and receivers inside the grid."""
+    wl = fg.workloads.small(seed=nx * 100 + ny + pml, nx=nx, ny=ny, shots=shots, nt=nt, pml=min(pml, 6) if pml else 0,
+                            nrx=3)
+    wl.pml = pml
+    dx = wl.dx
+    wl.source_location = [dx * (nx // 3), dx * (ny // 3), 0.0]
+    wl.source_step = [dx, 0.0, 0.0] if shots < nx // 3 else [0.0, 0.0, 0.0]
+    wl.receiver_location = [dx * (nx // 2), dx * (2 * ny // 3), 0.0]
+    wl.receiver_step = [dx, 0.0, 0.0]
+    return wl

@@ -58,16 +58,20 @@ def test_forward_static_rejects_plans_beyond_the_static_scratch(fg):
 
 
 @pytest.mark.gpu
-def test_forward_static_matches_forward(fg):
+@pytest.mark.parametrize("tuning", [None, {"kernel": 0, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4},
+                                    {"kernel": 2, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 8}])
+def test_forward_static_matches_forward(fg, tuning):
     """Two calls in a row through the C ABI give the traces and history of
-    fg_forward bit for bit (the forward tests' tolerance)."""
+    fg_forward bit for bit (the forward tests' tolerance), for the default
+    launch shape, the tile pipeline (whose tensor maps are pointed at the
+    array and back) and the band pipeline."""
     assert torch.cuda.is_available(), "GPU tests need a CUDA device"
     dev = torch.device("cuda:0")
     nat = helpers.native_mod()
     L = nat.lib()
     wl = fg.workloads.small(shots=3, nt=90)
     setup = helpers.setup_for(wl, dev)
-    solve = fg.Solve(dev, setup, tv=False)
+    solve = fg.Solve(dev, setup, tv=False, tuning=tuning)
     assert L.fg_plan_workspace_bytes(solve.plan.handle) <= 32 * 1024 * 1024
     er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
     want_tr, want_hist = solve.forward(er, se, mr)
@@ -85,3 +89,28 @@ def test_forward_static_matches_forward(fg):
     tr2, hist2 = solve.forward(er, se, mr)
     torch.cuda.synchronize()
     assert torch.equal(tr2, want_tr) and torch.equal(hist2, want_hist)
+
+
+@pytest.mark.gpu
+def test_forward_static_two_plans_in_turn(fg):
+    """Plans that take turns re-upload their tables into the shared array:
+    A, B, A again each match their own fg_forward."""
+    dev = torch.device("cuda:0")
+    nat = helpers.native_mod()
+    L = nat.lib()
+    runs = []
+    for wl in (fg.workloads.small(shots=3, nt=80), fg.workloads.small(seed=3, shots=2, nt=60, nx=40, ny=56, pml=5)):
+        solve = fg.Solve(dev, helpers.setup_for(wl, dev), tv=False)
+        er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+        want = solve.forward(er, se, mr)
+        runs.append((solve, (er, se, mr), want))
+    torch.cuda.synchronize()
+    stream = nat.stream_handle(dev)
+    for k in (0, 1, 0):
+        solve, (er, se, mr), (want_tr, want_hist) = runs[k]
+        tr = torch.full_like(want_tr, float("nan"))
+        hist = torch.full_like(want_hist, float("nan"))
+        nat.check(L.fg_forward_static(solve.plan.handle, er.data_ptr(), se.data_ptr(), mr.data_ptr(),
+                                      tr.data_ptr(), hist.data_ptr(), stream))
+        torch.cuda.synchronize()
+        assert torch.equal(tr, want_tr) and torch.equal(hist, want_hist), "plan %d" % k
