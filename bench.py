@@ -592,12 +592,13 @@ def cpu_baseline(wl, setup, seconds):
             "cpu": _cpu_model()}
 
 
-def fp64_error(fg, wl, dev, tuning, shots=8, nt=300):
+def fp64_error(fg, wl, dev, tuning, shots=4, nt=1000):
     """Relative L2 error of the benchmark's FP32 solve against the FP64 oracle
     of the same update equations, on a bounded sample of the workload: its
-    first `shots` shots over its first `nt` steps, solved on the GPU with the
-    benchmark's launch shape and on the host in double precision (FP64
-    coefficients, CPML profile and Ricker).  Traces, the reference-mode
+    first `shots` shots over its first `nt` steps (long enough for the forward
+    and adjoint fields to meet between the boreholes), solved on the GPU with
+    the benchmark's launch shape (shot lanes) and on the host in double
+    precision (FP64 coefficients, CPML profile and Ricker).  Traces, the reference-mode
     gradient (unit norm, as the step returns it) and the exact adjoint's
     gradient of the same weights."""
     from oracle import oracle as orc
@@ -619,8 +620,9 @@ def fp64_error(fg, wl, dev, tuning, shots=8, nt=300):
     xe, xs = orc.exact_gradient(s1, s2, np.maximum(sample.er, 1), np.maximum(sample.se, 0), setup.dt32)
     del o_hist
     wt = torch.tensor(w, device=dev)
-    tr, ge, gs = helpers.run_package(fg, sample, dev, wt, tuning=tuning)
-    _, ee, es = helpers.run_package(fg, sample, dev, wt, adjoint="exact")
+    shot_lanes = dict(tuning or {}, lanes=1)
+    tr, ge, gs = helpers.run_package(fg, sample, dev, wt, tuning=shot_lanes)
+    _, ee, es = helpers.run_package(fg, sample, dev, wt, tuning=shot_lanes, adjoint="exact")
     r = lambda a, b: round(helpers.rel_l2(a.cpu().numpy(), b), 9)
     out = {"sample": "%s grid %dx%d, shots 0-%d, first %d of %d steps; FP32 GPU solve vs FP64 oracle"
                      % (wl.name, sample.nx, sample.ny, shots - 1, nt, wl.nt),

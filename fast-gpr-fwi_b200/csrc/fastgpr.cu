@@ -1011,12 +1011,17 @@ int fg_adjoint_exact(fg_plan* p, const float* er, const float* se, const float* 
     g.out_hi = (const char*)(hist + (size_t)a->nt * hist_step_floats(a));
     const int2* rxpos = (const int2*)(a->ws + a->o_rxpos);
     const int nt = a->nt;
+    // row 0 and column 0 stay zero in the forward unless a source lies on them
+    int proj = 1;
+    for (size_t k = 0; k + 2 < a->src.size(); k += 3)
+        if (classify(a, a->src[k], a->src[k + 1], a->src[k + 2]) == 1 && (a->src[k] == 0 || a->src[k + 1] == 0))
+            proj = 0;
     if (nt >= 2) {
         // lambda_{nt-1} = R^T w_{nt-1} in parity 0; iteration it reads parity (nt-1-it) & 1
         if (a->nrx > 0) FG_CUDA(launch_inject_exact(g, rxpos, weights, nt - 1, 0, a->CS, st));
         for (int it = nt - 1; it >= 1; --it) {
             const int rp = (nt - 1 - it) & 1;
-            FG_CUDA(launch_adj_exact(g, it, rp, a->CS, st));
+            FG_CUDA(launch_adj_exact(g, it, rp, a->CS, proj, st));
             if (it >= 2 && a->nrx > 0) FG_CUDA(launch_inject_exact(g, rxpos, weights, it - 1, rp ^ 1, a->CS, st));
         }
     }

@@ -133,8 +133,18 @@ struct ExactView {
 // One adjoint iteration it (lambda_it -> H^T E^T lambda_it) for every cell and
 // shot slot, plus the imaging sums of lambda_it.  One thread per (group, cell,
 // slot), slot fastest.
+//
+// proj: row 0 (Ez, Hx and the y-slab auxiliaries of the row) and column 0
+// (Ez, Hy and the x-slab auxiliaries of the column) are closed subsystems of
+// the forward step -- updated only by the CPML terms of their own cells, they
+// feed the rest of the grid without being fed by it -- so with no source on
+// them they stay exactly zero in the forward and no functional depends on
+// them.  Their transposed dynamics (an unstable CPML-only recursion that the
+// rest of the grid drives in the adjoint) would overflow in FP32 after a few
+// hundred steps; with proj set their adjoint is held at zero, which leaves
+// the gradient unchanged.
 template <int CS>
-__global__ void __launch_bounds__(256) k_adj_exact(const Dev g, const int it, const int rp) {
+__global__ void __launch_bounds__(256) k_adj_exact(const Dev g, const int it, const int rp, const int proj) {
     extern __shared__ __align__(16) float Rs[];
     for (int k = threadIdx.x; k < 8 * g.th; k += blockDim.x) Rs[k] = __ldg(g.pml + k);
     __syncthreads();
@@ -187,15 +197,19 @@ __global__ void __launch_bounds__(256) k_adj_exact(const Dev g, const int it, co
     e = __fsub_rn(e, V.dzy(i, j, hym));
     if (j >= 1) e = __fadd_rn(e, V.dzx(i, j - 1, V.hx_mid(i, j - 1)));
     if (i >= 1) e = __fadd_rn(e, V.dzy(i - 1, j, V.hy_mid(i - 1, j)));
-    st1(g, g.ez[wp] + go + c, e);
-    st1(g, g.hx[wp] + go + c, hxm);
-    st1(g, g.hy[wp] + go + c, hym);
+    const bool row0 = proj && i == 0, col0 = proj && j == 0;
+    st1(g, g.ez[wp] + go + c, (row0 || col0) ? 0.f : e);
+    st1(g, g.hx[wp] + go + c, row0 ? 0.f : hxm);
+    st1(g, g.hy[wp] + go + c, col0 ? 0.f : hym);
     if (th <= 0) return;
     // auxiliaries: psi' = RE psi - RF D gives psi_bar = RE psi_bar' + (coefficient of psi in the field update) F_bar'
     const float u4 = ldro(g, g.cd + V.coef(i, j)), h4 = ldro(g, g.ci + V.coef(i, j));
     const float* HR = Rs + 4 * th;
+    // x-slab auxiliaries of column 0 and y-slab auxiliaries of row 0 are held
+    // at zero with proj (see above)
     auto upd = [&](const float* src, float* dst, long long o, float re, float coefb) {
-        st1(g, dst + o, __fmaf_rn(re, ldro(g, src + o), coefb));
+        const bool zero = (src == rd.ex || src == rd.hx) ? col0 : row0;
+        st1(g, dst + o, zero ? 0.f : __fmaf_rn(re, ldro(g, src + o), coefb));
     };
     if (i >= 1 && i <= th) {   // E x0
         const int k = th - i;

@@ -130,7 +130,7 @@ AdjFn pick_adj_band(int W, int C);       // band pipeline, adjoint
 size_t band_smem(int W, int C, int th, int D, bool adjoint);
 // Exact adjoint (steps_exact.cu): one transposed step of every cell and its
 // imaging sums; the receiver injection; the gradient from the sums.
-cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, cudaStream_t st);
+cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, int proj, cudaStream_t st);
 cudaError_t launch_inject_exact(const Dev& g, const int2* rxpos, const float* w, int t, int par, int CS,
                                 cudaStream_t st);
 cudaError_t launch_grad_exact(const double* sums, const float* er, const float* se, int nx, int ny, double a,

@@ -4,12 +4,12 @@
 
 namespace fgk {
 
-cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, cudaStream_t st) {
+cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, int proj, cudaStream_t st) {
     const long long n = (long long)g.ngroups * g.nx * g.ny * CS;
     const unsigned blocks = (unsigned)((n + 255) / 256);
     const size_t smem = (size_t)8 * g.th * sizeof(float);
-    if (CS == 32) fg::k_adj_exact<32><<<blocks, 256, smem, st>>>(g, it, rp);
-    else if (CS == 1) fg::k_adj_exact<1><<<blocks, 256, smem, st>>>(g, it, rp);
+    if (CS == 32) fg::k_adj_exact<32><<<blocks, 256, smem, st>>>(g, it, rp, proj);
+    else if (CS == 1) fg::k_adj_exact<1><<<blocks, 256, smem, st>>>(g, it, rp, proj);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }

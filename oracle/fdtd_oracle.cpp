@@ -534,6 +534,37 @@ int adjoint_exact_impl(const OracleProblem* p, const T* hist, const T* w, T* s1,
                 L.ez[L.at(s, i, j)] += w[((size_t)s * nt + t) * nrx + r];
             }
     };
+    // Row 0 (Ez, Hx, the y-slab auxiliaries of row 0) and column 0 (Ez, Hy,
+    // the x-slab auxiliaries of column 0) form closed subsystems of the
+    // forward step: they are updated only by the CPML terms of their own
+    // cells and feed the rest of the grid without being fed by it.  With no
+    // source on them they stay exactly zero in the forward, so no J depends
+    // on them; their transposed dynamics (an unstable CPML-only recursion,
+    // whose adjoint the rest of the grid drives) are projected out, which
+    // keeps the adjoint finite without changing the gradient.
+    bool edge_src = false;
+    for (int q = 0; q < S * p->nsrc; ++q)
+        if (p->src[2 * q] == 0 || p->src[2 * q + 1] == 0) edge_src = true;
+    auto project = [&]() {
+        if (edge_src) return;
+        for (int s = 0; s < S; ++s) {
+            for (int j = 0; j < ny; ++j) {
+                L.ez[L.at(s, 0, j)] = T(0);
+                L.hx[L.at(s, 0, j)] = T(0);
+            }
+            for (int i = 0; i < nx; ++i) {
+                L.ez[L.at(s, i, 0)] = T(0);
+                L.hy[L.at(s, i, 0)] = T(0);
+            }
+            const int th = p->th;
+            for (int q = 0; q < th; ++q) {
+                L.pe_y0[((size_t)s * nx + 0) * th + q] = L.pe_ym[((size_t)s * nx + 0) * th + q] = T(0);
+                L.ph_y0[((size_t)s * nx + 0) * th + q] = L.ph_ym[((size_t)s * nx + 0) * th + q] = T(0);
+                L.pe_x0[((size_t)s * th + q) * ny + 0] = L.pe_xm[((size_t)s * th + q) * ny + 0] = T(0);
+                L.ph_x0[((size_t)s * th + q) * ny + 0] = L.ph_xm[((size_t)s * th + q) * ny + 0] = T(0);
+            }
+        }
+    };
     if (nt < 2) return 0;
     inject(nt - 1);
     for (int t = nt - 1; t >= 1; --t) {
@@ -555,6 +586,7 @@ int adjoint_exact_impl(const OracleProblem* p, const T* hist, const T* w, T* s1,
         if (t >= 2) {
             e_phase_T<T>(L, k);
             h_phase_T<T>(L, k);
+            project();
             inject(t - 1);
         }
     }

@@ -3,7 +3,9 @@
   - config 1 (240x160, 13 shots, nt 3000): traces and both reference-mode
     gradients against the reference's own CUDA kernels (oracle/ref_driver.py),
     and against the FP64 oracle over its first 1000 steps;
-  - a config-2 sample (440x340, all 64 shots, 300 steps): traces and
+  - a config-2 sample (440x340, all 64 shots, 1000 steps -- long enough for
+    the forward and adjoint fields to meet between the source and receiver
+    boreholes, so the gradient is not zero): traces and
     gradients against the reference's kernels, for the default launch shape
     and the band pipeline;
   - every grid nx, ny in {17, 33, 65} with CPML 0, 1 and 8 cells, through the
@@ -51,6 +53,7 @@ def _vs_reference(fg, refdrv, wl, dev, tuning=None, seed=17):
     _, rtr, rge, rgs = helpers.run_reference(refdrv, wl, dev, w)
     errs = [helpers.rel_l2(a.cpu().numpy(), b.cpu().numpy()) for a, b in ((tr, rtr), (ge, rge), (gs, rgs))]
     print("%s (%s) vs reference kernels: traces %.3g, g_eps %.3g, g_sig %.3g" % (wl.name, tuning, *errs))
+    assert all(np.isfinite(e) for e in errs) and ge.abs().max() > 0 and gs.abs().max() > 0
     return errs
 
 
@@ -74,12 +77,12 @@ def test_config1_vs_fp64_oracle(fg, orc, dev):
     errs = (helpers.rel_l2(tr.cpu().numpy(), o_tr), helpers.rel_l2(ge.cpu().numpy(), oe),
             helpers.rel_l2(gs.cpu().numpy(), os_))
     print("config1 (nt 1000) vs FP64 oracle: traces %.3g, g_eps %.3g, g_sig %.3g" % errs)
-    assert max(errs) <= TOL_FP64
+    assert all(np.isfinite(e) for e in errs) and max(errs) <= TOL_FP64
 
 
 @pytest.mark.parametrize("tuning", [None, BAND])
 def test_config2_sample_vs_reference_kernels(fg, dev, refdrv, tuning):
-    errs = _vs_reference(fg, refdrv, fg.workloads.config2(shots=64, nt=300), dev, tuning=tuning)
+    errs = _vs_reference(fg, refdrv, fg.workloads.config2(shots=64, nt=1000), dev, tuning=tuning)
     assert max(errs) <= TOL_REF
 
 

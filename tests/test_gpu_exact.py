@@ -40,6 +40,7 @@ def test_exact_vs_fp64_oracle(fg, orc, dev, case, tuning):
         wl = fg.workloads.small(seed=11, shots=40, nt=90, nx=33, ny=65, pml=8, nrx=5)
         wl.source_step = [0.01, 0.02, 0.0]
         wl.receiver_step = [0.05, 0.0, 0.0]
+        wl.fixed_receiver = True
     else:
         wl = [fg.workloads.small(), fg.workloads.small(seed=3, shots=2, nt=150, nx=40, ny=56, pml=5, nrx=6), None,
               fg.workloads.config0()][case]
@@ -53,6 +54,7 @@ def test_exact_vs_fp64_oracle(fg, orc, dev, case, tuning):
     oe, os_ = orc.exact_gradient(s1, s2, np.maximum(wl.er, 1), np.maximum(wl.se, 0), setup.dt32)
     e_ge, e_gs = helpers.rel_l2(ge, oe), helpers.rel_l2(gs, os_)
     print("%s exact adjoint vs FP64 oracle: g_eps %.3g, g_sig %.3g" % (wl.name, e_ge, e_gs))
+    assert np.isfinite(ge).all() and np.isfinite(gs).all()
     assert e_ge <= TOL and e_gs <= TOL
 
 
@@ -79,6 +81,7 @@ def test_exact_vs_centred_fd_config1(fg, orc, dev):
         fd = (J(er + h * de, se + h * ds) - J(er - h * de, se - h * ds)) / (2 * h)
         ad = float(np.sum(ge * de) + np.sum(gs * ds))
         err = abs(fd - ad) / abs(fd)
+        assert np.isfinite(ad)
         print("config1 %s: centred FD %.9g, exact adjoint %.9g, rel err %.3g" % (name, fd, ad, err))
         assert err <= TOL
     # the reference-mode gradient of the same weights, for the cosine similarity of the two modes
