@@ -71,32 +71,6 @@ void build_tiles(fg_plan* p) {
     // tiles: chunks of exactly TI rows (the last one shorter); march: balanced chunks
     for (int c = 0; c <= p->nc; ++c)
         p->chunk_row[c] = p->kernel == 0 ? std::min(c * p->TI, p->nx) : (int)((long long)c * p->nx / p->nc);
-    // fetch order: tiles touching a CPML slab (more work per cell) first,
-    // each class in (group, chunk, band) order
-    {
-        const int th = p->th;
-        auto heavy = [&](int t) {
-            if (th == 0) return false;
-            const int band = t % p->nb, chunk = (t / p->nb) % p->nc;
-            const int i0 = p->chunk_row[chunk], i1 = p->chunk_row[chunk + 1];
-            const int b0 = band * p->BW, b1 = b0 + p->BW;
-            const bool xs = i0 <= th || i1 - 1 >= p->nx - th - 1;
-            const bool ys = b0 <= th + 1 || b1 - 1 >= p->ny - th - 1;
-            return xs || ys;
-        };
-        p->order.clear();
-        for (int t = 0; t < p->ntiles; ++t)
-            if (heavy(t)) p->order.push_back(t);
-        for (int t = 0; t < p->ntiles; ++t)
-            if (!heavy(t)) p->order.push_back(t);
-        p->tiles.resize(p->ntiles);
-        for (int q = 0; q < p->ntiles; ++q) {
-            const int t = p->order[q];
-            const int band = t % p->nb, chunk = (t / p->nb) % p->nc, grp = t / (p->nb * p->nc);
-            p->tiles[q] = make_int4(band * p->BW, p->chunk_row[chunk], grp, t);
-        }
-    }
-
     // events binned straight into their tiles (O(events), not O(tiles x events))
     const int bw = p->BW;
     std::vector<int> chunk_of_row(p->nx + 1, p->nc - 1);
@@ -159,6 +133,47 @@ void build_tiles(fg_plan* p) {
     finish(src, p->src_ev, p->src_off);
     finish(rxs, p->rx_ev, p->rx_off);
     finish(inj, p->inj_ev, p->inj_off);
+    // fetch order: tiles touching a CPML slab (more work per cell) first,
+    // each class in (group, chunk, band) order; with the interior split, the
+    // interior tiles (no cell of the tile or of its halo in a CPML slab or on
+    // the first / last rows and columns, no event) come last, from core0 on
+    {
+        const int th = p->th;
+        auto heavy = [&](int t) {
+            if (th == 0) return false;
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc;
+            const int i0 = p->chunk_row[chunk], i1 = p->chunk_row[chunk + 1];
+            const int b0 = band * p->BW, b1 = b0 + p->BW;
+            const bool xs = i0 <= th || i1 - 1 >= p->nx - th - 1;
+            const bool ys = b0 <= th + 1 || b1 - 1 >= p->ny - th - 1;
+            return xs || ys;
+        };
+        auto interior = [&](int t) {
+            if (!p->split) return false;
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc;
+            const int i0 = p->chunk_row[chunk], i1 = p->chunk_row[chunk + 1];
+            const int j0 = band * p->BW;
+            const bool rows = i0 >= th + 1 && i1 <= p->nx - th - 1;
+            const bool cols = j0 >= th + 1 && j0 + p->BW <= p->ny - th - 1;
+            const bool quiet = p->src_off[t + 1] == p->src_off[t] && p->rx_off[t + 1] == p->rx_off[t] &&
+                               p->inj_off[t + 1] == p->inj_off[t];
+            return rows && cols && quiet;
+        };
+        p->order.clear();
+        for (int t = 0; t < p->ntiles; ++t)
+            if (heavy(t) && !interior(t)) p->order.push_back(t);
+        for (int t = 0; t < p->ntiles; ++t)
+            if (!heavy(t) && !interior(t)) p->order.push_back(t);
+        p->core0 = (int)p->order.size();
+        for (int t = 0; t < p->ntiles; ++t)
+            if (interior(t)) p->order.push_back(t);
+        p->tiles.resize(p->ntiles);
+        for (int q = 0; q < p->ntiles; ++q) {
+            const int t = p->order[q];
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc, grp = t / (p->nb * p->nc);
+            p->tiles[q] = make_int4(band * p->BW, p->chunk_row[chunk], grp, t);
+        }
+    }
 }
 
 void layout(fg_plan* p) {
@@ -181,7 +196,7 @@ void layout(fg_plan* p) {
     p->o_chunk = take((p->nc + 1) * sizeof(int));
     p->o_order = take((size_t)p->ntiles * sizeof(int));
     p->o_tiles = take((size_t)p->ntiles * sizeof(int4));
-    p->o_ctr = take(2 * sizeof(int));
+    p->o_ctr = take(4 * sizeof(int));
     p->o_srcev = take(p->src_ev.size() * sizeof(Ev));
     p->o_rxev = take(p->rx_ev.size() * sizeof(Ev));
     p->o_injev = take(p->inj_ev.size() * sizeof(Ev));
@@ -227,6 +242,7 @@ void fill_grid(fg_plan* p) {
     g.tile_ctr = (int*)(w + p->o_ctr);
     g.fast_cpml = 2 * p->th < p->nx && 2 * p->th < p->ny;
     g.pf = p->pf;
+    g.core0 = p->core0;
     g.src_ev = (const Ev*)(w + p->o_srcev);
     g.rx_ev = (const Ev*)(w + p->o_rxev);
     g.inj_ev = (const Ev*)(w + p->o_injev);
@@ -253,7 +269,7 @@ int coefficients(const float* er, const float* se, const float* mr, int nx, int 
 int reset_state(fg_plan* p, cudaStream_t st) {
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_state, 0, p->state_bytes, st));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_psi, 0, p->psi_bytes, st));
-    FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 2 * sizeof(int), st));
+    FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 4 * sizeof(int), st));
     return FG_OK;
 }
 
@@ -616,6 +632,22 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // the band pipeline prefetches the CPML auxiliaries of the rows it streams
     p->pf = ((p->kernel == 1 && p->shot && !p->pair && p->D == 0) || p->kernel == 2) ? (pf == 0 ? 1 : std::max(pf, 0))
                                                                                       : 0;
+    // interior tiles in their own lean kernel (shot-lane lane march with direct loads)
+    const int interior = tune ? tune->interior : 0;
+    if (interior < -1 || interior > 8) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: interior must be -1 .. 8");
+    }
+    // by default only where a step is long enough to pay for its second launch
+    // (at least 2e5 cells x shot groups: the 440 x 340 x 2-group benchmark grid,
+    // not the small grids of the serving stream, whose steps take microseconds)
+    const long long work = (long long)p->nx * p->ny * ((p->S + 31) / 32);
+    p->split = p->kernel == 1 && p->shot && !p->pair && p->D == 0 && pick_fwd_core(p->W) &&
+               (interior > 0 || (interior == 0 && work >= 200000));
+    // measured on the 64-shot 440 x 340 benchmark grid: the forward's general
+    // kernel is fastest beside the interior kernel with 3 blocks per SM (the
+    // adjoint's, on its own plan, with 4; fg_plan_create passes that)
+    p->split_bpsm = interior > 0 ? interior : 3;
     if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: the ring needs more than 227 KB of shared memory");
@@ -670,12 +702,15 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     }
     if (tune && tune->adj_cells_per_thread) at.cells_per_thread = tune->adj_cells_per_thread;
     at.prefetch = tune ? tune->prefetch : 0;
+    at.interior = tune ? tune->interior : 0;
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {
         delete p;
         return rc;
     }
+    // the adjoint's general kernel beside its interior kernel: 4 blocks per SM by default
+    if (!(tune && tune->interior)) a->split_bpsm = 4;
     p->adj = a;
     *out = p;
     return FG_OK;
@@ -824,6 +859,19 @@ int fg_coefficients(const float* er, const float* se, const float* mr, int32_t n
 
 namespace {
 
+// Blocks of the general kernel's persistent launch when the interior tiles
+// run beside it: split_bpsm per SM (fewer than it could hold, so that the
+// interior kernel's blocks fit beside it), at most one warp per tile.
+cudaError_t split_blocks(const fg_plan* p, int* blocks) {
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int need = (p->core0 + p->WPB - 1) / p->WPB;
+    *blocks = std::max(1, std::min(need, p->split_bpsm * sms));
+    return cudaSuccess;
+}
+
 // Forward steps [t0, t1) of plan p with descriptor g.
 int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
     if (p->kernel == 0) {
@@ -834,6 +882,18 @@ int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
         FwdFn fn = pick_fwd_band(p->W, p->WPB);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int t = t0; t < t1; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
+    } else if (p->split) {
+        // the general lane march on the tiles before core0, the interior kernel on the rest
+        FwdFn fn = pick_fwd(p->shot, p->W), fc = pick_fwd_core(p->W);
+        if (!fn || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        Dev gb = g;
+        gb.ntiles = p->core0;
+        if (p->core0 > 0 && p->fwd_blocks == 0) FG_CUDA(split_blocks(p, &p->fwd_blocks));
+        const int pdl = p->core0 > 0;
+        for (int t = t0; t < t1; ++t) {
+            if (p->core0 > 0) FG_CUDA(fn(gb, t, p->WPB, p->D, &p->fwd_blocks, st));
+            if (p->core0 < p->ntiles) FG_CUDA(fc(g, t, 4, pdl, &p->fwd_core_blocks, st));
+        }
     } else {
         FwdFn fn = p->pair ? pick_fwd2(p->W) : pick_fwd(p->shot, p->W);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
@@ -857,6 +917,18 @@ int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t
         AdjFn fn = pick_adj_band(a->W, a->WPB);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int it = hi; it >= lo; --it) FG_CUDA(fn(g, it, (a->nt - 1 - it) & 1, a->WPB, a->D, &a->adj_blocks, st));
+    } else if (a->split) {
+        AdjFn fn = pick_adj(a->shot, a->W), fc = pick_adj_core(a->W);
+        if (!fn || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        Dev gb = g;
+        gb.ntiles = a->core0;
+        if (a->core0 > 0 && a->adj_blocks == 0) FG_CUDA(split_blocks(a, &a->adj_blocks));
+        const int pdl = a->core0 > 0;
+        for (int it = hi; it >= lo; --it) {
+            const int rp = (a->nt - 1 - it) & 1;
+            if (a->core0 > 0) FG_CUDA(fn(gb, it, rp, a->WPB, a->D, &a->adj_blocks, st));
+            if (a->core0 < a->ntiles) FG_CUDA(fc(g, it, rp, 4, pdl, &a->adj_core_blocks, st));
+        }
     } else {
         AdjFn fn = a->pair ? pick_adj2(a->W) : pick_adj(a->shot, a->W);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
@@ -1099,7 +1171,7 @@ int fg_adjoint_reference_checkpointed(fg_plan* p, const float* er, const float* 
             if ((rc = reset_state(p, st))) return rc;
         } else {
             if ((rc = checkpoint_copy(p, s0 & 1, (float*)ckpt + (size_t)(c - 1) * cf, false, st))) return rc;
-            FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 2 * sizeof(int), st));
+            FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 4 * sizeof(int), st));
         }
         gf.hist_t0 = s0;
         if ((rc = fwd_steps(p, gf, s0, s1, st))) return rc;

@@ -66,6 +66,7 @@ struct Dev {
     const int4* tiles;                      // (ntiles) (b0, i0, group, id) in fetch order
     int* tile_ctr;                          // 2 counters, one per launch parity
     int fast_cpml;                          // 2 th < nx and 2 th < ny: no cell in two slabs of one axis
+    int core0;                              // first fetch position of the interior tiles (lean kernels)
     int pf;                                 // lane march, shot lanes: prefetch a warp's next tile into L2
                                             // (0 no, 1 when the current tile starts, 2 at its middle row)
     const int* chunk_row;                   // (nc+1) row boundaries

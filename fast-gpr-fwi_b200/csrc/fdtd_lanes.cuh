@@ -261,6 +261,16 @@ __device__ __forceinline__ LaneTile<SHOT> decode_tile(const Dev& g, int id, int 
     return T;
 }
 
+// Programmatic dependent launch: a kernel launched behind this one with the
+// programmatic-serialization attribute may start once every block of this
+// one has executed launch_dependents; it calls griddep_wait before it
+// completes, so it never completes before this one.  Both are no-ops for
+// launches without a dependent / a prerequisite.
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Next tile position of this warp (lane 0 takes it, all lanes see it).
 __device__ __forceinline__ int fetch_tile(int* ctr, int lane) {
     int p = 0;
@@ -473,6 +483,9 @@ __device__ __forceinline__ void issue_fwd(const Dev& g, uint64_t* bar, float* st
 
 template <int W, bool SHOT, bool RING>
 __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
+    // an interior-tile kernel launched behind this one may start at once
+    // (it reads none of this launch's results; see fdtd_core.cuh)
+    griddep_launch_dependents();
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -941,6 +954,7 @@ __device__ __forceinline__ void issue_adj(const Dev& g, uint64_t* bar, float* st
 
 template <int W, bool SHOT, bool RING>
 __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
+    griddep_launch_dependents();
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
     extern __shared__ __align__(128) unsigned char smem[];

@@ -7,6 +7,7 @@
 //   steps_pairs.cu      shot-pair lane march (fdtd_pairs.cuh)
 //   steps_band.cu       band pipelines       (fdtd_band.cuh)
 //   steps_exact.cu      exact adjoint        (fdtd_exact.cuh)
+//   steps_core.cu       interior tiles       (fdtd_core.cuh)
 // Not part of the C ABI (include/fastgpr.h).
 #pragma once
 
@@ -38,6 +39,9 @@ struct fg_plan {
     bool pair = false;  // two shots per lane (CS = 64, lane march only)
     int W, TI, WPB, D;  // cells per thread, rows per tile, warps per block, ring stages (0 = direct loads)
     int pf = 0;         // next-tile L2 prefetch of the lane march (Dev::pf)
+    bool split = false; // interior tiles (positions >= core0) run in the lean interior kernels
+    int core0 = 0;      // first fetch position of an interior tile (== ntiles when none)
+    int split_bpsm = 2; // blocks per SM of the general kernel's launch beside the interior kernel
     // tensor maps of the tile kernels (encoded when a workspace is bound)
     CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
     int CS, SL;         // floats per cell in a group plane, shots per group
@@ -50,7 +54,7 @@ struct fg_plan {
     size_t o_coef, o_state, o_psi, o_chunk, o_order, o_tiles, o_ctr, o_srcev, o_rxev, o_injev, o_offs, o_srcw, o_pml, o_gacc,
         o_sums, o_partial, o_norms, o_err, o_rxpos, total;
     // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
-    int fwd_blocks = 0, adj_blocks = 0;
+    int fwd_blocks = 0, adj_blocks = 0, fwd_core_blocks = 0, adj_core_blocks = 0;
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
     float dinv = 0.f;
     int div_scaled = 0;   // the scaled step matches __fdiv_rn for every |x| < 2^31 (checked at bind)
@@ -124,6 +128,8 @@ FwdFn pick_fwd2(int W);                  // shot pairs, forward
 AdjFn pick_adj2(int W);                  // shot pairs, adjoint
 FwdTileFn pick_fwd_tile(bool shot, int W);
 AdjTileFn pick_adj_tile(bool shot, int W);
+FwdFn pick_fwd_core(int W);              // interior tiles of the lane march, forward
+AdjFn pick_adj_core(int W);              // interior tiles of the lane march, adjoint
 FwdFn pick_fwd_band(int W, int C);       // band pipeline (C consumer warps), forward
 AdjFn pick_adj_band(int W, int C);       // band pipeline, adjoint
 // Shared memory of a band-pipeline CTA (0: no kernel of that shape).

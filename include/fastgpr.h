@@ -109,6 +109,14 @@ typedef struct fg_tuning {
      * 0 = default (1), -1 = off, 1 = when the warp starts its current tile,
      * 2 = at the current tile's middle row. */
     int32_t prefetch;
+    /* Lane march with shot lanes and no stages: the interior tiles (no CPML
+     * cell in the tile or its halo, no source, receiver or injection) run in
+     * a lean kernel of their own, side by side with the general kernel on the
+     * other tiles.  -1 = off; 0 = default (on when nx * ny * shot groups is
+     * at least 2e5 -- smaller steps do not pay for the second launch -- with
+     * the general kernel at 3 blocks per SM for the forward and 4 for the
+     * adjoint); 1..8 = on, the general kernel with that many blocks per SM. */
+    int32_t interior;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
