@@ -31,7 +31,10 @@ EXPORTS = (
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
     "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
     "fg_fir_causal", "fg_adjoint_reference_l1", "fg_adjoint_exact",
+    "fg_forward_batch", "fg_adjoint_reference_batch",
 )
+
+BATCH_MAX = 8   # FG_BATCH_MAX
 
 
 class FgProblem(ctypes.Structure):
@@ -52,11 +55,12 @@ class FgTuning(ctypes.Structure):
         ("adj_kernel", ctypes.c_int32), ("adj_rows_per_tile", ctypes.c_int32),
         ("adj_warps_per_block", ctypes.c_int32), ("adj_stages", ctypes.c_int32),
         ("adj_cells_per_thread", ctypes.c_int32), ("prefetch", ctypes.c_int32), ("interior", ctypes.c_int32),
+        ("persistent", ctypes.c_int32),
     ]
 
     KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel",
             "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages", "adj_cells_per_thread",
-            "prefetch", "interior")
+            "prefetch", "interior", "persistent")
 
 
 class FastGprError(RuntimeError):
@@ -119,6 +123,10 @@ def lib() -> ctypes.CDLL:
     L.fg_adjoint_reference_l1.restype = ctypes.c_int
     L.fg_adjoint_exact.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.fg_adjoint_exact.restype = ctypes.c_int
+    L.fg_forward_batch.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
+    L.fg_forward_batch.restype = ctypes.c_int
+    L.fg_adjoint_reference_batch.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp]
+    L.fg_adjoint_reference_batch.restype = ctypes.c_int
     L.fg_fir_causal.argtypes = [vp, i64, i32, i32, vp, i32, vp, vp]
     L.fg_fir_causal.restype = ctypes.c_int
     L.fg_tv_workspace_bytes.argtypes = [i32, i32]
@@ -279,6 +287,37 @@ class Plan:
             stream_handle(self.device)))
         if checked_build():
             self.device_check()
+
+
+def _ptrs(ts) -> ctypes.Array:
+    return (ctypes.c_void_p * len(ts))(*[ptr(t) for t in ts])
+
+
+def forward_batch(plans, er32, se32, mr32, traces, hists):
+    """fg_forward_batch: the forward solves of several plans in one launch.
+
+    Every argument is a sequence with one entry per plan (hists entries may be
+    None); all plans on one device.
+    """
+    n = len(plans)
+    hs = (ctypes.c_void_p * n)(*[p.handle for p in plans])
+    check(lib().fg_forward_batch(hs, n, _ptrs(er32), _ptrs(se32), _ptrs(mr32), _ptrs(traces), _ptrs(hists),
+                                 stream_handle(plans[0].device)))
+    if checked_build():
+        for p in plans:
+            p.device_check()
+
+
+def adjoint_reference_batch(plans, er32, se32, mr32, hists, resids, grad_eps, grad_sig, normalize=True):
+    """fg_adjoint_reference_batch: the adjoint solves of several plans in one launch."""
+    n = len(plans)
+    hs = (ctypes.c_void_p * n)(*[p.handle for p in plans])
+    check(lib().fg_adjoint_reference_batch(hs, n, _ptrs(er32), _ptrs(se32), _ptrs(mr32), _ptrs(hists),
+                                           _ptrs(resids), _ptrs(grad_eps), _ptrs(grad_sig),
+                                           1 if normalize else 0, stream_handle(plans[0].device)))
+    if checked_build():
+        for p in plans:
+            p.device_check()
 
 
 def coefficients(er32, se32, mr32, dt32, dx32, adjoint, pitch=None):

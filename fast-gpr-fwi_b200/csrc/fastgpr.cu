@@ -210,6 +210,7 @@ void layout(fg_plan* p) {
     p->o_norms = take(2 * sizeof(double));
     p->o_err = take(sizeof(int) * 4);
     p->o_rxpos = take((size_t)p->S * p->nrx * sizeof(int2));
+    p->o_bar = take(4 * sizeof(unsigned));
     p->total = o;
 }
 
@@ -564,7 +565,16 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // lane march (4 cells x 4 rows) for shot lanes, tile pipeline (2 cells x 4
     // rows) for column lanes
     const bool tuned_kernel = tune && (tune->kernel || tune->stages || tune->rows_per_tile || tune->cells_per_thread);
-    p->kernel = tuned_kernel ? tune->kernel : (p->shot ? 1 : 0);
+    // the whole time loop in one persistent launch (fdtd_multi.cuh) only when
+    // asked for: measured on the 140 x 100 one-shot and 240 x 160 13-shot
+    // grids it is no faster than a launch per step (a step's time is the
+    // serial latency of a warp's tile, which the launch does not change)
+    const int persistent = tune ? tune->persistent : 0;
+    if (persistent < -1 || persistent > 1) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: persistent must be -1, 0 or 1");
+    }
+    p->kernel = tuned_kernel ? tune->kernel : ((p->shot || persistent == 1) ? 1 : 0);
     if (p->kernel < 0 || p->kernel > 2) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: kernel must be 0 (tiles), 1 (lane march) or 2 (band pipeline)");
@@ -648,6 +658,7 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // kernel is fastest beside the interior kernel with 3 blocks per SM (the
     // adjoint's, on its own plan, with 4; fg_plan_create passes that)
     p->split_bpsm = interior > 0 ? interior : 3;
+    p->persist = p->kernel == 1 && p->D == 0 && !p->pair && !p->split && persistent == 1;
     if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: the ring needs more than 227 KB of shared memory");
@@ -703,6 +714,7 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     if (tune && tune->adj_cells_per_thread) at.cells_per_thread = tune->adj_cells_per_thread;
     at.prefetch = tune ? tune->prefetch : 0;
     at.interior = tune ? tune->interior : 0;
+    at.persistent = tune ? tune->persistent : 0;
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {
@@ -872,6 +884,38 @@ cudaError_t split_blocks(const fg_plan* p, int* blocks) {
     return cudaSuccess;
 }
 
+// One persistent launch over the models plans[0..n) with descriptors devs:
+// forward steps [t0, t1) / adjoint rounds [k0, k1) (round k runs iteration
+// nt - 1 - k of each model).  The barrier words are the first plan's.
+cudaError_t multi_devs(fg_plan* const* plans, const Dev* devs, int n, fg::MultiDevs* M, int* want, cudaStream_t st) {
+    M->n = n;
+    int most = 1;
+    for (int m = 0; m < n; ++m) {
+        M->d[m] = devs[m];
+        most = std::max(most, plans[m]->ntiles);
+    }
+    M->bar = (unsigned*)(plans[0]->ws + plans[0]->o_bar);
+    M->err = devs[0].err;
+    *want = (most + 3) / 4;
+    return cudaMemsetAsync(M->bar, 0, sizeof(unsigned), st);
+}
+cudaError_t multi_fwd(fg_plan* const* plans, const Dev* devs, int n, int t0, int t1, cudaStream_t st) {
+    fg::MultiDevs M;
+    int want = 1;
+    cudaError_t e = multi_devs(plans, devs, n, &M, &want, st);
+    if (e != cudaSuccess) return e;
+    if (n == 1) return launch_fwd_persist(devs[0], plans[0]->shot, plans[0]->W, M.bar, want, t0, t1, st);
+    return launch_fwd_multi(M, plans[0]->shot, plans[0]->W, want, t0, t1, st);
+}
+cudaError_t multi_adj(fg_plan* const* plans, const Dev* devs, int n, int k0, int k1, cudaStream_t st) {
+    fg::MultiDevs M;
+    int want = 1;
+    cudaError_t e = multi_devs(plans, devs, n, &M, &want, st);
+    if (e != cudaSuccess) return e;
+    if (n == 1) return launch_adj_persist(devs[0], plans[0]->shot, plans[0]->W, M.bar, want, k0, k1, st);
+    return launch_adj_multi(M, plans[0]->shot, plans[0]->W, want, k0, k1, st);
+}
+
 // Forward steps [t0, t1) of plan p with descriptor g.
 int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
     if (p->kernel == 0) {
@@ -882,6 +926,8 @@ int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
         FwdFn fn = pick_fwd_band(p->W, p->WPB);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int t = t0; t < t1; ++t) FG_CUDA(fn(g, t, p->WPB, p->D, &p->fwd_blocks, st));
+    } else if (p->persist) {
+        FG_CUDA(multi_fwd(&p, &g, 1, t0, t1, st));
     } else if (p->split) {
         // the general lane march on the tiles before core0, the interior kernel on the rest
         FwdFn fn = pick_fwd(p->shot, p->W), fc = pick_fwd_core(p->W);
@@ -917,6 +963,8 @@ int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t
         AdjFn fn = pick_adj_band(a->W, a->WPB);
         if (!fn) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         for (int it = hi; it >= lo; --it) FG_CUDA(fn(g, it, (a->nt - 1 - it) & 1, a->WPB, a->D, &a->adj_blocks, st));
+    } else if (a->persist) {
+        FG_CUDA(multi_adj(&a, &g, 1, a->nt - 1 - hi, a->nt - lo, st));
     } else if (a->split) {
         AdjFn fn = pick_adj(a->shot, a->W), fc = pick_adj_core(a->W);
         if (!fn || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
@@ -938,7 +986,7 @@ int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t
     return FG_OK;
 }
 
-// Start of an adjoint solve on plan a: Ucgeta coefficients, zero state and accumulators.
+// Start of an adjoint solve on plan a: adjoint coefficients, zero state and accumulators.
 int adj_begin(fg_plan* a, const float* er, const float* se, const float* mr, cudaStream_t st) {
     int rc = coefficients(er, se, mr, a->nx, a->ny, a->dt, a->dx, 1, (float*)(a->ws + a->o_coef), a->P, fg::PADC, st);
     if (rc) return rc;
@@ -1103,6 +1151,88 @@ int fg_adjoint_exact(fg_plan* p, const float* er, const float* se, const float* 
     FG_CUDA(cudaGetLastError());
     const double e0 = (double)8.8541878128e-12f;   // the float constant of uc.cu:8
     FG_CUDA(launch_grad_exact(sums, er, se, a->nx, a->ny, e0 / (double)a->dt, grad_eps, grad_sig, st));
+    return FG_OK;
+}
+
+namespace {
+// The checks a batch of plans must pass: bound, persistent lane march, one
+// kernel shape for all (the launch is one kernel), at most FG_BATCH_MAX.
+int batch_args(fg_plan* const* plans, int32_t n, bool adjoint, const char* who) {
+    if (!plans || n < 1 || n > FG_BATCH_MAX)
+        return fail(FG_ERR_INVALID, std::string(who) + ": 1 to " + std::to_string(FG_BATCH_MAX) + " plans");
+    for (int m = 0; m < n; ++m) {
+        const fg_plan* p = plans[m];
+        if (!p) return fail(FG_ERR_INVALID, std::string(who) + ": NULL plan");
+        const fg_plan* q = adjoint ? (p->adj ? p->adj : p) : p;
+        const fg_plan* q0 = adjoint ? (plans[0]->adj ? plans[0]->adj : plans[0]) : plans[0];
+        if (!q->ws) return fail(FG_ERR_WORKSPACE, std::string(who) + ": plan has no workspace");
+        if (!q->persist)
+            return fail(FG_ERR_INVALID, std::string(who) + ": plan " + std::to_string(m) +
+                                            " is not a persistent lane-march plan (tuning persistent)");
+        if (q->shot != q0->shot || q->W != q0->W)
+            return fail(FG_ERR_INVALID, std::string(who) + ": the plans differ in lanes or cells_per_thread");
+    }
+    return FG_OK;
+}
+}  // namespace
+
+int fg_forward_batch(fg_plan* const* plans, int32_t n, const float* const* er, const float* const* se,
+                     const float* const* mr, float* const* traces, float* const* hist, void* stream) {
+    int rc = batch_args(plans, n, false, "fg_forward_batch");
+    if (rc) return rc;
+    if (!er || !se || !mr || !traces || !hist) return fail(FG_ERR_INVALID, "fg_forward_batch: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    Dev devs[FG_BATCH_MAX];
+    int nt = 0;
+    for (int m = 0; m < n; ++m) {
+        fg_plan* p = plans[m];
+        if (!er[m] || !se[m] || !mr[m] || (!traces[m] && p->nrx > 0))
+            return fail(FG_ERR_INVALID, "fg_forward_batch: NULL argument");
+        if ((rc = coefficients(er[m], se[m], mr[m], p->nx, p->ny, p->dt, p->dx, 0, (float*)(p->ws + p->o_coef), p->P,
+                               fg::PADC, st)))
+            return rc;
+        if ((rc = reset_state(p, st))) return rc;
+        if (p->nrx > 0) FG_CUDA(cudaMemsetAsync(traces[m], 0, (size_t)p->S * p->nt * p->nrx * sizeof(float), st));
+        devs[m] = p->g;
+        devs[m].traces = traces[m];
+        devs[m].hist = hist[m];
+        if (hist[m]) {
+            devs[m].out_lo = (const char*)hist[m];
+            devs[m].out_hi = (const char*)(hist[m] + (size_t)p->nt * hist_step_floats(p));
+        }
+        nt = std::max(nt, p->nt);
+    }
+    FG_CUDA(multi_fwd(plans, devs, n, 0, nt, st));
+    return FG_OK;
+}
+
+int fg_adjoint_reference_batch(fg_plan* const* plans, int32_t n, const float* const* er, const float* const* se,
+                               const float* const* mr, const float* const* hist, const float* const* resid,
+                               float* const* grad_eps, float* const* grad_sig, int32_t normalize, void* stream) {
+    int rc = batch_args(plans, n, true, "fg_adjoint_reference_batch");
+    if (rc) return rc;
+    if (!er || !se || !mr || !hist || !resid || !grad_eps || !grad_sig)
+        return fail(FG_ERR_INVALID, "fg_adjoint_reference_batch: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    fg_plan* as[FG_BATCH_MAX];
+    Dev devs[FG_BATCH_MAX];
+    int rounds = 0;
+    for (int m = 0; m < n; ++m) {
+        fg_plan* a = plans[m]->adj ? plans[m]->adj : plans[m];
+        if (!er[m] || !se[m] || !mr[m] || !hist[m] || (!resid[m] && a->nrx > 0))
+            return fail(FG_ERR_INVALID, "fg_adjoint_reference_batch: NULL argument");
+        if ((rc = adj_begin(a, er[m], se[m], mr[m], st))) return rc;
+        as[m] = a;
+        devs[m] = a->g;
+        devs[m].hist = const_cast<float*>(hist[m]);
+        devs[m].out_lo = (const char*)hist[m];
+        devs[m].out_hi = (const char*)(hist[m] + (size_t)a->nt * hist_step_floats(a));
+        devs[m].resid = resid[m];
+        rounds = std::max(rounds, a->nt - 1);
+    }
+    if (rounds > 0) FG_CUDA(multi_adj(as, devs, n, 0, rounds, st));
+    for (int m = 0; m < n; ++m)
+        if ((rc = adj_finish(as[m], devs[m], grad_eps[m], grad_sig[m], normalize, nullptr, st))) return rc;
     return FG_OK;
 }
 

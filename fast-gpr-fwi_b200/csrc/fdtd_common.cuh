@@ -104,11 +104,20 @@ __device__ __forceinline__ bool in_bounds(const Dev& g, const void* p, int bytes
 #define FG_OK_PTR(g, p, bytes) true
 #endif
 
-// Load of a value that no thread writes during the launch (old state of the
-// read parity, coefficients, CPML vectors, history): read-only cache path.
+// Loads of values that no thread writes during the step (old state of the
+// read parity, coefficients, CPML vectors, history) take the read-only cache
+// path.  A launch that runs several steps reads state that other blocks wrote
+// earlier in the same launch, which that path is not guaranteed to see: the
+// translation unit of such kernels defines FG_MULTI_STEP, and the loads then
+// go to L2 (ld.global.cg), which every block's stores reach.
+#ifdef FG_MULTI_STEP
+#define FG_LDRO(p) __ldcg(p)
+#else
+#define FG_LDRO(p) __ldg(p)
+#endif
 __device__ __forceinline__ float ldro(const Dev& g, const float* p) {
     if (!FG_OK_PTR(g, p, 4)) return 0.f;
-    return __ldg(p);
+    return FG_LDRO(p);
 }
 __device__ __forceinline__ void st1(const Dev& g, float* p, float x) {
     if (!FG_OK_PTR(g, p, 4)) return;
@@ -125,7 +134,7 @@ __device__ __forceinline__ void ld_cells(const Dev& g, float* x, const float* p)
                 x[k] = x[k + 1] = x[k + 2] = x[k + 3] = 0.f;
                 continue;
             }
-            const float4 q = __ldg(reinterpret_cast<const float4*>(p + k));
+            const float4 q = FG_LDRO(reinterpret_cast<const float4*>(p + k));
             x[k] = q.x; x[k + 1] = q.y; x[k + 2] = q.z; x[k + 3] = q.w;
         }
     } else if constexpr (CS == 1 && N == 2) {
@@ -133,7 +142,7 @@ __device__ __forceinline__ void ld_cells(const Dev& g, float* x, const float* p)
             x[0] = x[1] = 0.f;
             return;
         }
-        const float2 q = __ldg(reinterpret_cast<const float2*>(p));
+        const float2 q = FG_LDRO(reinterpret_cast<const float2*>(p));
         x[0] = q.x; x[1] = q.y;
     } else {
 #pragma unroll

@@ -481,17 +481,14 @@ __device__ __forceinline__ void issue_fwd(const Dev& g, uint64_t* bar, float* st
     });
 }
 
+// Forward step t of one solve by the warps of this block: tiles from the
+// step's counter until none is left.  R: the CPML profile (shared or global
+// memory); smem: the block's dynamic shared memory (RING stages after the
+// profile).
 template <int W, bool SHOT, bool RING>
-__global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
-    // an interior-tile kernel launched behind this one may start at once
-    // (it reads none of this launch's results; see fdtd_core.cuh)
-    griddep_launch_dependents();
+__device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned char* smem, const int t, const int D) {
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const float* R = stage_profile(g, smem);
-    // a stage of an earlier launch never landed: leave at once
-    if (RING && *(volatile int*)g.err != 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[(t + 1) & 1] = 0;   // the next launch's counter
     int* ctr = g.tile_ctr + (t & 1);
     const int lane = threadIdx.x & 31;
@@ -669,6 +666,18 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
         }
     }
 #undef FG_CELL
+}
+
+template <int W, bool SHOT, bool RING>
+__global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
+    // an interior-tile kernel launched behind this one may start at once
+    // (it reads none of this launch's results; see fdtd_core.cuh)
+    griddep_launch_dependents();
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* R = stage_profile(g, smem);
+    // a stage of an earlier launch never landed: leave at once
+    if (RING && *(volatile int*)g.err != 0) return;
+    fwd_step<W, SHOT, RING>(g, R, smem, t, D);
 }
 
 // ---------------------------------------------------------------------------
@@ -952,14 +961,13 @@ __device__ __forceinline__ void issue_adj(const Dev& g, uint64_t* bar, float* st
     });
 }
 
+// Reference-mode adjoint iteration it (reading parity rp) of one solve by the
+// warps of this block; R and smem as for fwd_step.
 template <int W, bool SHOT, bool RING>
-__global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
-    griddep_launch_dependents();
+__device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned char* smem, const int it, const int rp,
+                                         const int D) {
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const float* R = stage_profile(g, smem);
-    if (RING && *(volatile int*)g.err != 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[rp ^ 1] = 0;   // the next launch's counter
     int* ctr = g.tile_ctr + rp;
     const int lane = threadIdx.x & 31;
@@ -1126,6 +1134,15 @@ __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const
             pr.q[1] = tile_q<W, SHOT>(g, nxt, it);
         }
     }
+}
+
+template <int W, bool SHOT, bool RING>
+__global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
+    griddep_launch_dependents();
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float* R = stage_profile(g, smem);
+    if (RING && *(volatile int*)g.err != 0) return;
+    adj_step<W, SHOT, RING>(g, R, smem, it, rp, D);
 }
 
 // The last term of the summation by parts: g_eps -= sum_s Ez_f[0] lambda_1,

@@ -8,6 +8,7 @@
 //   steps_band.cu       band pipelines       (fdtd_band.cuh)
 //   steps_exact.cu      exact adjoint        (fdtd_exact.cuh)
 //   steps_core.cu       interior tiles       (fdtd_core.cuh)
+//   steps_multi.cu      persistent multi-step solves of one or more models (fdtd_multi.cuh)
 // Not part of the C ABI (include/fastgpr.h).
 #pragma once
 
@@ -23,6 +24,7 @@
 #include "fdtd_common.cuh"
 #include "fdtd_lanes.cuh"
 #include "fdtd_tile.cuh"
+#include "fdtd_multi.cuh"
 
 using fg::Dev;
 using fg::Ev;
@@ -42,6 +44,7 @@ struct fg_plan {
     bool split = false; // interior tiles (positions >= core0) run in the lean interior kernels
     int core0 = 0;      // first fetch position of an interior tile (== ntiles when none)
     int split_bpsm = 2; // blocks per SM of the general kernel's launch beside the interior kernel
+    bool persist = false;   // whole solves in one persistent cooperative launch (small grids)
     // tensor maps of the tile kernels (encoded when a workspace is bound)
     CUtensorMap tm_fez, tm_fhx, tm_fhy, tm_aez, tm_ahx, tm_ahy, tm_co;
     int CS, SL;         // floats per cell in a group plane, shots per group
@@ -52,7 +55,7 @@ struct fg_plan {
     std::vector<int> src_off, rx_off, inj_off;
     // workspace layout (byte offsets)
     size_t o_coef, o_state, o_psi, o_chunk, o_order, o_tiles, o_ctr, o_srcev, o_rxev, o_injev, o_offs, o_srcw, o_pml, o_gacc,
-        o_sums, o_partial, o_norms, o_err, o_rxpos, total;
+        o_sums, o_partial, o_norms, o_err, o_rxpos, o_bar, total;
     // blocks of a persistent launch (0 = not yet measured) for the forward and adjoint kernels
     int fwd_blocks = 0, adj_blocks = 0, fwd_core_blocks = 0, adj_core_blocks = 0;
     // RN(1/dx) when the reciprocal division step is enabled (checked at bind), else 0
@@ -134,6 +137,14 @@ FwdFn pick_fwd_band(int W, int C);       // band pipeline (C consumer warps), fo
 AdjFn pick_adj_band(int W, int C);       // band pipeline, adjoint
 // Shared memory of a band-pipeline CTA (0: no kernel of that shape).
 size_t band_smem(int W, int C, int th, int D, bool adjoint);
+// Persistent multi-step solves (steps_multi.cu): every step of the models in
+// M in one cooperative launch of at most `want` blocks.
+cudaError_t launch_fwd_persist(const fg::Dev& g, bool shot, int W, unsigned* bar, int want, int t0, int t1,
+                               cudaStream_t st);
+cudaError_t launch_adj_persist(const fg::Dev& g, bool shot, int W, unsigned* bar, int want, int k0, int k1,
+                               cudaStream_t st);
+cudaError_t launch_fwd_multi(const fg::MultiDevs& M, bool shot, int W, int want, int t0, int t1, cudaStream_t st);
+cudaError_t launch_adj_multi(const fg::MultiDevs& M, bool shot, int W, int want, int k0, int k1, cudaStream_t st);
 // Exact adjoint (steps_exact.cu): one transposed step of every cell and its
 // imaging sums; the receiver injection; the gradient from the sums.
 cudaError_t launch_adj_exact(const Dev& g, int it, int rp, int CS, int proj, cudaStream_t st);

@@ -117,6 +117,15 @@ typedef struct fg_tuning {
      * the general kernel at 3 blocks per SM for the forward and 4 for the
      * adjoint); 1..8 = on, the general kernel with that many blocks per SM. */
     int32_t interior;
+    /* Lane march without stages or shot pairs: the whole time loop of a
+     * solve in one persistent cooperative launch, the steps separated by a
+     * grid barrier, instead of one launch per step; needed by the batch calls
+     * below.  0 or -1 = off (default), 1 = on (the lane march also for column
+     * lanes when no kernel is given).  A step then costs the serial latency
+     * of one warp's tile plus about 2.4 us of barrier, so on small grids it
+     * is no faster than a launch per step; several models in one launch
+     * (fg_forward_batch) fill the GPU better than one. */
+    int32_t persistent;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;
@@ -195,6 +204,25 @@ int fg_adjoint_reference_l1(fg_plan* plan, const float* er, const float* se, con
  * the plan's adjoint state (like fg_adjoint_reference). */
 int fg_adjoint_exact(fg_plan* plan, const float* er, const float* se, const float* mr, const float* hist,
                      const float* weights, float* grad_eps, float* grad_sig, void* stream);
+
+/* Several models in one launch: no counterpart in the reference, which
+ * solves one model per call.  fg_forward_batch runs fg_forward for plans[0..n)
+ * -- models of any grid, shot count and step count -- with every time step of
+ * all of them in one persistent launch (the warps take each model's tiles of
+ * a step in turn, a grid barrier separates the steps, a model whose steps
+ * are done sits out); fg_adjoint_reference_batch does the same for
+ * fg_adjoint_reference (each model's gradient normalised on its own when
+ * normalize != 0).  Every plan must be bound, use the persistent lane march
+ * (fg_tuning.persistent = 1) and share
+ * lanes and cells_per_thread; at most FG_BATCH_MAX plans.  The arrays hold one
+ * pointer per model with the meaning of the single-model calls.  Results
+ * equal the single-model calls' bit for bit. */
+#define FG_BATCH_MAX 8
+int fg_forward_batch(fg_plan* const* plans, int32_t n, const float* const* er, const float* const* se,
+                     const float* const* mr, float* const* traces, float* const* hist, void* stream);
+int fg_adjoint_reference_batch(fg_plan* const* plans, int32_t n, const float* const* er, const float* const* se,
+                               const float* const* mr, const float* const* hist, const float* const* resid,
+                               float* const* grad_eps, float* const* grad_sig, int32_t normalize, void* stream);
 
 /* Checkpointed solve, for histories that do not fit in device memory (the
  * reference keeps the whole Ez history, src/compute.py:553, which limits it

@@ -30,6 +30,10 @@ TUNINGS = [
     {"lanes": 1, "kernel": 2, "cells_per_thread": 4, "warps_per_block": 4, "rows_per_tile": 8, "stages": 4},
     {"lanes": 1, "kernel": 0, "cells_per_thread": 4, "rows_per_tile": 4},
     {"lanes": 2},
+    # the persistent launch; the interior split forced (few or no interior tiles)
+    {"lanes": 1, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 4, "persistent": 1},
+    {"lanes": 1, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 2, "interior": 2},
+    {"lanes": 2, "kernel": 1, "cells_per_thread": 4, "persistent": 1},
 ]
 
 

@@ -129,6 +129,15 @@ TUNINGS = [
     {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 9, "stages": 2},
     {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 16, "warps_per_block": 2, "stages": 4},
     {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 6, "stages": 3},
+    # the whole time loop in one persistent launch
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "persistent": 1},
+    {"kernel": 1, "lanes": 2, "cells_per_thread": 2, "rows_per_tile": 5, "persistent": 1},
+    {"kernel": 1, "lanes": 2, "cells_per_thread": 8, "rows_per_tile": 2, "persistent": 1},
+    # the interior split forced on small grids (general kernel at 1 and 2 blocks per SM)
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "interior": 2},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 2, "rows_per_tile": 3, "interior": 1, "prefetch": 2},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 2, "interior": 2, "adj_kernel": 2,
+     "adj_cells_per_thread": 4},
     # shot pairs (two shots per lane)
     {"kernel": 1, "lanes": 3, "cells_per_thread": 2, "rows_per_tile": 4},
     {"kernel": 1, "lanes": 3, "cells_per_thread": 4, "rows_per_tile": 5},
