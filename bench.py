@@ -83,6 +83,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample length")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-config3", action="store_true", help="skip the config-3 multiscale inversion leg")
     return ap.parse_args()
 
 
@@ -352,6 +353,13 @@ def run_ours(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_e2e:
         per_shot = run_per_shot(args, fg, wl, dev)
 
+    small = ckpt = cfg3 = None
+    if rank == 0 and world == 1 and not args.no_e2e:
+        small = run_small_configs(fg, dev)
+        ckpt = run_checkpointed(args, fg, wl, dev, tuning)
+        if not args.no_config3:
+            cfg3 = run_config3(fg, dev)
+
     serving = None
     if rank == 0 and world == 1 and not args.no_serve:
         serving = run_serving(fg, dev)
@@ -385,6 +393,9 @@ def run_ours(args, rank, local, world):
             "clocks": clk,
             "e2e": e2e,
             "per_shot_path": per_shot,
+            "small_configs": small,
+            "checkpointed": ckpt,
+            "config3": cfg3,
             "serving": serving,
             "cpu_baseline": cpu,
             "fp64_err": fp64,
@@ -473,6 +484,169 @@ def run_per_shot(args, fg, wl, dev, shots=4):
     return {"value": round(wl.nx * wl.ny * shots * wl.nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
             "shots": shots, "ms_per_shot": round(ms / shots, 3),
             "api": "compute(..., step=1, tv=False) + traces.backward(resid), looped over shots"}
+
+
+def run_small_configs(fg, dev, reps=3):
+    """The benchmark's two smaller configurations, each as one forward +
+    reference-mode adjoint per step with inputs resident on the device and
+    the default launch shapes: config 0 (140x100, 1 shot, nt 1200) and
+    config 1 (240x160, 13 shots, nt 3000); same metric as the headline."""
+    out = {}
+    for wl in (fg.workloads.config0(), fg.workloads.config1()):
+        kw = wl.kwargs(dev, tv=False)
+        setup = fg.grid.build_setup(dev, kw["dx"], kw["ny"], kw["nx"], kw["nz"], kw["time_windows"], kw["source"],
+                                    kw["source_location"], kw["source_step"], kw["receiver_location"],
+                                    kw["receiver_step"], kw["pmlthick"], kw["source_apmlitudes"], kw["step"],
+                                    torch.clamp(kw["er"], min=1), kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"], None,
+                                    None, kw["Fixedreceiver"], None, None)
+        solve = fg.Solve(dev, setup, tv=False)
+        plan = solve.plan
+        er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+        S, nt = setup.shots, setup.nt
+        traces = torch.empty((S, nt, plan.nrx), device=dev)
+        hist = plan.new_hist()
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(77)
+        resid = torch.randn(traces.shape, device=dev, generator=gen) * 1e-3
+        ge = torch.empty((setup.nx, setup.ny), device=dev)
+        gs = torch.empty_like(ge)
+
+        def step():
+            plan.forward(er, se, mr, traces, hist)
+            plan.adjoint_reference(er, se, mr, hist, resid, ge, gs)
+
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            step()
+        t1.record()
+        torch.cuda.synchronize(dev)
+        plan.device_check()
+        ms = t0.elapsed_time(t1) / reps
+        out[wl.name] = {"value": round(setup.nx * setup.ny * S * nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                        "ms_per_step": round(ms, 3), "grid": [setup.nx, setup.ny], "shots": S, "nt": nt,
+                        "lanes": "shot lanes" if S >= 8 else "column lanes", "steps": reps, "warmup": 3}
+        del hist, traces, solve, plan
+        torch.cuda.empty_cache()
+    return out
+
+
+def _setup_of(fg, wl, dev, er=None):
+    kw = wl.kwargs(dev, tv=False)
+    er = torch.clamp(kw["er"] if er is None else er, min=1)
+    return fg.grid.build_setup(dev, kw["dx"], kw["ny"], kw["nx"], kw["nz"], kw["time_windows"], kw["source"],
+                               kw["source_location"], kw["source_step"], kw["receiver_location"],
+                               kw["receiver_step"], kw["pmlthick"], kw["source_apmlitudes"], kw["step"], er,
+                               kw["mr"], kw["nsrc"], kw["nrx"], kw["dt"], None, None, kw["Fixedreceiver"], None,
+                               None)
+
+
+def run_checkpointed(args, fg, wl, dev, tuning, steps=2):
+    """The headline workload with checkpoint='auto': the solver state every K
+    steps (K the autotuner's: the fastest checkpointed gradient that fits in
+    80% of the free memory) instead of the whole Ez history; the adjoint
+    recomputes each history segment (one more forward solve per step).  Same
+    metric, inputs resident on the device."""
+    autotune = importlib.import_module(PKG + ".autotune")
+    setup = _setup_of(fg, wl, dev)
+    t_tune = time.perf_counter()
+    solve = fg.Solve(dev, setup, tuning=tuning, tv=False, checkpoint="auto")
+    t_tune = time.perf_counter() - t_tune
+    plan, k = solve.plan, solve.interval
+    er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+    S, nt = setup.shots, setup.nt
+    traces = torch.empty((S, nt, plan.nrx), device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234)
+    resid = torch.randn(traces.shape, device=dev, generator=gen) * 1e-3
+    ge = torch.empty((setup.nx, setup.ny), device=dev)
+    gs = torch.empty_like(ge)
+    ck = plan.new_checkpoints(k)
+    seg = plan.new_segment(k)
+
+    def step():
+        plan.forward_checkpointed(er, se, mr, traces, ck, k)
+        plan.adjoint_reference_checkpointed(er, se, mr, ck, k, seg, resid, ge, gs)
+
+    step()
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        step()
+    t1.record()
+    torch.cuda.synchronize(dev)
+    plan.device_check()
+    ms = t0.elapsed_time(t1) / steps
+    mem = autotune.checkpoint_memory(plan, k)
+    del ck, seg, traces, solve, plan
+    torch.cuda.empty_cache()
+    return {"value": round(setup.nx * setup.ny * S * nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+            "ms_per_step": round(ms, 3), "interval": k, "steps": steps, "warmup": 1,
+            "checkpoints_plus_segment_gb": round(mem / 1e9, 2),
+            "full_history_gb": round(4 * setup.nx * setup.ny * S * nt / 1e9, 1),
+            "autotune_s": round(t_tune, 1),
+            "api": "Solve(checkpoint='auto'): fg_forward_checkpointed + fg_adjoint_reference_checkpointed"}
+
+
+def run_config3(fg, dev, epochs_per_stage=1):
+    """Config 3 end to end: 840x540 (800x500 + 2x20 CPML), 30 shots, nt 6000,
+    the three-stage multiscale inversion of the reference's example (observed
+    traces low-passed at 50, 100 and 200 MHz by apply_filter, compute()'s
+    freq set to the stage's), TV weight 1e-3, one epoch per stage, the
+    gradient checkpointed at the autotuned interval (the full Ez history
+    would be 327 GB).  Observed traces: a forward solve of the true layered
+    model; starting model: its smoothed copy."""
+    ms_mod = importlib.import_module(PKG + ".multiscale")
+    autotune = importlib.import_module(PKG + ".autotune")
+    wl = fg.workloads.config3()
+    setup = _setup_of(fg, wl, dev)
+    true_er, true_se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+    obs, _ = fg.Solve(dev, setup, tv=False).forward(true_er, true_se, mr, keep_history=False)
+    torch.cuda.synchronize(dev)
+    kernel = torch.ones((1, 1, 21, 21), device=dev) / 441.0
+    smooth = lambda a: torch.nn.functional.conv2d(a[None, None], kernel, padding=10)[0, 0]
+    er = smooth(true_er)[:, :, None].contiguous()
+    se = smooth(true_se)[:, :, None].contiguous()
+    mr3 = mr[:, :, None].contiguous()
+    kw = wl.kwargs(dev)
+    for key in ("er", "se", "mr", "tv", "device"):
+        kw.pop(key)
+    stages = []
+    cells = setup.nx * setup.ny * setup.shots * setup.nt
+    for f in (5e7, 1e8, 2e8):
+        obs_f = ms_mod.apply_filter(obs, 1.0 / setup.dt, f)
+        t_plan = time.perf_counter()
+        inv = fg.Inversion(dev, dict(kw, freq=f), obs_f, er, se, mr3, tv_weight=1e-3, checkpoint="auto",
+                           phase1_epochs=0)
+        t_plan = time.perf_counter() - t_plan
+        for _ in range(epochs_per_stage):
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            loss = inv.epoch()
+            t1.record()
+            torch.cuda.synchronize(dev)
+            ms = t0.elapsed_time(t1)
+        k = inv.solve.interval
+        stages.append({"cutoff_mhz": int(f / 1e6), "epoch_ms": round(ms, 1), "loss": round(loss, 6),
+                       "value": round(cells / (ms * 1e-3) / 1e9, 3), "interval": k,
+                       "checkpoints_plus_segment_gb": round(autotune.checkpoint_memory(inv.solve.plan, k) / 1e9, 2),
+                       "plan_and_autotune_s": round(t_plan, 1)})
+        er, se = inv.er.detach(), inv.se.detach()
+        del inv
+        torch.cuda.empty_cache()
+    fp64 = fp64_error(fg, wl, dev, None, shots=1, nt=3000)
+    total_ms = sum(st["epoch_ms"] for st in stages)
+    return {"value": round(len(stages) * cells / (total_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+            "grid": [setup.nx, setup.ny], "shots": setup.shots, "nt": setup.nt, "stages": stages,
+            "epoch": "forward + recomputed forward + fused-L1 reference adjoint + TV (weight 1e-3) + Adam",
+            "full_history_gb": round(4 * cells / 1e9, 1), "fp64_err": fp64}
 
 
 def serving_stream(fg, n=24, seed=4004):
@@ -604,9 +778,13 @@ def fp64_error(fg, wl, dev, tuning, shots=4, nt=1000):
     from oracle import oracle as orc
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import helpers
-    if wl.name != "config2":
+    if wl.name == "config2":
+        sample = fg.workloads.config2(shots=shots, nt=nt)
+    elif wl.name == "config3":
+        sample = fg.workloads.config3()
+        sample.shots, sample.nt = shots, nt
+    else:
         return None
-    sample = fg.workloads.config2(shots=shots, nt=nt)
     t0 = time.perf_counter()
     rng = np.random.default_rng(64)
     w = rng.standard_normal((shots, nt, sample.nrx)).astype(np.float32)

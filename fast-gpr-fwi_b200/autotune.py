@@ -101,3 +101,75 @@ def autotune(device, setup, er, se, mr, probe_steps: int = 64, reps: int = 2, la
     tuning = dict(base, **best_f[1], **best_a[1])
     _CACHE[key] = dict(tuning)
     return tuning
+
+
+# ---------------------------------------------------------------------------
+# Checkpoint interval
+# ---------------------------------------------------------------------------
+CKPT_CANDIDATES = (4, 8, 16, 32, 64, 128, 256)
+_CKPT_CACHE: Dict[Tuple, int] = {}
+
+
+def checkpoint_memory(plan, interval: int) -> int:
+    """Device bytes of a checkpointed gradient at `interval`: the checkpoints
+    plus one history segment."""
+    return max(0, plan.checkpoint_bytes(interval)) + 4 * interval * (plan.hist_floats // plan.nt)
+
+
+def autotune_checkpoint(device, setup, tuning=None, budget: Optional[int] = None, probe_steps: int = 512,
+                        reps: int = 1) -> int:
+    """The checkpoint interval K of the fastest checkpointed gradient
+    (fg_forward_checkpointed + fg_adjoint_reference_checkpointed) among the
+    candidate intervals whose checkpoints and history segment fit in `budget`
+    bytes (default: 80% of the free device memory).
+
+    Each candidate is timed on a truncated run of `probe_steps` steps (at
+    least two segments of the largest candidate); its cost per step --
+    the checkpoint copies every K steps, the recomputed forward and the
+    adjoint, with a segment that stays in L2 or not -- carries over to the
+    full run.  Ties within 2% go to the smaller footprint.  Cached per
+    (device, grid, shots, nt, CPML, tuning, budget argument)."""
+    device = torch.device(device)
+    key = (torch.cuda.get_device_name(device), setup.nx, setup.ny, setup.shots, setup.nt, setup.th,
+           repr(sorted((tuning or {}).items())), budget)
+    if key in _CKPT_CACHE:
+        return _CKPT_CACHE[key]
+    if budget is None:
+        free, _ = torch.cuda.mem_get_info(device)
+        budget = int(0.8 * free)
+    s = setup
+    pml = s.profile.packed() if s.profile is not None else None
+    full = _native.Plan(s.nx, s.ny, s.shots, s.nt, s.th, s.dx, s.dt32, s.src.cpu().numpy(), s.rx.cpu().numpy(),
+                        s.srcw, pml, device, tuning, bind=False)
+    fits = [k for k in CKPT_CANDIDATES if k < s.nt and full.workspace_bytes + checkpoint_memory(full, k) <= budget]
+    if not fits:
+        # the smallest footprint there is (the interval that minimises it)
+        from .compute import checkpoint_interval
+        k = checkpoint_interval(full, True)
+        _CKPT_CACHE[key] = k
+        return k
+    steps = min(s.nt, max(int(probe_steps), 2 * max(fits)))
+    p = _probe_plan(setup, device, tuning, steps)
+    ones = torch.ones((s.nx, s.ny), dtype=torch.float32, device=device)
+    er, se, mr = 4 * ones, 1e-3 * ones, ones
+    tr = torch.empty((s.shots, steps, p.nrx), device=device)
+    resid = torch.zeros_like(tr)
+    ge = torch.empty((s.nx, s.ny), device=device)
+    gs = torch.empty_like(ge)
+    timed = []
+    for k in fits:
+        ck = p.new_checkpoints(k)
+        seg = p.new_segment(k)
+
+        def run():
+            p.forward_checkpointed(er, se, mr, tr, ck, k)
+            p.adjoint_reference_checkpointed(er, se, mr, ck, k, seg, resid, ge, gs)
+
+        timed.append((_time_ms(run, reps), checkpoint_memory(full, k), k))
+        del ck, seg
+    del p
+    torch.cuda.empty_cache()
+    fastest = min(t for t, _, _ in timed)
+    k = min((m, k) for t, m, k in timed if t <= 1.02 * fastest)[1]
+    _CKPT_CACHE[key] = k
+    return k

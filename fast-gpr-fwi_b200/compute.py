@@ -105,6 +105,11 @@ class Solve:
         self.plan = _native.Plan(s.nx, s.ny, s.shots, s.nt, s.th, s.dx, s.dt32,
                                  s.src.cpu().numpy(), s.rx.cpu().numpy(), s.srcw, pml, self.device, tuning,
                                  bind=bind)
+        if isinstance(checkpoint, str):
+            if checkpoint != "auto":
+                raise ValueError("checkpoint must be None, True, an interval or 'auto'")
+            from .autotune import autotune_checkpoint
+            checkpoint = autotune_checkpoint(self.device, s, tuning=tuning)
         self.interval = checkpoint_interval(self.plan, checkpoint)
         if adjoint == "exact" and self.interval is not None:
             raise ValueError("adjoint='exact' keeps the whole Ez history (checkpoint=None)")
@@ -200,7 +205,10 @@ def compute(device, dx, ny, nx, nz, source, source_apmlitudes, step, er, se, mr,
     reference): None keeps the whole Ez history for the gradient, as the
     reference does; an int K keeps the solver state every K steps instead and
     recomputes the history segment by segment during the backward pass (one
-    extra forward solve, same results bit for bit); True picks K.
+    extra forward solve, same results bit for bit); True picks the K of the
+    smallest footprint; 'auto' the K of the fastest checkpointed gradient
+    that fits in 80% of the free device memory, measured on a truncated run
+    (autotune.autotune_checkpoint, cached per geometry).
     ``tuning`` (not in the reference): None = default launch shapes, a dict of
     fg_tuning fields, or 'auto' = the fastest shapes for this geometry
     measured on a truncated run (autotune.py, cached per geometry).

@@ -697,8 +697,12 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
         at.warps_per_block = p->WPB;
         at.stages = p->D;
     } else if (ak == 0) {
+        // 8 cells per thread where the interior split runs (the 440 x 340
+        // 64-shot grid), 4 on smaller steps (measured on 240 x 160, 13 shots:
+        // 110 against 130 ms per adjoint)
+        const long long work = (long long)prob->nx * prob->ny * ((prob->shots + 31) / 32);
         at.kernel = 1;
-        at.cells_per_thread = 8;
+        at.cells_per_thread = work >= 200000 ? 8 : 4;
         at.rows_per_tile = tune && tune->adj_rows_per_tile ? tune->adj_rows_per_tile : 4;
         at.warps_per_block = tune && tune->adj_warps_per_block ? tune->adj_warps_per_block : 4;
         at.stages = tune && tune->adj_stages ? tune->adj_stages : 0;

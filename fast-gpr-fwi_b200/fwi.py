@@ -12,6 +12,12 @@ tensor torch's L1Loss backward would build is never materialised.
 With the same inputs an epoch produces the gradients the notebook's
 compute() + L1Loss + backward() produce (tests/test_gpu_fwi.py).
 
+checkpoint (an interval, True or 'auto', as compute()'s) keeps the solver
+state every K steps instead of the whole Ez history and recomputes the
+history segment by segment in the adjoint; the L1 derivative is then formed
+by three tensor operations (the same float32 values) and injected as a
+residual.  Results equal the full-history epoch's bit for bit.
+
 graph=True captures an epoch's solve -- the coefficient kernels, state
 resets, 2 nt - 1 step launches and the gradient reductions -- in a CUDA graph
 with static model, trace and gradient buffers, and replays it every epoch
@@ -43,7 +49,7 @@ class Inversion:
     def __init__(self, device, kwargs: dict, observed: torch.Tensor, er0: torch.Tensor, se0: torch.Tensor,
                  mr: torch.Tensor, phase1_epochs: int = 50, lr: Sequence[float] = (0.2, 0.1, 1e-4),
                  loss_weight: float = 100.0, tv: bool = True, tv_weight: float = 0.01,
-                 tuning: Optional[dict] = None, graph: bool = False):
+                 tuning: Optional[dict] = None, graph: bool = False, checkpoint=None):
         self.device = torch.device(device)
         kw = dict(kwargs)
         self.pml = int(kw.get("pmlthick", 0))
@@ -56,7 +62,7 @@ class Inversion:
         self.opt1 = torch.optim.Adam([{"params": self.er, "lr": lr[0]}])
         self.opt2 = torch.optim.Adam([{"params": self.er, "lr": lr[1]}, {"params": self.se, "lr": lr[2]}])
         self.kw = kw
-        self.solve_args = dict(tuning=tuning, tv=tv, tv_weight=tv_weight)
+        self.solve_args = dict(tuning=tuning, tv=tv, tv_weight=tv_weight, checkpoint=checkpoint)
         self.use_graph = bool(graph)
         self._graph = None
         self._row0 = None
@@ -92,7 +98,15 @@ class Inversion:
         self._s32 = torch.empty_like(self._e32)
         self._m32 = self.solve.materials(self.mr, self.mr, self.mr)[2]
         self._traces = torch.empty((s.shots, s.nt, p.nrx), dtype=torch.float32, device=self.device)
-        self._hist = p.new_hist()
+        k = self.solve.interval
+        if k is None:
+            self._hist = p.new_hist()
+        else:
+            # checkpoints every k steps, one history segment, the L1 derivative
+            self._hist = None
+            self._ck = p.new_checkpoints(k)
+            self._seg = p.new_segment(k)
+            self._resid = torch.empty_like(self._traces)
         self._ge = torch.empty((s.nx, s.ny), dtype=torch.float32, device=self.device)
         self._gs = torch.empty_like(self._ge)
 
@@ -100,10 +114,21 @@ class Inversion:
         """Forward + fused L1 adjoint on the static buffers (eagerly or as a graph replay)."""
         p = self.solve.plan
 
+        k = self.solve.interval
+
         def run():
-            p.forward(self._e32, self._s32, self._m32, self._traces, self._hist)
-            p.adjoint_reference_l1(self._e32, self._s32, self._m32, self._hist, self._traces, self.observed,
-                                   self.scale, self._ge, self._gs)
+            if k is None:
+                p.forward(self._e32, self._s32, self._m32, self._traces, self._hist)
+                p.adjoint_reference_l1(self._e32, self._s32, self._m32, self._hist, self._traces, self.observed,
+                                       self.scale, self._ge, self._gs)
+                return
+            p.forward_checkpointed(self._e32, self._s32, self._m32, self._traces, self._ck, k)
+            # scale * sign(syn - obs) in float32, the value the fused injection forms
+            torch.sub(self._traces, self.observed, out=self._resid)
+            torch.sign(self._resid, out=self._resid)
+            self._resid.mul_(self.scale)
+            p.adjoint_reference_checkpointed(self._e32, self._s32, self._m32, self._ck, k, self._seg, self._resid,
+                                             self._ge, self._gs)
 
         if not self.use_graph:
             run()

@@ -93,7 +93,8 @@ typedef struct fg_tuning {
     /* The adjoint runs on a plan of its own (own state and accumulators); its
      * launch shape: adj_kernel 0 = the forward's shape when the fields above
      * name one, else the default adjoint shape (shot lanes: lane march with
-     * 8 cells per thread over 4 rows; column lanes: the forward's);
+     * 8 cells per thread over 4 rows -- 4 cells when nx * ny * shot groups is
+     * below 2e5; column lanes: the forward's);
      * 1 = tile pipeline, 2 = lane march, shaped by the three fields below
      * (0 = their defaults).  lanes is shared; adj_cells_per_thread (0 = the
      * forward's cells_per_thread) sets the adjoint's own.  The Ez history

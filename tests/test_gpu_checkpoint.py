@@ -67,7 +67,7 @@ def test_checkpoint_keyword_through_compute(fg):
     dev = torch.device("cuda:0")
     wl = fg.workloads.small(shots=3, nt=100)
     res = []
-    for ckp in (None, 9, True):
+    for ckp in (None, 9, True, "auto"):
         er = torch.tensor(wl.er[:, :, None], device=dev, requires_grad=True)
         se = torch.tensor(wl.se[:, :, None], device=dev, requires_grad=True)
         traces, _ = fg.compute(**wl.kwargs(dev, er=er, se=se, tv=False, checkpoint=ckp))
@@ -77,3 +77,24 @@ def test_checkpoint_keyword_through_compute(fg):
     for other in res[1:]:
         for a, b in zip(res[0], other):
             assert np.array_equal(a, b)
+
+
+@gpu
+def test_autotuned_interval_fits_the_budget(fg):
+    """autotune_checkpoint: a candidate interval whose checkpoints plus one
+    history segment fit the budget; the smallest-footprint interval when
+    none does."""
+    from importlib import import_module
+    at = import_module(helpers.PKG + ".autotune")
+    dev = torch.device("cuda:0")
+    wl = fg.workloads.small(shots=9, nt=300, nx=64, ny=56, fixed=True)
+    wl.source_step = [0.05, 0.02, 0.0]
+    setup = helpers.setup_for(wl, dev)
+    plan = fg.Solve(dev, setup, tv=False, bind=False).plan
+    k = at.autotune_checkpoint(dev, setup, probe_steps=64)
+    assert k in at.CKPT_CANDIDATES
+    budget = plan.workspace_bytes + at.checkpoint_memory(plan, 32)
+    k2 = at.autotune_checkpoint(dev, setup, budget=budget, probe_steps=64)
+    assert plan.workspace_bytes + at.checkpoint_memory(plan, k2) <= budget
+    k3 = at.autotune_checkpoint(dev, setup, budget=1)
+    assert k3 == import_module(helpers.PKG + ".compute").checkpoint_interval(plan, True)

@@ -87,3 +87,20 @@ def test_inversion_graph_replay_equals_eager(fg):
     assert runs[0][0] == runs[1][0]
     assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][2], runs[1][2])
     assert runs[1][3] and not runs[0][3]
+
+
+def test_inversion_checkpointed_equals_full_history(fg):
+    """Checkpointed epochs (state every k steps, L1 derivative as a residual)
+    give the full-history epochs' losses and models bit for bit."""
+    wl, dev, obs, er0, se0, mr = _problem(fg)
+    kw = wl.kwargs(dev, tv=True)
+    for k in ("er", "se", "mr", "tv", "device"):
+        kw.pop(k)
+    runs = []
+    for ckp in (None, 7, "auto"):
+        inv = fg.Inversion(dev, kw, obs, er0, se0, mr, phase1_epochs=2, checkpoint=ckp)
+        losses = [inv.epoch() for _ in range(4)]
+        runs.append((losses, inv.er.detach().cpu().numpy(), inv.se.detach().cpu().numpy()))
+    for other in runs[1:]:
+        assert other[0] == runs[0][0]
+        assert np.array_equal(other[1], runs[0][1]) and np.array_equal(other[2], runs[0][2])
