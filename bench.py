@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU sample length")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-config3", action="store_true", help="skip the config-3 multiscale inversion leg")
+    ap.add_argument("--aux", action="store_true",
+                    help="time only the TV and FIR kernels at config-3 sizes (one JSON line, not the headline)")
     return ap.parse_args()
 
 
@@ -855,8 +857,54 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_aux(args):
+    """The kernels around the solver at config-3 sizes, timed alone: the TV
+    kernel on an 840x540 model (ADMM, up to 500 iterations, tol 1e-5, the
+    reference's defaults) and the causal FIR kernel on 30 shots x 6000 steps
+    x 120 receivers at the 50 MHz stage.  One JSON line (not the headline)."""
+    fg = _fg()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ms_mod = importlib.import_module(PKG + ".multiscale")
+    nat = importlib.import_module(PKG + "._native")
+    wl = fg.workloads.config3()
+    model = torch.tensor(wl.er, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    traces = torch.randn((wl.shots, wl.nt, wl.nrx), device=dev, generator=gen)
+    fs = 1.0 / wl.dt
+    numtaps = int(fs / 5e7)
+    taps = ms_mod.design_fir_filter(5e7, fs, numtaps)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            out = fn()
+        t1.record()
+        torch.cuda.synchronize(dev)
+        return t0.elapsed_time(t1) / reps, out
+
+    reps = max(1, args.steps)
+    tv_ms, (_, iters) = timed(lambda: nat.total_variation(model, 0.02, 1.0, 500, 1e-5), reps)
+    fir_ms, _ = timed(lambda: nat.fir_causal(traces, taps), reps)
+    moved = 2 * traces.numel() * 4
+    line = {"aux": True, "config": "config-3 sizes: model 840x540; traces 30x6000x120, %d taps" % numtaps,
+            "tv": {"ms": round(tv_ms, 3), "iterations": iters, "cells": model.numel()},
+            "fir": {"ms": round(fir_ms, 3), "taps": numtaps, "bytes_in_out": moved,
+                    "achieved_gbs": round(moved / (fir_ms * 1e-3) / 1e9, 1)},
+            "steps": reps}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.aux:
+        run_aux(args)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
