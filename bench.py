@@ -61,8 +61,14 @@ UNIT = "Gcell-steps/s"
 
 # DRAM bytes per shot-cell-step of each step kernel, from one ncu capture on the 440 x 340 grid with 64 shots
 # (read + write); a kernel with no capture reports null traffic
-NCU_BYTES_PER_SHOT_CELL_STEP = {"fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340),
-                                "fg::k_adj (": 293.9e6 / (64 * 440 * 340)}
+# DRAM bytes (read + write) per launch of a step from one ncu capture of the
+# 64-shot 440x340 workload, per shot and cell; a split step adds its two
+# kernels (boundary lane march + interior kernel)
+NCU_BYTES_PER_SHOT_CELL_STEP = {
+    "fg::k_fwd + fg::k_fwd_core": (54.3e6 + 14.7e6 + 89.8e6 + 63.9e6) / (64 * 440 * 340),
+    "fg::k_adj + fg::k_adj_core": (79.9e6 + 15.4e6 + 119.6e6 + 50.4e6) / (64 * 440 * 340),
+    "fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340),
+    "fg::k_adj (": 293.9e6 / (64 * 440 * 340)}
 
 
 def _fg():
@@ -118,9 +124,14 @@ def strip_cells(nx, ny, th):
     return 2 * th * ny + 2 * th * nx
 
 
-def kernel_name(tuning, direction):
-    """The step kernel a default (or given) launch shape runs, for the report."""
+def kernel_name(tuning, direction, split=False):
+    """The step kernel a default (or given) launch shape runs, for the report
+    (split: the interior tiles run in a kernel of their own beside it)."""
     t = tuning or {}
+    if split:
+        d = "fwd" if direction == "forward" else "adj"
+        return "fg::k_%s + fg::k_%s_core (lane march on the boundary tiles beside the interior kernel, %s step)" % (
+            d, d, direction)
     if direction == "forward":
         k = t.get("kernel", 1)
     else:
@@ -332,11 +343,17 @@ def run_ours(args, rank, local, world):
     bytes_launch = adj_b if dom == "adjoint" else fwd_b
     launch_ms = adj_launch_ms if dom == "adjoint" else fwd_launch_ms
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
-    ncu = next((v for k, v in NCU_BYTES_PER_SHOT_CELL_STEP.items() if kernel_name(tuning, dom).startswith(k)), None)
+    # the interior split of the lane march (shot lanes, no stages, nx * ny * groups >= 2e5)
+    t = tuning or {}
+    shot = t.get("lanes", 1 if S >= 8 else 2) == 1
+    split = (shot and t.get("interior", 0) != -1 and not t.get("stages") and t.get("kernel", 1) == 1
+             and (t.get("interior", 0) > 0 or nx * ny * ((S + 31) // 32) >= 200000))
+    kname = kernel_name(tuning, dom, split)
+    ncu = next((v for k, v in NCU_BYTES_PER_SHOT_CELL_STEP.items() if kname.startswith(k)), None)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": None if ncu is None else int(ncu * S * nx * ny),
-                "kernel": kernel_name(tuning, dom),
+                "kernel": kname,
                 "algorithmic_bytes_per_launch": int(bytes_launch), "launch_ms": round(launch_ms, 5)}
     other = {"forward": {"launch_ms": round(fwd_launch_ms, 5), "algorithmic_bytes_per_launch": int(fwd_b),
                          "achieved_gbs": round(fwd_b / (fwd_launch_ms * 1e-3) / 1e9, 1),
