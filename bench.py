@@ -613,11 +613,12 @@ def run_checkpointed(args, fg, wl, dev, tuning, steps=2):
             "api": "Solve(checkpoint='auto'): fg_forward_checkpointed + fg_adjoint_reference_checkpointed"}
 
 
-def run_config3(fg, dev, epochs_per_stage=1):
+def run_config3(fg, dev, epochs_per_stage=2):
     """Config 3 end to end: 840x540 (800x500 + 2x20 CPML), 30 shots, nt 6000,
     the three-stage multiscale inversion of the reference's example (observed
     traces low-passed at 50, 100 and 200 MHz by apply_filter, compute()'s
-    freq set to the stage's), TV weight 1e-3, one epoch per stage, the
+    freq set to the stage's), TV weight 1e-3, two epochs per stage (the
+    workload names 20; every epoch is the same work), the
     gradient checkpointed at the autotuned interval (the full Ez history
     would be 327 GB).  Observed traces: a forward solve of the true layered
     model; starting model: its smoothed copy."""
@@ -644,16 +645,19 @@ def run_config3(fg, dev, epochs_per_stage=1):
         inv = fg.Inversion(dev, dict(kw, freq=f), obs_f, er, se, mr3, tv_weight=1e-3, checkpoint="auto",
                            phase1_epochs=0)
         t_plan = time.perf_counter() - t_plan
+        times, losses = [], []
         for _ in range(epochs_per_stage):
             t0 = torch.cuda.Event(enable_timing=True)
             t1 = torch.cuda.Event(enable_timing=True)
             t0.record()
-            loss = inv.epoch()
+            losses.append(round(inv.epoch(), 6))
             t1.record()
             torch.cuda.synchronize(dev)
-            ms = t0.elapsed_time(t1)
+            times.append(t0.elapsed_time(t1))
+        ms = float(np.mean(times))
         k = inv.solve.interval
-        stages.append({"cutoff_mhz": int(f / 1e6), "epoch_ms": round(ms, 1), "loss": round(loss, 6),
+        stages.append({"cutoff_mhz": int(f / 1e6), "epoch_ms": round(ms, 1), "epochs": epochs_per_stage,
+                       "losses": losses,
                        "value": round(cells / (ms * 1e-3) / 1e9, 3), "interval": k,
                        "checkpoints_plus_segment_gb": round(autotune.checkpoint_memory(inv.solve.plan, k) / 1e9, 2),
                        "plan_and_autotune_s": round(t_plan, 1)})
@@ -661,62 +665,100 @@ def run_config3(fg, dev, epochs_per_stage=1):
         del inv
         torch.cuda.empty_cache()
     fp64 = fp64_error(fg, wl, dev, None, shots=1, nt=3000)
-    total_ms = sum(st["epoch_ms"] for st in stages)
+    total_ms = sum(st["epoch_ms"] for st in stages)   # one epoch of each stage
     return {"value": round(len(stages) * cells / (total_ms * 1e-3) / 1e9, 3), "unit": UNIT,
             "grid": [setup.nx, setup.ny], "shots": setup.shots, "nt": setup.nt, "stages": stages,
             "epoch": "forward + recomputed forward + fused-L1 reference adjoint + TV (weight 1e-3) + Adam",
             "full_history_gb": round(4 * cells / 1e9, 1), "fp64_err": fp64}
 
 
-def serving_stream(fg, n=24, seed=4004):
-    """A seeded stream in the spirit of the serving workload: grids from
-    100x60 to 256x256 plus a 20-cell CPML, 1-32 shots, nt 1000-2000,
-    100-200 MHz Ricker, layered models as the benchmark's; half forward,
-    half gradient requests."""
+def serving_stream(fg, n=12, seed=4004):
+    """A seeded stream drawn from the serving workload's distribution:
+    physical grids uniform from 100x60 to 1024x1024 cells (plus a 20-cell
+    CPML per side), dx 0.025 m, nt uniform in 1000-8000, 1-32 shots, 100-200
+    MHz Ricker, layered models as the benchmark's, cross-hole geometry.  Half
+    the requests are gradients, each on its own survey; the other half are
+    forward requests in pairs that share a survey (grid, model, waveform)
+    with different shot positions, which the server may merge."""
     serve = importlib.import_module(PKG + ".serve")
+    wmod = fg.workloads
     rng = np.random.default_rng(seed)
     reqs = []
+    survey = None
     for k in range(n):
-        nz_, nx_ = int(rng.integers(60, 257)), int(rng.integers(100, 257))
+        forward = k % 4 in (1, 2)               # pairs of forward requests: (1, 2), (5, 6), ...
+        if not (forward and k % 4 == 2):
+            nx_ = int(rng.integers(100, 1025))
+            ny_ = int(rng.integers(60, 1025))
+            nt = int(rng.integers(1000, 8001))
+            freq = float(rng.uniform(1e8, 2e8))
+            dx = 0.025
+            er, se = wmod._layered_model(rng, nx_, ny_, dx)
+            er = wmod._pad(er, wmod.PAD).astype(np.float32)
+            se = wmod._pad(se, wmod.PAD).astype(np.float32)
+            survey = (nx_, ny_, nt, freq, er, se)
+        nx_, ny_, nt, freq, er, se = survey
         shots = int(rng.integers(1, 33))
-        nt = int(rng.integers(1000, 2001))
-        wl = fg.workloads.small(seed=seed + k, nx=nx_ + 40, ny=nz_ + 40, shots=shots, nt=nt, pml=20, dx=0.025,
-                                fixed=True, nrx=16)
-        wl.freq = float(rng.uniform(1e8, 2e8))
-        wl.source_step = [0.0, 0.0, 0.0]
+        p = wmod.PAD * dx
+        lx, ly = nx_ * dx, ny_ * dx
+        wl = wmod.Workload("serve", nx_ + 2 * wmod.PAD, ny_ + 2 * wmod.PAD, dx, shots, nt, freq, er, se,
+                           np.ones_like(er), source_location=[p + 0.05 * lx, p + 0.1 * ly, 0.0],
+                           source_step=[0.9 * lx / shots, 0.0, 0.0],
+                           receiver_location=[p + 0.05 * lx, p + 0.9 * ly, 0.0],
+                           receiver_step=[0.9 * lx / 16, 0.0, 0.0], nrx=16, fixed_receiver=True)
+        if forward and k % 4 == 2:
+            wl.source_location[0] += 0.45 * lx / shots     # the pair's second request: shots in between
         kw = wl.kwargs("cuda")
         for key in ("er", "se", "mr", "device", "tv"):
             kw.pop(key)
         resid = None
-        if k % 2:
+        if not forward:
             resid = torch.tensor(rng.standard_normal((shots, nt, wl.nrx)).astype(np.float32) * 1e-3)
-        reqs.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid))
+        reqs.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid,
+                                  merge_key=("survey", k // 4) if forward else None))
     return serve, reqs
 
 
-def run_serving(fg, dev, rate_hz=40.0):
-    """Continuous batching against one request at a time, same stream and
-    arrivals (Poisson, seeded): p50 / p99 latency and throughput."""
+def _serve_once(serve, dev, reqs, gaps, active):
+    srv = serve.Server(dev, max_active=active)
+    futs = []
+    for r, gap in zip(reqs, gaps):
+        time.sleep(float(gap))
+        futs.append(srv.submit(r))
+    for f in futs:
+        f.result()
+    st = srv.stats()
+    srv.close()
+    return {"p50_ms": round(st["p50_s"] * 1e3, 1), "p99_ms": round(st["p99_s"] * 1e3, 1),
+            "throughput_gcs": round(st["throughput_gcs"], 3), "peak_active": st["peak_active"],
+            "merged": st["merged"]}
+
+
+def run_serving(fg, dev, rates_x=(0.5, 1.0, 2.0)):
+    """The stream at Poisson rates swept across saturation, served with
+    continuous batching (4 requests on the GPU at once, forward requests of
+    one survey merged), against the plain one-request-at-a-time path at the
+    highest rate.  The saturation rate is measured first: requests per second
+    of the one-at-a-time path with all requests queued at once."""
     serve, reqs = serving_stream(fg)
-    gaps = np.random.default_rng(7).exponential(1.0 / rate_hz, size=len(reqs))
-    out = {}
-    for name, active in (("continuous", 4), ("one_at_a_time", 1)):
-        srv = serve.Server(dev, max_active=active)
-        srv.submit(reqs[0]).result()          # warm-up (plan, kernels)
-        srv.results.clear()
-        futs = []
-        for r, gap in zip(reqs, gaps):
-            time.sleep(float(gap))
-            futs.append(srv.submit(r))
-        for f in futs:
-            f.result()
-        st = srv.stats()
-        srv.close()
-        out[name] = {"p50_ms": round(st["p50_s"] * 1e3, 2), "p99_ms": round(st["p99_s"] * 1e3, 2),
-                     "throughput_gcs": round(st["throughput_gcs"], 3), "peak_active": st["peak_active"]}
+    warm = serve.Server(dev, max_active=1)
+    warm.submit(reqs[0]).result()                 # plans, kernels, allocator
+    warm.close()
+    t0 = time.perf_counter()
+    base = _serve_once(serve, dev, reqs, np.zeros(len(reqs)), 1)
+    sat = len(reqs) / (time.perf_counter() - t0)
+    rates = []
+    for x in rates_x:
+        gaps = np.random.default_rng(7).exponential(1.0 / (x * sat), size=len(reqs))
+        rates.append(dict(rate_hz=round(x * sat, 3), **_serve_once(serve, dev, reqs, gaps, 4)))
+    top = np.random.default_rng(7).exponential(1.0 / (rates_x[-1] * sat), size=len(reqs))
+    one = dict(rate_hz=round(rates_x[-1] * sat, 3), **_serve_once(serve, dev, reqs, top, 1))
     torch.cuda.empty_cache()
-    return {"requests": len(reqs), "arrivals": "Poisson %.0f/s" % rate_hz,
-            "unit": "Gcell-steps/s of solver steps (forward and adjoint steps each counted)", **out}
+    return {"requests": len(reqs), "saturation_hz": round(sat, 3), "all_queued_one_at_a_time": base,
+            "rates": rates, "one_at_a_time": one,
+            "stream": "grids 100x60-1024x1024 (+2x20 CPML), nt 1000-8000, 1-32 shots, 100-200 MHz; "
+                      "half gradients, half forward requests in same-survey pairs",
+            "unit": "Gcell-steps/s, nx*ny*shots*nt per request counted once (forward or gradient)"}
 
 
 # ---------------------------------------------------------------------------

@@ -31,7 +31,7 @@ EXPORTS = (
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
     "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
     "fg_fir_causal", "fg_adjoint_reference_l1", "fg_adjoint_exact",
-    "fg_forward_batch", "fg_adjoint_reference_batch",
+    "fg_forward_batch", "fg_adjoint_reference_batch", "fg_plan_set_profile",
 )
 
 BATCH_MAX = 8   # FG_BATCH_MAX
@@ -123,6 +123,8 @@ def lib() -> ctypes.CDLL:
     L.fg_adjoint_reference_l1.restype = ctypes.c_int
     L.fg_adjoint_exact.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.fg_adjoint_exact.restype = ctypes.c_int
+    L.fg_plan_set_profile.argtypes = [vp, vp, vp]
+    L.fg_plan_set_profile.restype = ctypes.c_int
     L.fg_forward_batch.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp]
     L.fg_forward_batch.restype = ctypes.c_int
     L.fg_adjoint_reference_batch.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, i32, vp]
@@ -223,6 +225,13 @@ class Plan:
         nt, groups, nx, pitch, slots = self.hist_shape
         h = hist.view(nt, groups, nx, pitch, slots).permute(0, 1, 4, 2, 3).reshape(nt, groups * slots, nx, pitch)
         return h[:, :self.shots, :, :self.ny]
+
+    def set_profile(self, pml: np.ndarray):
+        """fg_plan_set_profile: a new CPML profile (8 * th floats), same tables and buffers."""
+        self._pml = np.ascontiguousarray(pml, dtype=np.float32)
+        if self._pml.size != 8 * self.th:
+            raise ValueError("profile must hold 8 * th = %d floats" % (8 * self.th))
+        check(lib().fg_plan_set_profile(self._h, self._pml.ctypes.data, stream_handle(self.device)))
 
     def device_check(self):
         """Synchronise and raise if a kernel recorded a device-side error."""
@@ -331,8 +340,10 @@ def coefficients(er32, se32, mr32, dt32, dx32, adjoint, pitch=None):
     return out
 
 
-def total_variation(data: torch.Tensor, lamda: float, rho: float, num_iter: int, tol: float):
-    """fg_total_variation on a 2-D float32 CUDA tensor: (denoised copy, iterations)."""
+def total_variation(data: torch.Tensor, lamda: float, rho: float, num_iter: int, tol: float, wait: bool = True):
+    """fg_total_variation on a 2-D float32 CUDA tensor: (denoised copy,
+    iterations).  wait=False only enqueues (capturable in a CUDA graph; the
+    iteration count is then None and a barrier time-out is not reported)."""
     if data.dim() != 2 or data.dtype != torch.float32 or not data.is_cuda:
         raise ValueError("total_variation kernel: needs a 2-D float32 CUDA tensor")
     L = lib()
@@ -344,8 +355,9 @@ def total_variation(data: torch.Tensor, lamda: float, rho: float, num_iter: int,
     with torch.cuda.device(d.device):
         stream = torch.cuda.current_stream(d.device).cuda_stream
         check(L.fg_total_variation(d.data_ptr(), M, N, float(lamda), float(rho), int(num_iter), float(tol),
-                                   out.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(iters), stream))
-    return out, int(iters.value)
+                                   out.data_ptr(), ws.data_ptr(), ws.numel(), ctypes.byref(iters) if wait else None,
+                                   stream))
+    return out, int(iters.value) if wait else None
 
 
 def fir_causal(x: torch.Tensor, taps: torch.Tensor) -> torch.Tensor:

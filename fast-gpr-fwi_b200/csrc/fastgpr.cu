@@ -496,11 +496,12 @@ int fg_total_variation(const float* data, int32_t M, int32_t N, double lamda, do
     void* args[] = {&a};
     FG_CUDA(cudaLaunchCooperativeKernel((const void*)fg::k_total_variation, dim3((unsigned)blocks),
                                         dim3(fg::TV_THREADS), args, 0, st));
+    if (!iters) return FG_OK;   // enqueue only (capturable): the status words stay in the workspace
     int words[2] = {0, 0};
     FG_CUDA(cudaMemcpyAsync(words, w + L.words + 8, sizeof(words), cudaMemcpyDeviceToHost, st));
     FG_CUDA(cudaStreamSynchronize(st));
     if (words[0] != 0) return fail(FG_ERR_TIMEOUT, "fg_total_variation: a grid barrier gave up");
-    if (iters) *iters = words[1];
+    *iters = words[1];
     return FG_OK;
 }
 
@@ -862,6 +863,24 @@ int fg_plan_bind(fg_plan* p, void* workspace, int64_t bytes, void* stream) {
     if (rc == FG_OK && p->adj)
         rc = bind_one(p->adj, (char*)workspace + own_bytes(p), bytes - (int64_t)own_bytes(p), stream);
     return rc;
+}
+
+int fg_plan_set_profile(fg_plan* p, const float* pml, void* stream) {
+    if (!p) return fail(FG_ERR_INVALID, "fg_plan_set_profile: NULL plan");
+    if (p->th == 0) return FG_OK;
+    if (!pml) return fail(FG_ERR_INVALID, "fg_plan_set_profile: NULL profile");
+    cudaStream_t st = (cudaStream_t)stream;
+    fg_plan* plans[2] = {p, p->adj};
+    for (fg_plan* q : plans) {
+        if (!q) continue;
+        q->pml.assign(pml, pml + 8 * (size_t)q->th);
+        // the allocation-free entry point re-uploads the tables of a plan it has not seen
+        q->id = g_next_plan_id.fetch_add(1);
+        if (q->ws)
+            FG_CUDA(cudaMemcpyAsync(q->ws + q->o_pml, q->pml.data(), q->pml.size() * sizeof(float),
+                                    cudaMemcpyHostToDevice, st));
+    }
+    return FG_OK;
 }
 
 int fg_coefficients(const float* er, const float* se, const float* mr, int32_t nx, int32_t ny, float dt, float dx,

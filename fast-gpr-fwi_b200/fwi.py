@@ -2,9 +2,10 @@
 cell): Adam on eps_r (and, after a first phase, sigma), an L1 misfit times a
 weight, gradients zeroed on the CPML columns, the TV term of the default
 gradient.  Each epoch is one forward solve and one adjoint solve; the plan is
-rebuilt only when the model's first row changes (the HORIPML profile
-averages it, grid.slab_average) -- the reference rebuilds its grid, PML
-profile and coefficient arrays in every compute() call -- and the L1
+built once, and when the model's first row changes (the HORIPML profile
+averages it, grid.slab_average) only its CPML profile is replaced -- the
+reference rebuilds its grid, PML profile and coefficient arrays in every
+compute() call -- and the L1
 misfit's derivative is formed
 inside the adjoint's injection (fg_adjoint_reference_l1), so the residual
 tensor torch's L1Loss backward would build is never materialised.
@@ -18,11 +19,21 @@ history segment by segment in the adjoint; the L1 derivative is then formed
 by three tensor operations (the same float32 values) and injected as a
 residual.  Results equal the full-history epoch's bit for bit.
 
+graph='epoch' captures the whole epoch -- clamps, coefficient kernels,
+solve, loss, the TV kernel, the clamps' backward, border zeroing and the
+Adam step (capturable Adam) -- and replays it; only the loss and row 0 of
+eps_r (to see whether the CPML profile changed; when it did, the new profile
+is uploaded before the replay) come back to the host.  It
+computes the bits of the eager epoch with adam_capturable=True (capturable
+Adam rounds its bias corrections on the device, so it can differ from the
+default Adam in the last ulp).
+
 graph=True captures an epoch's solve -- the coefficient kernels, state
 resets, 2 nt - 1 step launches and the gradient reductions -- in a CUDA graph
 with static model, trace and gradient buffers, and replays it every epoch
-after copying the current models in; the graph is captured again when the
-plan is rebuilt.  Replays compute the eager solve's bits.
+after copying the current models in (a new CPML profile is written into
+the plan's workspace before the replay, so the capture stays valid).
+Replays compute the eager solve's bits.
 """
 from __future__ import annotations
 
@@ -49,7 +60,7 @@ class Inversion:
     def __init__(self, device, kwargs: dict, observed: torch.Tensor, er0: torch.Tensor, se0: torch.Tensor,
                  mr: torch.Tensor, phase1_epochs: int = 50, lr: Sequence[float] = (0.2, 0.1, 1e-4),
                  loss_weight: float = 100.0, tv: bool = True, tv_weight: float = 0.01,
-                 tuning: Optional[dict] = None, graph: bool = False, checkpoint=None):
+                 tuning: Optional[dict] = None, graph=False, checkpoint=None, adam_capturable: bool = False):
         self.device = torch.device(device)
         kw = dict(kwargs)
         self.pml = int(kw.get("pmlthick", 0))
@@ -59,12 +70,20 @@ class Inversion:
         self.observed = observed.detach().to(self.device, torch.float32).contiguous()
         self.loss_weight = float(loss_weight)
         self.phase1_epochs = int(phase1_epochs)
-        self.opt1 = torch.optim.Adam([{"params": self.er, "lr": lr[0]}])
-        self.opt2 = torch.optim.Adam([{"params": self.er, "lr": lr[1]}, {"params": self.se, "lr": lr[2]}])
+        if graph not in (False, True, "epoch"):
+            raise ValueError("graph must be False, True or 'epoch'")
+        self.graph_epoch = graph == "epoch"
+        cap = bool(adam_capturable) or self.graph_epoch
+        self.opt1 = torch.optim.Adam([{"params": self.er, "lr": lr[0]}], capturable=cap)
+        self.opt2 = torch.optim.Adam([{"params": self.er, "lr": lr[1]}, {"params": self.se, "lr": lr[2]}],
+                                     capturable=cap)
         self.kw = kw
         self.solve_args = dict(tuning=tuning, tv=tv, tv_weight=tv_weight, checkpoint=checkpoint)
-        self.use_graph = bool(graph)
+        self.use_graph = graph is True
         self._graph = None
+        self._plan_gen = 0         # plans built so far
+        self._egraph = {}          # phase (False/True) -> the whole epoch captured (graph='epoch')
+        self._loss = torch.zeros((), dtype=torch.float32, device=self.device)
         self._row0 = None
         self._plan_for(torch.clamp(self.er.detach(), min=1))
         setup = self.setup
@@ -77,20 +96,30 @@ class Inversion:
         self.epochs = 0
 
     def _plan_for(self, er_c: torch.Tensor) -> None:
-        """(Re)build the set-up and plan when the profile's input (row 0 of the
-        clamped eps_r) differs from the one the current plan was built on."""
+        """Keep the set-up and plan in step with the model: the CPML profile
+        is the one part that depends on it (HORIPML averages row 0 of the
+        clamped eps_r).  When row 0 changes, the new set-up's profile is
+        written into the existing plan (fg_plan_set_profile): its tables,
+        buffers and captured graphs stay valid.  The first call builds it."""
         row0 = er_c[0].detach()
         if self._row0 is not None and torch.equal(row0, self._row0):
             return
         kw = self.kw
-        self.setup = build_setup(self.device, kw["dx"], kw["ny"], kw["nx"], kw.get("nz", 1), kw.get("time_windows"),
-                                 kw["source"], kw.get("source_location"), kw.get("source_step"),
-                                 kw.get("receiver_location"), kw.get("receiver_step"), kw.get("pmlthick", 0),
-                                 kw["source_apmlitudes"], kw["step"], er_c.detach(), self.mr, kw["nsrc"], kw["nrx"],
-                                 kw.get("dt"), kw.get("freq"), kw.get("total_step"), kw.get("Fixedreceiver", False),
-                                 kw.get("customsource"), kw.get("customreceiver"))
-        self.solve = Solve(self.device, self.setup, **self.solve_args)
+        setup = build_setup(self.device, kw["dx"], kw["ny"], kw["nx"], kw.get("nz", 1), kw.get("time_windows"),
+                            kw["source"], kw.get("source_location"), kw.get("source_step"),
+                            kw.get("receiver_location"), kw.get("receiver_step"), kw.get("pmlthick", 0),
+                            kw["source_apmlitudes"], kw["step"], er_c.detach(), self.mr, kw["nsrc"], kw["nrx"],
+                            kw.get("dt"), kw.get("freq"), kw.get("total_step"), kw.get("Fixedreceiver", False),
+                            kw.get("customsource"), kw.get("customreceiver"))
         self._row0 = row0.clone()
+        if self._plan_gen > 0:
+            if setup.profile is not None:
+                self.solve.plan.set_profile(setup.profile.packed())
+            self.setup = self.solve.setup = setup
+            return
+        self.setup = setup
+        self.solve = Solve(self.device, self.setup, **self.solve_args)
+        self._plan_gen += 1
         self._graph = None
         s, p = self.setup, self.solve.plan
         # static buffers of the solve (the graph's inputs and outputs)
@@ -145,9 +174,67 @@ class Inversion:
             self._graph = g
         self._graph.replay()
 
+    def _epoch_body(self, phase2: bool) -> None:
+        """The epoch of graph='epoch', without autograd: the clamps' backward
+        is where(m >= bound, g, 0), as torch's clamp backward forms it, and
+        the gradients are written into the parameters' .grad tensors."""
+        opt = self.opt2 if phase2 else self.opt1
+        er_c = torch.clamp(self.er.detach(), min=1)
+        se_c = torch.clamp(self.se.detach(), min=0)
+        e32, s32, _ = self.solve.materials(er_c, se_c, self.mr)
+        self._e32.copy_(e32)
+        self._s32.copy_(s32)
+        self._solve_into_static()
+        self._loss.copy_((self._traces - self.observed).abs().mean() * self.loss_weight)
+        zero = torch.zeros((), dtype=torch.float32, device=self.device)
+        p = self.pml
+        pairs = [(self.er, er_c, self._ge, 1)] + ([(self.se, se_c, self._gs, 0)] if phase2 else [])
+        for param, m_c, g_static, bound in pairs:
+            g = g_static.view(m_c.shape)
+            if self.solve.tv:
+                tv = total_variation(m_c.clone(), capturable=True)
+                g = g + self.solve.tv_weight * (2 * (m_c - tv))
+            g = torch.where(param.detach() >= bound, g, zero)
+            if p > 0:
+                g[:, :p, :] = 0
+                g[:, -p:, :] = 0
+            param.grad.copy_(g)
+        opt.step()
+
+    def _epoch_graphed(self) -> float:
+        """graph='epoch': the first epoch of each phase (and the first after a
+        plan rebuild) runs eagerly and is then captured; later epochs replay
+        the capture.  Only the loss and row 0 of eps_r come back to the host."""
+        phase2 = self.epochs >= self.phase1_epochs
+        gen = self._plan_gen
+        self._plan_for(torch.clamp(self.er.detach(), min=1))
+        if self._plan_gen != gen:
+            self._egraph = {}                      # new static buffers: capture again
+        for param in (self.er, self.se):
+            if param.grad is None:
+                param.grad = torch.zeros_like(param)
+        g = self._egraph.get(phase2)
+        if g is None:
+            cur = torch.cuda.current_stream(self.device)
+            side = torch.cuda.Stream(self.device)
+            side.wait_stream(cur)
+            with torch.cuda.stream(side):
+                self._epoch_body(phase2)           # this epoch, eagerly (creates the optimiser state)
+            cur.wait_stream(side)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._epoch_body(phase2)           # recorded, not run
+            self._egraph[phase2] = g
+        else:
+            g.replay()
+        self.epochs += 1
+        return float(self._loss)
+
     def epoch(self) -> float:
         """One epoch: forward, loss, fused adjoint, border zeroing, Adam step.
         Returns the loss (L1 mean times the weight)."""
+        if self.graph_epoch:
+            return self._epoch_graphed()
         phase2 = self.epochs >= self.phase1_epochs
         opt = self.opt2 if phase2 else self.opt1
         opt.zero_grad()

@@ -12,16 +12,30 @@ while others are on the GPU overlap with them on the device.  Every result
 is computed by the same kernels in the same order as the request alone, so
 it is the same alone and in the mix, bit for bit.
 
+Forward requests that share a survey -- the same merge_key, grid, time
+axis, source waveform, receiver count and model -- are merged when admitted
+into one solve over all their shots (up to MERGE_SHOTS), so a few requests
+of a few shots each fill the 32 shot lanes of a warp together instead of
+one partly filled solve each; each request gets its own shots' traces, the
+bits it gets alone (a shot's result does not depend on the shots beside
+it).  Gradient requests are not merged: the imaging sums add the shots of
+a shot group together, and a request's gradient must hold its own shots
+only.
+
+Throughput counts a request's nx * ny * shots * nt cell-steps once, forward
+or gradient (a forward + adjoint pair counted once, the benchmark's unit).
+
 The reference has no serving path: one compute() call at a time, each
 rebuilding its grid.
 """
 from __future__ import annotations
 
 import concurrent.futures as cf
+import dataclasses
 import threading
 import time
-from dataclasses import dataclass
-from typing import Optional
+from dataclasses import dataclass, field
+from typing import Hashable, List, Optional
 
 import numpy as np
 import torch
@@ -41,6 +55,7 @@ class Request:
     mr: torch.Tensor
     resid: Optional[torch.Tensor] = None
     tuning: Optional[dict] = None
+    merge_key: Optional[Hashable] = None   # forward requests of one survey: may share a solve
 
 
 @dataclass
@@ -68,6 +83,32 @@ class _Job:
     solve: Optional[Solve] = None
     need: int = 0
     interval: Optional[int] = None
+    members: List["_Job"] = field(default_factory=list)   # a merged solve: its requests, in shot order
+
+
+MERGE_SHOTS = 64   # shots of one merged forward solve at most (two groups of 32 shot lanes)
+
+
+def _mergeable(a: "_Job", b: "_Job") -> bool:
+    """Two forward requests that may share one solve: same survey key, grid,
+    time axis, waveform, receivers and model (checked, not assumed)."""
+    ra, rb = a.req, b.req
+    if ra.resid is not None or rb.resid is not None or ra.merge_key is None or ra.merge_key != rb.merge_key:
+        return False
+    if ra.tuning != rb.tuning:
+        return False
+    sa, sb = a.solve.setup, b.solve.setup
+    if (sa.nx, sa.ny, sa.nt, sa.th, sa.dx, sa.dt32) != (sb.nx, sb.ny, sb.nt, sb.th, sb.dx, sb.dt32):
+        return False
+    if sa.src.shape[1:] != sb.src.shape[1:] or sa.rx.shape[1:] != sb.rx.shape[1:]:
+        return False
+    if not np.array_equal(sa.srcw, sb.srcw):
+        return False
+    if (sa.profile is None) != (sb.profile is None) or (
+            sa.profile is not None and not np.array_equal(sa.profile.packed(), sb.profile.packed())):
+        return False
+    return all(torch.equal(torch.as_tensor(x), torch.as_tensor(y)) for x, y in ((ra.er, rb.er), (ra.se, rb.se),
+                                                                               (ra.mr, rb.mr)))
 
 
 def _setup(device, req: Request):
@@ -108,6 +149,7 @@ class Server:
         self._pool = cf.ThreadPoolExecutor(max_workers=self.max_active)
         self._closed = False
         self.results: list = []
+        self.merged = 0     # requests served by a merged forward solve
 
     # -- admission ----------------------------------------------------------
     def _plan(self, job: _Job) -> None:
@@ -143,10 +185,36 @@ class Server:
             self._admit_locked()
         return job.fut
 
+    def _merge_locked(self, job: _Job) -> _Job:
+        """A forward job with the queued forward jobs of its survey, as one
+        solve over all their shots (the job itself when there is none, or
+        when the merged solve would not fit)."""
+        if job.req.resid is not None or job.req.merge_key is None:
+            return job
+        members, shots = [job], job.solve.setup.shots
+        for other in list(self._queue):
+            if shots + other.solve.setup.shots <= MERGE_SHOTS and _mergeable(job, other):
+                members.append(other)
+                shots += other.solve.setup.shots
+        if len(members) == 1:
+            return job
+        s0 = job.solve.setup
+        setup = dataclasses.replace(s0, shots=shots, src=torch.cat([m.solve.setup.src for m in members]),
+                                    rx=torch.cat([m.solve.setup.rx for m in members]))
+        solve = Solve(self.device, setup, tuning=job.req.tuning, tv=False, bind=False)
+        p = solve.plan
+        need = p.workspace_bytes + 4 * shots * setup.nt * p.nrx
+        if self.used + need > self.budget:
+            return job
+        for m in members[1:]:
+            self._queue.remove(m)
+        merged = _Job(job.req, cf.Future(), job.submitted, solve, need, None, members)
+        return merged
+
     def _admit_locked(self) -> None:
         # first come, first served; a request waits until its bytes fit
         while self._queue and self.active < self.max_active and self.used + self._queue[0].need <= self.budget:
-            job = self._queue.pop(0)
+            job = self._merge_locked(self._queue.pop(0))
             self.used += job.need
             self.active += 1
             self.peak_active = max(self.peak_active, self.active)
@@ -167,13 +235,29 @@ class Server:
             with torch.cuda.device(self.device), torch.cuda.stream(stream):
                 res = self._solve(job)
                 stream.synchronize()
-            res.submitted, res.started, res.finished = job.submitted, started, time.perf_counter()
+            finished = time.perf_counter()
             job.solve = None
+            if job.members:
+                # a merged forward: each request takes its own shots' traces
+                out, o = [], 0
+                for m in job.members:
+                    S = m.solve.setup.shots
+                    r = dataclasses.replace(res, traces=res.traces[o:o + S].clone(),
+                                            cell_steps=res.cell_steps // res.traces.shape[0] * S)
+                    o += S
+                    r.submitted, r.started, r.finished = m.submitted, started, finished
+                    out.append((m, r))
+            else:
+                res.submitted, res.started, res.finished = job.submitted, started, finished
+                out = [(job, res)]
             with self._lock:
-                self.results.append(res)
-            job.fut.set_result(res)
-        except Exception as e:   # delivered to the caller through the future
-            job.fut.set_exception(e)
+                self.results.extend(r for _, r in out)
+                self.merged += len(job.members)
+            for m, r in out:
+                m.fut.set_result(r)
+        except Exception as e:   # delivered to the caller(s) through the future(s)
+            for m in (job.members or [job]):
+                m.fut.set_exception(e)
         finally:
             self._release(job)
 
@@ -203,7 +287,7 @@ class Server:
                 seg = p.new_segment(job.interval)
                 p.forward_checkpointed(er, se, mr, traces, ck, job.interval)
                 p.adjoint_reference_checkpointed(er, se, mr, ck, job.interval, seg, resid, ge, gs)
-        cells = s.nx * s.ny * S * nt * (2 if req.resid is not None else 1)
+        cells = s.nx * s.ny * S * nt
         return Result(traces, ge, gs, cells, job.need, job.interval)
 
     # -- reporting ----------------------------------------------------------
@@ -223,4 +307,4 @@ class Server:
         cells = sum(r.cell_steps for r in res)
         return {"requests": len(res), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
                 "throughput_gcs": cells / span / 1e9 if span > 0 else float("nan"),
-                "peak_active": self.peak_active}
+                "peak_active": self.peak_active, "merged": self.merged}

@@ -28,14 +28,17 @@ def _d(x: torch.Tensor, dim: int) -> torch.Tensor:
     return x - torch.roll(x, 1, dims=dim)
 
 
-def total_variation(data, lamda=0.02, rho=1.0, num_iter=500, tol=1e-5):
+def total_variation(data, lamda=0.02, rho=1.0, num_iter=500, tol=1e-5, capturable=False):
     """float32 CUDA models run the whole ADMM solve as one kernel
     (fg_total_variation, libfastgpr.so); other tensors (CPU, float64) take
-    the tensor arithmetic below, which is the reference's own."""
+    the tensor arithmetic below, which is the reference's own.
+    capturable=True (not in the reference): the kernel is only enqueued, with
+    no wait for its iteration count, so the call may be captured in a CUDA
+    graph."""
     data.squeeze_(-1)
     if data.is_cuda and data.dtype == torch.float32 and data.dim() == 2:
         from . import _native
-        out, _ = _native.total_variation(data, lamda, rho, num_iter, tol)
+        out, _ = _native.total_variation(data, lamda, rho, num_iter, tol, wait=not capturable)
         return out.unsqueeze(-1)
     return _total_variation_tensor(data, lamda, rho, num_iter, tol)
 

@@ -25,7 +25,8 @@
  *     void*; NULL = legacy default stream) and returns an FG_* status.  The
  *     solves return without waiting; the calls that wait for their stream are
  *     fg_plan_bind (the plan's tables must stay valid until uploaded),
- *     fg_total_variation (it returns the iteration count), fg_plan_check and
+ *     fg_total_variation with iters != NULL (it returns the iteration count),
+ *     fg_plan_check and
  *     fg_forward_static when it uploads a plan's tables (see there); the first
  *     bind of a cell size on a device also runs its division check and waits
  *     for it.  fg_last_error() gives the message of the most recent failure
@@ -206,6 +207,15 @@ int fg_adjoint_reference_l1(fg_plan* plan, const float* er, const float* se, con
 int fg_adjoint_exact(fg_plan* plan, const float* er, const float* se, const float* mr, const float* hist,
                      const float* weights, float* grad_eps, float* grad_sig, void* stream);
 
+/* Replace the CPML profile of a plan (and of its adjoint plan) -- the 8*th
+ * floats of fg_problem.pml, HOST -- keeping its tables, workspace and launch
+ * shape.  The profile is the only part of a plan that depends on the model
+ * (HORIPML averages the first row of eps_r, src/compute.py:267-313), so an
+ * inversion whose model changes keeps its plan, buffers and captured CUDA
+ * graphs.  A bound plan's copy in the workspace is updated on `stream`
+ * (pageable-memory copy: pml may be reused when the call returns). */
+int fg_plan_set_profile(fg_plan* p, const float* pml, void* stream);
+
 /* Several models in one launch: no counterpart in the reference, which
  * solves one model per call.  fg_forward_batch runs fg_forward for plans[0..n)
  * -- models of any grid, shot count and step count -- with every time step of
@@ -306,9 +316,10 @@ int fg_fir_causal(const float* x, int64_t batch, int32_t T, int32_t R, const flo
  * operations; the convergence norm is summed in float64.  data, out and
  * workspace are device memory (workspace: fg_tv_workspace_bytes(M, N) bytes,
  * 256-byte aligned, not overlapping data or out).  One cooperative launch on
- * `stream`, then a synchronisation of `stream`: *iters (host, may be NULL)
- * receives the iteration count.  Returns FG_ERR_TIMEOUT if a device-side
- * barrier gave up. */
+ * `stream`; with iters != NULL the call then waits for `stream`, *iters
+ * (host) receives the iteration count, and FG_ERR_TIMEOUT is returned if a
+ * device-side barrier gave up.  With iters == NULL the call only enqueues
+ * (it may be captured in a CUDA graph) and reports neither. */
 int64_t fg_tv_workspace_bytes(int32_t M, int32_t N);
 int fg_total_variation(const float* data, int32_t M, int32_t N, double lamda, double rho, int32_t num_iter,
                        double tol, float* out, void* workspace, int64_t bytes, int32_t* iters, void* stream);

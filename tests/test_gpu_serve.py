@@ -71,3 +71,49 @@ def test_budget_admission_and_checkpoint_fallback(fg):
     with pytest.raises(MemoryError):
         tiny.submit(grad).result()
     tiny.close()
+
+
+def _survey_requests(fg, serve, n=3, shots=(3, 5, 2)):
+    """Forward requests of one survey: same grid, model and waveform, each
+    with its own shot positions."""
+    out = []
+    for k in range(n):
+        wl = fg.workloads.small(seed=77, nx=64, ny=56, shots=shots[k], nt=110, pml=6, fixed=True)
+        wl.source_location = [0.3 + 0.6 + 0.2 * k, 0.25 + 0.3, 0.0]
+        wl.source_step = [0.05, 0.01, 0.0]
+        kw = wl.kwargs("cuda")
+        for key in ("er", "se", "mr", "device", "tv"):
+            kw.pop(key)
+        out.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), None,
+                                 merge_key="survey-77"))
+    return out
+
+
+def test_merged_forward_requests_equal_alone(fg):
+    """Forward requests of one survey queued behind a running request are
+    merged into one solve; each gets the traces it gets alone."""
+    serve, _ = _requests(fg)
+    survey = _survey_requests(fg, serve)
+    alone = []
+    for r in survey:
+        srv = serve.Server("cuda:0", max_active=1)
+        alone.append(srv.submit(r).result().traces.cpu().numpy())
+        srv.close()
+    big = fg.workloads.small(seed=5, nx=200, ny=200, shots=16, nt=2500, pml=10, fixed=True)
+    big.source_step = [0.05, 0.01, 0.0]
+    kw = big.kwargs("cuda")
+    for key in ("er", "se", "mr", "device", "tv"):
+        kw.pop(key)
+    hold = serve.Request(kw, torch.tensor(big.er), torch.tensor(big.se), torch.tensor(big.mr),
+                         torch.zeros((16, 2500, big.nrx)))
+    srv = serve.Server("cuda:0", max_active=1)
+    first = srv.submit(hold)                     # a gradient request holds the one slot for ~0.1 s
+    futs = [srv.submit(r) for r in survey]       # these queue up behind it and are merged
+    first.result()
+    got = [f.result() for f in futs]
+    st = srv.stats()
+    srv.close()
+    assert st["merged"] == len(survey)
+    for a, res in zip(alone, got):
+        assert res.traces.shape[0] == a.shape[0]
+        assert np.array_equal(a, res.traces.cpu().numpy())
