@@ -719,8 +719,8 @@ def serving_stream(fg, n=12, seed=4004):
     return serve, reqs
 
 
-def _serve_once(serve, dev, reqs, gaps, active):
-    srv = serve.Server(dev, max_active=active)
+def _serve_once(serve, dev, reqs, gaps, active, policy="sjf", merge=True):
+    srv = serve.Server(dev, max_active=active, policy=policy, merge=merge)
     futs = []
     for r, gap in zip(reqs, gaps):
         time.sleep(float(gap))
@@ -736,23 +736,24 @@ def _serve_once(serve, dev, reqs, gaps, active):
 
 def run_serving(fg, dev, rates_x=(0.5, 1.0, 2.0)):
     """The stream at Poisson rates swept across saturation, served with
-    continuous batching (4 requests on the GPU at once, forward requests of
-    one survey merged), against the plain one-request-at-a-time path at the
-    highest rate.  The saturation rate is measured first: requests per second
+    continuous batching (up to 4 requests on the GPU at once, a GPU-filling
+    request alone, forward requests of one survey merged, shortest job first
+    with a 2 s bound on waiting), against the plain one-request-at-a-time
+    path (first come, first served, no merging) at the highest rate.  The saturation rate is measured first: requests per second
     of the one-at-a-time path with all requests queued at once."""
     serve, reqs = serving_stream(fg)
     warm = serve.Server(dev, max_active=1)
     warm.submit(reqs[0]).result()                 # plans, kernels, allocator
     warm.close()
     t0 = time.perf_counter()
-    base = _serve_once(serve, dev, reqs, np.zeros(len(reqs)), 1)
+    base = _serve_once(serve, dev, reqs, np.zeros(len(reqs)), 1, "fifo", False)
     sat = len(reqs) / (time.perf_counter() - t0)
     rates = []
     for x in rates_x:
         gaps = np.random.default_rng(7).exponential(1.0 / (x * sat), size=len(reqs))
         rates.append(dict(rate_hz=round(x * sat, 3), **_serve_once(serve, dev, reqs, gaps, 4)))
     top = np.random.default_rng(7).exponential(1.0 / (rates_x[-1] * sat), size=len(reqs))
-    one = dict(rate_hz=round(rates_x[-1] * sat, 3), **_serve_once(serve, dev, reqs, top, 1))
+    one = dict(rate_hz=round(rates_x[-1] * sat, 3), **_serve_once(serve, dev, reqs, top, 1, "fifo", False))
     torch.cuda.empty_cache()
     return {"requests": len(reqs), "saturation_hz": round(sat, 3), "all_queued_one_at_a_time": base,
             "rates": rates, "one_at_a_time": one,

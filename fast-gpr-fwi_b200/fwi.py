@@ -24,9 +24,10 @@ solve, loss, the TV kernel, the clamps' backward, border zeroing and the
 Adam step (capturable Adam) -- and replays it; only the loss and row 0 of
 eps_r (to see whether the CPML profile changed; when it did, the new profile
 is uploaded before the replay) come back to the host.  It
-computes the bits of the eager epoch with adam_capturable=True (capturable
-Adam rounds its bias corrections on the device, so it can differ from the
-default Adam in the last ulp).
+computes the bits of the eager epoch with adam_capturable=True.  Capturable
+Adam keeps its step count on the device and arranges the bias corrections
+and eps differently from the default Adam, so cells whose gradient is near
+eps move differently from the notebook's loop.
 
 graph=True captures an epoch's solve -- the coefficient kernels, state
 resets, 2 nt - 1 step launches and the gradient reductions -- in a CUDA graph

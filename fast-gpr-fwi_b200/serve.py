@@ -8,7 +8,9 @@ whole Ez history or, when that does not fit, checkpoints plus one history
 segment (the checkpointed solve, bit-identical results).  Admitted requests
 run side by side, each on a CUDA stream of its own driven by a worker
 thread (the library's launches release the GIL), so requests that arrive
-while others are on the GPU overlap with them on the device.  Every result
+while others are on the GPU overlap with them on the device -- except a
+request whose steps fill the GPU on their own (EXCLUSIVE_WORK), which runs
+alone: side by side such solves only share the SMs and the L2.  Every result
 is computed by the same kernels in the same order as the request alone, so
 it is the same alone and in the mix, bit for bit.
 
@@ -84,9 +86,25 @@ class _Job:
     need: int = 0
     interval: Optional[int] = None
     members: List["_Job"] = field(default_factory=list)   # a merged solve: its requests, in shot order
+    slots: int = 0
+    work: float = 0.0     # cell-steps the job costs (a gradient 2.5 times its forward)
 
 
 MERGE_SHOTS = 64   # shots of one merged forward solve at most (two groups of 32 shot lanes)
+
+# A solve whose step holds at least this many cells x shot groups keeps the
+# whole GPU busy on its own (its persistent launches span every SM), and two
+# of them side by side only share the SMs and the L2 (measured: a stream of
+# such requests ran at 30 Gcell-steps/s four at a time against 36 one at a
+# time).  Such a request runs alone; smaller ones share the GPU.
+EXCLUSIVE_WORK = 150_000
+
+
+def _weight(job: "_Job", max_active: int) -> int:
+    """Slots a job takes: all of them for a step that fills the GPU, else one."""
+    s = job.solve.setup
+    groups = (s.shots + 31) // 32 if s.shots >= 8 else s.shots
+    return max_active if s.nx * s.ny * groups >= EXCLUSIVE_WORK else 1
 
 
 def _mergeable(a: "_Job", b: "_Job") -> bool:
@@ -132,9 +150,19 @@ class Server:
 
     hbm_budget: bytes the server may hold on the device (default: 90% of the
     free memory when the server starts); max_active: requests on the GPU at
-    once (streams / worker threads)."""
+    once (streams / worker threads); policy: which queued request goes next --
+    'sjf' the one with the least work (nx * ny * shots * nt, a gradient
+    counted 2.5 times: forward, recomputed or stored history, adjoint),
+    unless the oldest has waited max_wait seconds, then the oldest; 'fifo'
+    the oldest; merge: merge queued forward requests of one survey."""
 
-    def __init__(self, device="cuda:0", hbm_budget: Optional[int] = None, max_active: int = 4):
+    def __init__(self, device="cuda:0", hbm_budget: Optional[int] = None, max_active: int = 4,
+                 policy: str = "sjf", max_wait: float = 2.0, merge: bool = True):
+        if policy not in ("sjf", "fifo"):
+            raise ValueError("policy must be 'sjf' or 'fifo'")
+        self.policy = policy
+        self.max_wait = float(max_wait)
+        self.merge = bool(merge)
         self.device = torch.device(device)
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -143,6 +171,7 @@ class Server:
         self.used = 0
         self.max_active = int(max_active)
         self.active = 0
+        self.slots = 0      # slots taken by the running jobs (_weight)
         self.peak_active = 0
         self._queue: list = []
         self._lock = threading.Condition()
@@ -170,6 +199,7 @@ class Server:
             full = fixed                            # a forward alone keeps no history
         job.solve = solve
         job.need = full
+        job.work = setup.nx * setup.ny * S * nt * (2.5 if req.resid is not None else 1.0)
 
     def submit(self, req: Request) -> cf.Future:
         """Queue a request; the future resolves to a Result."""
@@ -189,7 +219,7 @@ class Server:
         """A forward job with the queued forward jobs of its survey, as one
         solve over all their shots (the job itself when there is none, or
         when the merged solve would not fit)."""
-        if job.req.resid is not None or job.req.merge_key is None:
+        if not self.merge or job.req.resid is not None or job.req.merge_key is None:
             return job
         members, shots = [job], job.solve.setup.shots
         for other in list(self._queue):
@@ -204,17 +234,29 @@ class Server:
         solve = Solve(self.device, setup, tuning=job.req.tuning, tv=False, bind=False)
         p = solve.plan
         need = p.workspace_bytes + 4 * shots * setup.nt * p.nrx
-        if self.used + need > self.budget:
+        merged = _Job(job.req, cf.Future(), job.submitted, solve, need, None, members)
+        if self.used + need > self.budget or self.slots + _weight(merged, self.max_active) > self.max_active:
             return job
         for m in members[1:]:
             self._queue.remove(m)
-        merged = _Job(job.req, cf.Future(), job.submitted, solve, need, None, members)
         return merged
 
+    def _next_locked(self) -> int:
+        """Index of the queued job that goes next (policy)."""
+        if self.policy == "fifo" or time.perf_counter() - self._queue[0].submitted > self.max_wait:
+            return 0
+        return min(range(len(self._queue)), key=lambda i: self._queue[i].work)
+
     def _admit_locked(self) -> None:
-        # first come, first served; a request waits until its bytes fit
-        while self._queue and self.active < self.max_active and self.used + self._queue[0].need <= self.budget:
-            job = self._merge_locked(self._queue.pop(0))
+        # the next job (policy) waits until its bytes and its slots fit
+        while self._queue:
+            i = self._next_locked()
+            nxt = self._queue[i]
+            if self.slots + _weight(nxt, self.max_active) > self.max_active or self.used + nxt.need > self.budget:
+                break
+            job = self._merge_locked(self._queue.pop(i))
+            job.slots = _weight(job, self.max_active)
+            self.slots += job.slots
             self.used += job.need
             self.active += 1
             self.peak_active = max(self.peak_active, self.active)
@@ -223,6 +265,7 @@ class Server:
     def _release(self, job: _Job) -> None:
         with self._lock:
             self.used -= job.need
+            self.slots -= job.slots
             self.active -= 1
             self._admit_locked()
             self._lock.notify_all()
