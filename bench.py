@@ -129,6 +129,9 @@ def kernel_name(tuning, direction, split=False):
     (split: the interior tiles run in a kernel of their own beside it)."""
     t = tuning or {}
     if split:
+        if direction == "forward" and t.get("slab", 0) != -1:
+            return ("fg::k_fwd + fg::k_fwd_slab + fg::k_fwd_core (lane march on the tiles with events or in two "
+                    "slabs, slab kernel on the CPML slabs, interior kernel, forward step)")
         d = "fwd" if direction == "forward" else "adj"
         return "fg::k_%s + fg::k_%s_core (lane march on the boundary tiles beside the interior kernel, %s step)" % (
             d, d, direction)

@@ -55,12 +55,12 @@ class FgTuning(ctypes.Structure):
         ("adj_kernel", ctypes.c_int32), ("adj_rows_per_tile", ctypes.c_int32),
         ("adj_warps_per_block", ctypes.c_int32), ("adj_stages", ctypes.c_int32),
         ("adj_cells_per_thread", ctypes.c_int32), ("prefetch", ctypes.c_int32), ("interior", ctypes.c_int32),
-        ("persistent", ctypes.c_int32),
+        ("persistent", ctypes.c_int32), ("slab", ctypes.c_int32),
     ]
 
     KEYS = ("lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages", "kernel",
             "adj_kernel", "adj_rows_per_tile", "adj_warps_per_block", "adj_stages", "adj_cells_per_thread",
-            "prefetch", "interior", "persistent")
+            "prefetch", "interior", "persistent", "slab")
 
 
 class FastGprError(RuntimeError):

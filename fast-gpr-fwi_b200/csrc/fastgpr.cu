@@ -159,11 +159,39 @@ void build_tiles(fg_plan* p) {
                                p->inj_off[t + 1] == p->inj_off[t];
             return rows && cols && quiet;
         };
+        // slab tiles (split plans with shot lanes): no event, and either the
+        // interior's columns with rows touching an x slab (x tiles) or the
+        // interior's rows with columns touching one y slab only, in the grid
+        // (y tiles); they run in the slab kernel, between the general tiles
+        // and the interior ones
+        const bool fast = th > 0 && 2 * th < p->nx && 2 * th < p->ny;
+        auto slab = [&](int t) -> int {
+            if (!p->slab_on || !fast || interior(t)) return 0;
+            const int band = t % p->nb, chunk = (t / p->nb) % p->nc;
+            const int i0 = p->chunk_row[chunk], i1 = p->chunk_row[chunk + 1];
+            const int j0 = band * p->BW, j1 = j0 + p->BW;
+            const bool quiet = p->src_off[t + 1] == p->src_off[t] && p->rx_off[t + 1] == p->rx_off[t] &&
+                               p->inj_off[t + 1] == p->inj_off[t];
+            if (!quiet) return 0;
+            const bool rows_in = i0 >= th + 1 && i1 <= p->nx - th - 1;
+            const bool cols_in = j0 >= th + 1 && j1 <= p->ny - th - 1;
+            if (cols_in) return 1;
+            // the forward's H cells start at j0-1, the adjoint's E cells end at j0+W
+            const bool one_side = !(j0 - 1 <= th && j1 >= p->ny - th);
+            if (rows_in && j1 <= p->ny && one_side) return 2;
+            return 0;
+        };
         p->order.clear();
         for (int t = 0; t < p->ntiles; ++t)
-            if (heavy(t) && !interior(t)) p->order.push_back(t);
+            if (heavy(t) && !interior(t) && !slab(t)) p->order.push_back(t);
         for (int t = 0; t < p->ntiles; ++t)
-            if (!heavy(t) && !interior(t)) p->order.push_back(t);
+            if (!heavy(t) && !interior(t) && !slab(t)) p->order.push_back(t);
+        p->slab0 = (int)p->order.size();
+        for (int t = 0; t < p->ntiles; ++t)
+            if (slab(t) == 1) p->order.push_back(t);
+        p->yslab0 = (int)p->order.size();
+        for (int t = 0; t < p->ntiles; ++t)
+            if (slab(t) == 2) p->order.push_back(t);
         p->core0 = (int)p->order.size();
         for (int t = 0; t < p->ntiles; ++t)
             if (interior(t)) p->order.push_back(t);
@@ -196,7 +224,7 @@ void layout(fg_plan* p) {
     p->o_chunk = take((p->nc + 1) * sizeof(int));
     p->o_order = take((size_t)p->ntiles * sizeof(int));
     p->o_tiles = take((size_t)p->ntiles * sizeof(int4));
-    p->o_ctr = take(4 * sizeof(int));
+    p->o_ctr = take(8 * sizeof(int));
     p->o_srcev = take(p->src_ev.size() * sizeof(Ev));
     p->o_rxev = take(p->rx_ev.size() * sizeof(Ev));
     p->o_injev = take(p->inj_ev.size() * sizeof(Ev));
@@ -244,6 +272,8 @@ void fill_grid(fg_plan* p) {
     g.fast_cpml = 2 * p->th < p->nx && 2 * p->th < p->ny;
     g.pf = p->pf;
     g.core0 = p->core0;
+    g.slab0 = p->slab0;
+    g.yslab0 = p->yslab0;
     g.src_ev = (const Ev*)(w + p->o_srcev);
     g.rx_ev = (const Ev*)(w + p->o_rxev);
     g.inj_ev = (const Ev*)(w + p->o_injev);
@@ -266,11 +296,11 @@ int coefficients(const float* er, const float* se, const float* mr, int nx, int 
     return FG_OK;
 }
 
-// Zero fields, auxiliaries and the two tile counters before a solve.
+// Zero fields, auxiliaries and the tile counters before a solve.
 int reset_state(fg_plan* p, cudaStream_t st) {
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_state, 0, p->state_bytes, st));
     FG_CUDA(cudaMemsetAsync(p->ws + p->o_psi, 0, p->psi_bytes, st));
-    FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 4 * sizeof(int), st));
+    FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 8 * sizeof(int), st));
     return FG_OK;
 }
 
@@ -659,6 +689,22 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // kernel is fastest beside the interior kernel with 3 blocks per SM (the
     // adjoint's, on its own plan, with 4; fg_plan_create passes that)
     p->split_bpsm = interior > 0 ? interior : 3;
+    const int slab = tune ? tune->slab : 0;
+    if (slab < -1 || slab > 8) {
+        delete p;
+        return fail(FG_ERR_INVALID, "unsupported tuning: slab must be -1 .. 8");
+    }
+    // measured on the 64-shot 440 x 340 benchmark grid (us per step): the
+    // forward's slab kernel at 2 blocks per SM beside the others 68.1 against
+    // 75.3 without it (1: 88.9, 3: 77.7, as many as fit: 83.9); the
+    // adjoint's (8 cells per thread, 168 registers) 109.3 against 98.5
+    // without it, so fg_plan_create leaves it off for the adjoint plan
+    p->slab_on = p->split && slab != -1;
+    p->slab_bpsm = slab > 0 ? slab : 2;
+    // beside the interior kernel the general kernel's next-tile prefetch only
+    // competes for bandwidth (measured on that grid: forward 74.0 against
+    // 78.1 us, adjoint 99.2 against 101.9 us without it): off unless asked for
+    if (p->split && pf == 0) p->pf = 0;
     p->persist = p->kernel == 1 && p->D == 0 && !p->pair && !p->split && persistent == 1;
     if (p->kernel == 1 && fg::prof_bytes(p->th) + plan_ring_smem(p) > 227 * 1024) {
         delete p;
@@ -720,6 +766,8 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     at.prefetch = tune ? tune->prefetch : 0;
     at.interior = tune ? tune->interior : 0;
     at.persistent = tune ? tune->persistent : 0;
+    // the adjoint's slab kernel only when asked for (measured slower)
+    at.slab = tune && tune->slab ? tune->slab : -1;
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {
@@ -902,7 +950,7 @@ cudaError_t split_blocks(const fg_plan* p, int* blocks) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    const int need = (p->core0 + p->WPB - 1) / p->WPB;
+    const int need = (p->slab0 + p->WPB - 1) / p->WPB;
     *blocks = std::max(1, std::min(need, p->split_bpsm * sms));
     return cudaSuccess;
 }
@@ -952,16 +1000,19 @@ int fwd_steps(fg_plan* p, const Dev& g, int t0, int t1, cudaStream_t st) {
     } else if (p->persist) {
         FG_CUDA(multi_fwd(&p, &g, 1, t0, t1, st));
     } else if (p->split) {
-        // the general lane march on the tiles before core0, the interior kernel on the rest
-        FwdFn fn = pick_fwd(p->shot, p->W), fc = pick_fwd_core(p->W);
-        if (!fn || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        // the general lane march on the tiles before slab0, the slab kernel on
+        // [slab0, core0), the interior kernel on the rest; each behind the one
+        // before with programmatic dependent launch
+        FwdFn fn = pick_fwd(p->shot, p->W), fs = pick_fwd_slab(p->W), fc = pick_fwd_core(p->W);
+        if (!fn || !fs || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         Dev gb = g;
-        gb.ntiles = p->core0;
-        if (p->core0 > 0 && p->fwd_blocks == 0) FG_CUDA(split_blocks(p, &p->fwd_blocks));
-        const int pdl = p->core0 > 0;
+        gb.ntiles = p->slab0;
+        if (p->slab0 > 0 && p->fwd_blocks == 0) FG_CUDA(split_blocks(p, &p->fwd_blocks));
+        const bool gen = p->slab0 > 0, slab = p->core0 > p->slab0, core = p->core0 < p->ntiles;
         for (int t = t0; t < t1; ++t) {
-            if (p->core0 > 0) FG_CUDA(fn(gb, t, p->WPB, p->D, &p->fwd_blocks, st));
-            if (p->core0 < p->ntiles) FG_CUDA(fc(g, t, 4, pdl, &p->fwd_core_blocks, st));
+            if (gen) FG_CUDA(fn(gb, t, p->WPB, p->D, &p->fwd_blocks, st));
+            if (slab) FG_CUDA(fs(g, t, p->slab_bpsm, gen, &p->fwd_slab_blocks, st));
+            if (core) FG_CUDA(fc(g, t, 4, gen || slab, &p->fwd_core_blocks, st));
         }
     } else {
         FwdFn fn = p->pair ? pick_fwd2(p->W) : pick_fwd(p->shot, p->W);
@@ -989,16 +1040,17 @@ int adj_steps(fg_plan* a, const Dev& g, int hi, int lo, int nsteps, cudaStream_t
     } else if (a->persist) {
         FG_CUDA(multi_adj(&a, &g, 1, a->nt - 1 - hi, a->nt - lo, st));
     } else if (a->split) {
-        AdjFn fn = pick_adj(a->shot, a->W), fc = pick_adj_core(a->W);
-        if (!fn || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
+        AdjFn fn = pick_adj(a->shot, a->W), fs = pick_adj_slab(a->W), fc = pick_adj_core(a->W);
+        if (!fn || !fs || !fc) return fail(FG_ERR_INVALID, "no kernel for this tuning");
         Dev gb = g;
-        gb.ntiles = a->core0;
-        if (a->core0 > 0 && a->adj_blocks == 0) FG_CUDA(split_blocks(a, &a->adj_blocks));
-        const int pdl = a->core0 > 0;
+        gb.ntiles = a->slab0;
+        if (a->slab0 > 0 && a->adj_blocks == 0) FG_CUDA(split_blocks(a, &a->adj_blocks));
+        const bool gen = a->slab0 > 0, slab = a->core0 > a->slab0, core = a->core0 < a->ntiles;
         for (int it = hi; it >= lo; --it) {
             const int rp = (a->nt - 1 - it) & 1;
-            if (a->core0 > 0) FG_CUDA(fn(gb, it, rp, a->WPB, a->D, &a->adj_blocks, st));
-            if (a->core0 < a->ntiles) FG_CUDA(fc(g, it, rp, 4, pdl, &a->adj_core_blocks, st));
+            if (gen) FG_CUDA(fn(gb, it, rp, a->WPB, a->D, &a->adj_blocks, st));
+            if (slab) FG_CUDA(fs(g, it, rp, a->slab_bpsm, gen, &a->adj_slab_blocks, st));
+            if (core) FG_CUDA(fc(g, it, rp, 4, gen || slab, &a->adj_core_blocks, st));
         }
     } else {
         AdjFn fn = a->pair ? pick_adj2(a->W) : pick_adj(a->shot, a->W);
@@ -1324,7 +1376,7 @@ int fg_adjoint_reference_checkpointed(fg_plan* p, const float* er, const float* 
             if ((rc = reset_state(p, st))) return rc;
         } else {
             if ((rc = checkpoint_copy(p, s0 & 1, (float*)ckpt + (size_t)(c - 1) * cf, false, st))) return rc;
-            FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 4 * sizeof(int), st));
+            FG_CUDA(cudaMemsetAsync(p->ws + p->o_ctr, 0, 8 * sizeof(int), st));
         }
         gf.hist_t0 = s0;
         if ((rc = fwd_steps(p, gf, s0, s1, st))) return rc;

@@ -43,6 +43,11 @@ struct fg_plan {
     int pf = 0;         // next-tile L2 prefetch of the lane march (Dev::pf)
     bool split = false; // interior tiles (positions >= core0) run in the lean interior kernels
     int core0 = 0;      // first fetch position of an interior tile (== ntiles when none)
+    int slab0 = 0;      // first fetch position of a slab tile: x tiles [slab0, yslab0), y tiles [yslab0, core0)
+    int yslab0 = 0;
+    int fwd_slab_blocks = 0, adj_slab_blocks = 0;
+    bool slab_on = false; // slab tiles in the slab kernel (else in the general kernel)
+    int slab_bpsm = 0;    // slab kernel blocks per SM at most (0 = as many as fit)
     int split_bpsm = 2; // blocks per SM of the general kernel's launch beside the interior kernel
     bool persist = false;   // whole solves in one persistent cooperative launch (small grids)
     // tensor maps of the tile kernels (encoded when a workspace is bound)
@@ -133,6 +138,8 @@ FwdTileFn pick_fwd_tile(bool shot, int W);
 AdjTileFn pick_adj_tile(bool shot, int W);
 FwdFn pick_fwd_core(int W);              // interior tiles of the lane march, forward
 AdjFn pick_adj_core(int W);              // interior tiles of the lane march, adjoint
+FwdFn pick_fwd_slab(int W);              // slab tiles of the lane march, forward
+AdjFn pick_adj_slab(int W);              // slab tiles of the lane march, adjoint
 FwdFn pick_fwd_band(int W, int C);       // band pipeline (C consumer warps), forward
 AdjFn pick_adj_band(int W, int C);       // band pipeline, adjoint
 // Shared memory of a band-pipeline CTA (0: no kernel of that shape).

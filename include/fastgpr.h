@@ -108,8 +108,9 @@ typedef struct fg_tuning {
     /* Lane march with shot lanes and no stages (forward and adjoint): each
      * warp prefetches into L2 the rows of the tile it will take next, so the
      * loads of that tile find their lines in L2 instead of waiting for HBM.
-     * 0 = default (1), -1 = off, 1 = when the warp starts its current tile,
-     * 2 = at the current tile's middle row. */
+     * 0 = default (1; off where the interior split runs, beside which it
+     * only competes for bandwidth), -1 = off, 1 = when the warp starts its
+     * current tile, 2 = at the current tile's middle row. */
     int32_t prefetch;
     /* Lane march with shot lanes and no stages: the interior tiles (no CPML
      * cell in the tile or its halo, no source, receiver or injection) run in
@@ -128,6 +129,12 @@ typedef struct fg_tuning {
      * is no faster than a launch per step; several models in one launch
      * (fg_forward_batch) fill the GPU better than one. */
     int32_t persistent;
+    /* With the interior split: the slab tiles (in one CPML slab, no event)
+     * run in a lean kernel of their own between the general and the interior
+     * kernel.  -1 = off (they stay in the general kernel); 0 = default (the
+     * forward's on with at most 2 blocks per SM, the adjoint's off); 1..8 =
+     * on for both, at most that many blocks per SM. */
+    int32_t slab;
 } fg_tuning;
 
 typedef struct fg_plan fg_plan;

@@ -34,6 +34,8 @@ TUNINGS = [
     {"lanes": 1, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 4, "persistent": 1},
     {"lanes": 1, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 2, "interior": 2},
     {"lanes": 2, "kernel": 1, "cells_per_thread": 4, "persistent": 1},
+    # the slab kernels of both solves, the frame rows and columns included
+    {"lanes": 1, "kernel": 1, "cells_per_thread": 4, "rows_per_tile": 3, "interior": 2, "slab": 2},
 ]
 
 

@@ -138,6 +138,11 @@ TUNINGS = [
     {"kernel": 1, "lanes": 1, "cells_per_thread": 2, "rows_per_tile": 3, "interior": 1, "prefetch": 2},
     {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 2, "interior": 2, "adj_kernel": 2,
      "adj_cells_per_thread": 4},
+    # the slab kernels (x-slab and y-slab tiles) for the forward and the adjoint, forced on small grids
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 4, "rows_per_tile": 4, "interior": 2, "slab": 1},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 8, "rows_per_tile": 3, "interior": 1, "slab": 3},
+    {"kernel": 1, "lanes": 1, "cells_per_thread": 2, "rows_per_tile": 2, "interior": 2, "slab": 2, "adj_kernel": 2,
+     "adj_cells_per_thread": 4},
     # shot pairs (two shots per lane)
     {"kernel": 1, "lanes": 3, "cells_per_thread": 2, "rows_per_tile": 4},
     {"kernel": 1, "lanes": 3, "cells_per_thread": 4, "rows_per_tile": 5},
