@@ -349,7 +349,7 @@ __device__ __forceinline__ void adj_h_slab(const Dev& g, const float* R, const B
 // Reference-mode adjoint iteration it on the slab tiles
 // ---------------------------------------------------------------------------
 template <int W>
-__global__ void __launch_bounds__(128, 3) k_adj_slab(const Dev g, const int it, const int rp) {
+__global__ void __launch_bounds__(128, 2) k_adj_slab(const Dev g, const int it, const int rp) {
     griddep_launch_dependents();
     extern __shared__ __align__(128) unsigned char smem[];
     const float* R = stage_profile(g, smem);
