@@ -25,7 +25,8 @@
 // launch_dependents); the interior kernel is launched behind it with
 // programmatic stream serialisation, runs beside it on the SMs it leaves
 // free, and waits for it (griddepcontrol wait) only before it completes, so
-// the next step, launched behind the interior kernel, starts after both.
+// the next step's general kernel, launched behind the interior kernel the same
+// way, waits for it (and so for both) before it touches the state.
 #pragma once
 
 #include "fdtd_common.cuh"
@@ -58,6 +59,8 @@ __device__ __forceinline__ CoreTile core_tile(const Dev& g, int pos) {
 // ---------------------------------------------------------------------------
 template <int W>
 __global__ void __launch_bounds__(128, core_min_blocks<W>()) k_fwd_core(const Dev g, const int t) {
+    // the next step's general kernel may launch now (it waits for this one)
+    griddep_launch_dependents();
     if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[2 + ((t + 1) & 1)] = 0;   // the next launch's counter
     int* ctr = g.tile_ctr + 2 + (t & 1);
     const int lane = threadIdx.x & 31;
@@ -136,6 +139,7 @@ __global__ void __launch_bounds__(128, core_min_blocks<W>()) k_fwd_core(const De
 // ---------------------------------------------------------------------------
 template <int W>
 __global__ void __launch_bounds__(128, core_min_blocks<W>()) k_adj_core(const Dev g, const int it, const int rp) {
+    griddep_launch_dependents();
     if (blockIdx.x == 0 && threadIdx.x == 0) g.tile_ctr[2 + (rp ^ 1)] = 0;   // the next launch's counter
     int* ctr = g.tile_ctr + 2 + rp;
     const int lane = threadIdx.x & 31;

@@ -668,13 +668,18 @@ __device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned 
 #undef FG_CELL
 }
 
+// Step kernels are launched with programmatic stream serialisation behind the
+// kernel before them (the last launch of the previous step, or any other
+// kernel), so their blocks take the SMs as that kernel's blocks leave: each
+// waits for it to complete (griddep_wait) before it touches anything the step
+// reads or writes, then lets the slab and interior kernels behind it start
+// (they read none of this launch's results; see fdtd_core.cuh).
 template <int W, bool SHOT, bool RING>
 __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
-    // an interior-tile kernel launched behind this one may start at once
-    // (it reads none of this launch's results; see fdtd_core.cuh)
-    griddep_launch_dependents();
     extern __shared__ __align__(128) unsigned char smem[];
-    const float* R = stage_profile(g, smem);
+    const float* R = stage_profile(g, smem);   // the profile is fixed for the solve
+    griddep_wait();
+    griddep_launch_dependents();
     // a stage of an earlier launch never landed: leave at once
     if (RING && *(volatile int*)g.err != 0) return;
     fwd_step<W, SHOT, RING>(g, R, smem, t, D);
@@ -1138,9 +1143,10 @@ __device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned 
 
 template <int W, bool SHOT, bool RING>
 __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
-    griddep_launch_dependents();
     extern __shared__ __align__(128) unsigned char smem[];
     const float* R = stage_profile(g, smem);
+    griddep_wait();   // as k_fwd
+    griddep_launch_dependents();
     if (RING && *(volatile int*)g.err != 0) return;
     adj_step<W, SHOT, RING>(g, R, smem, it, rp, D);
 }

@@ -96,6 +96,24 @@ inline cudaError_t allow_smem(K kernel, size_t bytes) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Launch `kernel` on `st` with programmatic stream serialisation behind the
+// kernel before it (the kernel waits for that one with griddepcontrol.wait
+// before it reads or writes any state).
+template <class K, class... A>
+inline cudaError_t launch_pdl(K kernel, int blocks, int threads, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Blocks of a persistent launch: as many as are resident on the device at
 // once, at most one warp per tile.
 template <class K>

@@ -12,8 +12,7 @@ cudaError_t launch_adj_k(const Dev& g, int it, int rp, int wpb, int D, int* bloc
         if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
         if (e != cudaSuccess) return e;
     }
-    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, it, rp, D);
-    return cudaSuccess;
+    return launch_pdl(kernel, *blocks, 32 * wpb, smem, st, g, it, rp, D);
 }
 template <int W, bool SHOT>
 cudaError_t launch_adj(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {

@@ -12,8 +12,7 @@ cudaError_t launch_fwd_k(const Dev& g, int t, int wpb, int D, int* blocks, cudaS
         if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
         if (e != cudaSuccess) return e;
     }
-    kernel<<<*blocks, 32 * wpb, smem, st>>>(g, t, D);
-    return cudaSuccess;
+    return launch_pdl(kernel, *blocks, 32 * wpb, smem, st, g, t, D);
 }
 template <int W, bool SHOT>
 cudaError_t launch_fwd(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
