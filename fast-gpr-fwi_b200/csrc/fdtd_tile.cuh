@@ -359,6 +359,11 @@ __global__ void __launch_bounds__(288) k_fwd_pipe(const Dev g, const __grid_cons
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
     float* Rp = reinterpret_cast<float*>(smem + M.prof);
     volatile int* flags = reinterpret_cast<volatile int*>(smem + M.flag);
+    // launched with programmatic stream serialisation behind the previous
+    // step: wait for it before anything of the solve is read, then let the
+    // next step's launch place its blocks as these leave
+    griddep_wait();
+    griddep_launch_dependents();
     if (abort_launch(g, flags)) return;
     if (threadIdx.x == 0) {
         flags[1] = 0;
@@ -662,6 +667,11 @@ __global__ void __launch_bounds__(288) k_adj_pipe(const Dev g, const __grid_cons
     uint64_t* empty = reinterpret_cast<uint64_t*>(smem + M.empty);
     float* Rp = reinterpret_cast<float*>(smem + M.prof);
     volatile int* flags = reinterpret_cast<volatile int*>(smem + M.flag);
+    // launched with programmatic stream serialisation behind the previous
+    // step: wait for it before anything of the solve is read, then let the
+    // next step's launch place its blocks as these leave
+    griddep_wait();
+    griddep_launch_dependents();
     if (abort_launch(g, flags)) return;
     if (threadIdx.x == 0) {
         flags[1] = 0;

@@ -11,8 +11,8 @@ cudaError_t launch_fwd_tile(fg_plan* p, const Dev& g, int t, cudaStream_t st) {
     const int threads = 32 * (p->WPB + 1);
     const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->fwd_blocks);
     if (e != cudaSuccess) return e;
-    kernel<<<p->fwd_blocks, threads, M.total, st>>>(g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t, p->D, p->TI);
-    return cudaSuccess;
+    return launch_pdl(kernel, p->fwd_blocks, threads, M.total, st, g, p->tm_fez, p->tm_fhx, p->tm_fhy, p->tm_co, t,
+                      p->D, p->TI);
 }
 template <int W, bool SHOT>
 cudaError_t launch_adj_tile(fg_plan* p, const Dev& g, const CUtensorMap& tmh, int it, int rp, cudaStream_t st) {
@@ -22,9 +22,8 @@ cudaError_t launch_adj_tile(fg_plan* p, const Dev& g, const CUtensorMap& tmh, in
     const int threads = 32 * (p->WPB + 1);
     const cudaError_t e = pipe_blocks(kernel, threads, M.total, p->ntiles, &p->adj_blocks);
     if (e != cudaSuccess) return e;
-    kernel<<<p->adj_blocks, threads, M.total, st>>>(g, p->tm_aez, p->tm_ahx, p->tm_ahy, p->tm_co, tmh, it, rp,
-                                                     p->D, p->TI);
-    return cudaSuccess;
+    return launch_pdl(kernel, p->adj_blocks, threads, M.total, st, g, p->tm_aez, p->tm_ahx, p->tm_ahy, p->tm_co, tmh,
+                      it, rp, p->D, p->TI);
 }
 FwdTileFn pick_fwd_tile(bool shot, int W) {
     if (shot) return W == 4 ? launch_fwd_tile<4, true> : W == 8 ? launch_fwd_tile<8, true> : nullptr;
