@@ -352,6 +352,14 @@ def run_ours(args, rank, local, world):
     split = (shot and t.get("interior", 0) != -1 and not t.get("stages") and t.get("kernel", 1) == 1
              and (t.get("interior", 0) > 0 or nx * ny * ((S + 31) // 32) >= 200000))
     kname = kernel_name(tuning, dom, split)
+    # this library's kernels per fwd + adj step: the forward's (general, slab,
+    # interior) per time step, the adjoint's (general, interior; slab when
+    # asked for) per iteration, two coefficient kernels, the imaging tail and
+    # three gradient reductions
+    slab = t.get("slab", 0)
+    fwd_k = (3 if slab != -1 else 2) if split else 1
+    adj_k = (3 if slab > 0 else 2) if split else 1
+    launches_per_step = fwd_k * nt + adj_k * (nt - 1) + 6
     ncu = next((v for k, v in NCU_BYTES_PER_SHOT_CELL_STEP.items() if kname.startswith(k)), None)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
@@ -409,7 +417,7 @@ def run_ours(args, rank, local, world):
                        "tuning": tuning or "default",
                        "parallelism": "replicas: shots per GPU, one all-reduce of the imaging sums" if world > 1
                        else "single GPU"},
-            "gpu_launches": int(args.steps * (2 * nt + 4)),
+            "gpu_launches": int(args.steps * launches_per_step),
             "roofline": roofline,
             "kernels": other,
             "clocks": clk,
