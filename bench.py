@@ -372,6 +372,37 @@ def run_ours(args, rank, local, world):
              "adjoint": {"launch_ms": round(adj_launch_ms, 5), "algorithmic_bytes_per_launch": int(adj_b),
                          "achieved_gbs": round(adj_b / (adj_launch_ms * 1e-3) / 1e9, 1),
                          "phase_ms": round(float(np.median(adj_ms)), 3)}}
+    # the same step captured once in a CUDA graph and replayed (the method of
+    # the batched-gradient workload): every launch of the fwd + adj step in one
+    # graph, programmatic dependencies included
+    graph = None
+    if world == 1 and not args.no_e2e:
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(stream)
+        with torch.cuda.stream(side):
+            one_step()
+        stream.wait_stream(side)
+        torch.cuda.synchronize(dev)
+        t_cap = time.perf_counter()
+        cg = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(cg):
+            one_step()
+        t_cap = time.perf_counter() - t_cap
+        cg.replay()
+        torch.cuda.synchronize(dev)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(2):
+            cg.replay()
+        g1.record(stream)
+        torch.cuda.synchronize(dev)
+        plan.device_check()
+        gms = g0.elapsed_time(g1) / 2
+        graph = {"value": round(cell_steps / (gms * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_step": round(gms, 3),
+                 "replays": 2, "capture_s": round(t_cap, 2),
+                 "launches_per_step": int(launches_per_step)}
+        del cg
     del hist, traces
     torch.cuda.empty_cache()
 
@@ -422,6 +453,7 @@ def run_ours(args, rank, local, world):
             "kernels": other,
             "clocks": clk,
             "e2e": e2e,
+            "graph_replay": graph,
             "per_shot_path": per_shot,
             "small_configs": small,
             "checkpointed": ckpt,
