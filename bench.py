@@ -65,6 +65,7 @@ UNIT = "Gcell-steps/s"
 # 64-shot 440x340 workload, per shot and cell; a split step adds its two
 # kernels (boundary lane march + interior kernel)
 NCU_BYTES_PER_SHOT_CELL_STEP = {
+    "fg::k_fwd + fg::k_fwd_slab + fg::k_fwd_core": (7.8e6 + 41.2e6 + 8.4e6 + 89.5e6 + 64.0e6) / (64 * 440 * 340),
     "fg::k_fwd + fg::k_fwd_core": (54.3e6 + 14.7e6 + 89.8e6 + 63.9e6) / (64 * 440 * 340),
     "fg::k_adj + fg::k_adj_core": (79.9e6 + 15.4e6 + 119.6e6 + 50.4e6) / (64 * 440 * 340),
     "fg::k_fwd (": 259.6e6 / (64 * 440 * 340), "fg::k_adj_pipe": 281.5e6 / (64 * 440 * 340),
