@@ -117,3 +117,33 @@ def test_merged_forward_requests_equal_alone(fg):
     for a, res in zip(alone, got):
         assert res.traces.shape[0] == a.shape[0]
         assert np.array_equal(a, res.traces.cpu().numpy())
+
+
+def test_shortest_job_first_and_fifo(fg):
+    """Behind a running request, 'sjf' admits the queued request with the least
+    work first and 'fifo' the oldest; every result is the same either way."""
+    serve, reqs = _requests(fg)
+    big = fg.workloads.small(seed=6, nx=200, ny=200, shots=16, nt=6000, pml=10, fixed=True)
+    big.source_step = [0.05, 0.01, 0.0]
+    kw = big.kwargs("cuda")
+    for key in ("er", "se", "mr", "device", "tv"):
+        kw.pop(key)
+    hold = serve.Request(kw, torch.tensor(big.er), torch.tensor(big.se), torch.tensor(big.mr),
+                         torch.zeros((16, 6000, big.nrx)))   # holds the one slot while the others queue
+    queued = [reqs[3], reqs[4], reqs[0]]   # forward 56x48x12x100; gradients 48x40x1x200, 48x40x3x120
+    order = {}
+    results = {}
+    for policy in ("sjf", "fifo"):
+        srv = serve.Server("cuda:0", max_active=1, policy=policy, max_wait=60.0)
+        first = srv.submit(hold)
+        futs = [srv.submit(r) for r in queued]
+        first.result()
+        got = [f.result() for f in futs]
+        srv.close()
+        order[policy] = [k for k, _ in sorted(enumerate(got), key=lambda kv: kv[1].started)]
+        results[policy] = [r.traces.cpu().numpy() for r in got]
+    # work (nx * ny * shots * nt, gradients x 2.5): 3.2e6 (forward), 0.96e6, 1.73e6
+    assert order["fifo"] == [0, 1, 2]
+    assert order["sjf"] == [1, 2, 0]
+    for a, b in zip(results["sjf"], results["fifo"]):
+        assert np.array_equal(a, b)
