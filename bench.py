@@ -415,9 +415,10 @@ def run_ours(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_e2e:
         per_shot = run_per_shot(args, fg, wl, dev)
 
-    small = ckpt = cfg3 = None
+    small = ckpt = cfg3 = batch = None
     if rank == 0 and world == 1 and not args.no_e2e:
         small = run_small_configs(fg, dev)
+        batch = run_batch_uneven(fg, dev)
         ckpt = run_checkpointed(args, fg, wl, dev, tuning)
         if not args.no_config3:
             cfg3 = run_config3(fg, dev)
@@ -457,6 +458,7 @@ def run_ours(args, rank, local, world):
             "graph_replay": graph,
             "per_shot_path": per_shot,
             "small_configs": small,
+            "batch_uneven": batch,
             "checkpointed": ckpt,
             "config3": cfg3,
             "serving": serving,
@@ -547,6 +549,73 @@ def run_per_shot(args, fg, wl, dev, shots=4):
     return {"value": round(wl.nx * wl.ny * shots * wl.nt / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
             "shots": shots, "ms_per_shot": round(ms / shots, 3),
             "api": "compute(..., step=1, tv=False) + traces.backward(resid), looped over shots"}
+
+
+def run_batch_uneven(fg, dev, n_models=8, seed=2024, reps=2):
+    """Many small models of uneven size: 8 seeded models (grids 100x60 to
+    256x256 plus a 20-cell CPML, 8-32 shots, nt 800-1600, layered), each a
+    forward + reference-mode adjoint, solved (a) one after another with the
+    default launch shapes and (b) all in one persistent launch per direction
+    (fg_forward_batch / fg_adjoint_reference_batch, plans with persistent = 1).
+    Same metric, the pair counted once; inputs resident on the device."""
+    nat = importlib.import_module(PKG + "._native")
+    wmod = fg.workloads
+    rng = np.random.default_rng(seed)
+    models = []
+    for _ in range(n_models):
+        nx_, ny_ = int(rng.integers(100, 257)), int(rng.integers(60, 257))
+        shots, nt = int(rng.integers(8, 33)), int(rng.integers(800, 1601))
+        er, se = wmod._layered_model(rng, nx_, ny_, 0.025)
+        er = wmod._pad(er, wmod.PAD).astype(np.float32)
+        se = wmod._pad(se, wmod.PAD).astype(np.float32)
+        p, lx, ly = wmod.PAD * 0.025, nx_ * 0.025, ny_ * 0.025
+        models.append(wmod.Workload("batch", nx_ + 40, ny_ + 40, 0.025, shots, nt, 2e8, er, se, np.ones_like(er),
+                                    source_location=[p + 0.05 * lx, p + 0.1 * ly, 0.0],
+                                    source_step=[0.9 * lx / shots, 0.0, 0.0],
+                                    receiver_location=[p + 0.05 * lx, p + 0.9 * ly, 0.0],
+                                    receiver_step=[0.9 * lx / 16, 0.0, 0.0], nrx=16, fixed_receiver=True))
+    cells = sum(w.nx * w.ny * w.shots * w.nt for w in models)
+    out = {"models": n_models, "cell_steps": int(cells)}
+    for mode, tuning in (("one_after_another", None), ("one_persistent_launch", {"lanes": 1, "persistent": 1})):
+        solves, mats, bufs = [], [], []
+        for w in models:
+            setup = _setup_of(fg, w, dev)
+            s = fg.Solve(dev, setup, tuning=tuning, tv=False)
+            m = tuple(torch.tensor(a, device=dev) for a in (w.er, w.se, w.mr))
+            tr = torch.empty((setup.shots, setup.nt, s.plan.nrx), device=dev)
+            bufs.append((tr, s.plan.new_hist(), torch.randn(tr.shape, device=dev) * 1e-3,
+                         torch.empty((setup.nx, setup.ny), device=dev), torch.empty((setup.nx, setup.ny), device=dev)))
+            solves.append(s)
+            mats.append(m)
+        plans = [s.plan for s in solves]
+
+        def step():
+            if mode == "one_after_another":
+                for p, m, b in zip(plans, mats, bufs):
+                    p.forward(m[0], m[1], m[2], b[0], b[1])
+                    p.adjoint_reference(m[0], m[1], m[2], b[1], b[2], b[3], b[4])
+            else:
+                cols = lambda k: [m[k] for m in mats]
+                nat.forward_batch(plans, cols(0), cols(1), cols(2), [b[0] for b in bufs], [b[1] for b in bufs])
+                nat.adjoint_reference_batch(plans, cols(0), cols(1), cols(2), [b[1] for b in bufs],
+                                            [b[2] for b in bufs], [b[3] for b in bufs], [b[4] for b in bufs])
+
+        step()
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(reps):
+            step()
+        t1.record()
+        torch.cuda.synchronize(dev)
+        for p in plans:
+            p.device_check()
+        ms = t0.elapsed_time(t1) / reps
+        out[mode] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": UNIT, "ms_per_step": round(ms, 2)}
+        del solves, plans, bufs, mats
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_small_configs(fg, dev, reps=3):
