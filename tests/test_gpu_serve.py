@@ -147,3 +147,47 @@ def test_shortest_job_first_and_fifo(fg):
     assert order["sjf"] == [1, 2, 0]
     for a, b in zip(results["sjf"], results["fifo"]):
         assert np.array_equal(a, b)
+
+
+def test_batched_small_requests_equal_alone(fg):
+    """Small shot-lane requests of different grids, models and step counts
+    queued behind a running request are solved together in one persistent
+    launch per direction; each gets the bits it gets alone."""
+    serve = __import__("importlib").import_module("fast-gpr-fwi_b200.serve")
+    reqs = []
+    for n, (nx, ny, shots, nt) in enumerate([(56, 48, 12, 100), (64, 40, 9, 130), (48, 64, 20, 90)]):
+        wl = fg.workloads.small(seed=30 + n, nx=nx, ny=ny, shots=shots, nt=nt, pml=6, fixed=True)
+        wl.source_step = [0.02, 0.01, 0.0]
+        kw = wl.kwargs("cuda")
+        for key in ("er", "se", "mr", "device", "tv"):
+            kw.pop(key)
+        resid = None
+        if n != 1:
+            rng = np.random.default_rng(n)
+            resid = torch.tensor(rng.standard_normal((shots, nt, wl.nrx)).astype(np.float32) * 1e-3)
+        reqs.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid))
+    alone = []
+    for r in reqs:
+        srv = serve.Server("cuda:0", max_active=1)
+        alone.append(_arrays(srv.submit(r).result()))
+        srv.close()
+    big = fg.workloads.small(seed=5, nx=200, ny=200, shots=4, nt=6000, pml=10, fixed=True)
+    big.source_step = [0.05, 0.01, 0.0]
+    kw = big.kwargs("cuda")
+    for key in ("er", "se", "mr", "device", "tv"):
+        kw.pop(key)
+    hold = serve.Request(kw, torch.tensor(big.er), torch.tensor(big.se), torch.tensor(big.mr), None)
+    srv = serve.Server("cuda:0", max_active=1)
+    first = srv.submit(hold)                     # holds the one slot while the small ones queue
+    futs = [srv.submit(r) for r in reqs]
+    first.result()
+    got = [_arrays(f.result()) for f in futs]
+    st = srv.stats()
+    srv.close()
+    assert st["batched"] == len(reqs)
+    for a, b in zip(alone, got):
+        for x, y in zip(a, b):
+            if x is None:
+                assert y is None
+            else:
+                assert np.array_equal(x, y)
