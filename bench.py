@@ -833,7 +833,7 @@ def serving_stream(fg, n=12, seed=4004):
 
 
 def _serve_once(serve, dev, reqs, gaps, active, policy="sjf", merge=True):
-    srv = serve.Server(dev, max_active=active, policy=policy, merge=merge)
+    srv = serve.Server(dev, max_active=active, policy=policy, merge=merge, batch=merge)
     futs = []
     for r, gap in zip(reqs, gaps):
         time.sleep(float(gap))
@@ -844,7 +844,7 @@ def _serve_once(serve, dev, reqs, gaps, active, policy="sjf", merge=True):
     srv.close()
     return {"p50_ms": round(st["p50_s"] * 1e3, 1), "p99_ms": round(st["p99_s"] * 1e3, 1),
             "throughput_gcs": round(st["throughput_gcs"], 3), "peak_active": st["peak_active"],
-            "merged": st["merged"]}
+            "merged": st["merged"], "batched": st["batched"]}
 
 
 def run_serving(fg, dev, rates_x=(0.5, 1.0, 2.0)):
