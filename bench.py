@@ -847,6 +847,44 @@ def _serve_once(serve, dev, reqs, gaps, active, policy="sjf", merge=True):
             "merged": st["merged"], "batched": st["batched"]}
 
 
+def run_serving_small(fg, dev, n=16, seed=5005):
+    """A burst of small requests (grids 100x60 to 256x256 plus a 20-cell
+    CPML, 8-32 shots, nt 800-1600, half gradients), all queued at once:
+    continuous batching (small shot-lane requests batched into one persistent
+    launch per direction, up to 4 launches on the GPU at once) against the
+    plain one-request-at-a-time path."""
+    serve = importlib.import_module(PKG + ".serve")
+    wmod = fg.workloads
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for k in range(n):
+        nx_, ny_ = int(rng.integers(100, 257)), int(rng.integers(60, 257))
+        shots, nt = int(rng.integers(8, 33)), int(rng.integers(800, 1601))
+        er, se = wmod._layered_model(rng, nx_, ny_, 0.025)
+        er = wmod._pad(er, wmod.PAD).astype(np.float32)
+        se = wmod._pad(se, wmod.PAD).astype(np.float32)
+        p, lx, ly = wmod.PAD * 0.025, nx_ * 0.025, ny_ * 0.025
+        wl = wmod.Workload("serve", nx_ + 40, ny_ + 40, 0.025, shots, nt, 2e8, er, se, np.ones_like(er),
+                           source_location=[p + 0.05 * lx, p + 0.1 * ly, 0.0], source_step=[0.9 * lx / shots, 0.0, 0.0],
+                           receiver_location=[p + 0.05 * lx, p + 0.9 * ly, 0.0], receiver_step=[0.9 * lx / 16, 0.0, 0.0],
+                           nrx=16, fixed_receiver=True)
+        kw = wl.kwargs("cuda")
+        for key in ("er", "se", "mr", "device", "tv"):
+            kw.pop(key)
+        resid = None
+        if k % 2:
+            resid = torch.tensor(rng.standard_normal((shots, nt, wl.nrx)).astype(np.float32) * 1e-3)
+        reqs.append(serve.Request(kw, torch.tensor(wl.er), torch.tensor(wl.se), torch.tensor(wl.mr), resid))
+    warm = serve.Server(dev, max_active=1)
+    warm.submit(reqs[0]).result()
+    warm.close()
+    out = {"requests": n, "arrivals": "all at once"}
+    for name, active, plain in (("continuous", 4, False), ("one_at_a_time", 1, True)):
+        out[name] = _serve_once(serve, dev, reqs, np.zeros(n), active, "fifo" if plain else "sjf", not plain)
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_serving(fg, dev, rates_x=(0.5, 1.0, 2.0)):
     """The stream at Poisson rates swept across saturation, served with
     continuous batching (up to 4 requests on the GPU at once, a GPU-filling
@@ -868,8 +906,9 @@ def run_serving(fg, dev, rates_x=(0.5, 1.0, 2.0)):
     top = np.random.default_rng(7).exponential(1.0 / (rates_x[-1] * sat), size=len(reqs))
     one = dict(rate_hz=round(rates_x[-1] * sat, 3), **_serve_once(serve, dev, reqs, top, 1, "fifo", False))
     torch.cuda.empty_cache()
+    small = run_serving_small(fg, dev)
     return {"requests": len(reqs), "saturation_hz": round(sat, 3), "all_queued_one_at_a_time": base,
-            "rates": rates, "one_at_a_time": one,
+            "rates": rates, "one_at_a_time": one, "small_burst": small,
             "stream": "grids 100x60-1024x1024 (+2x20 CPML), nt 1000-8000, 1-32 shots, 100-200 MHz; "
                       "half gradients, half forward requests in same-survey pairs",
             "unit": "Gcell-steps/s, nx*ny*shots*nt per request counted once (forward or gradient)"}
