@@ -270,6 +270,12 @@ void fill_grid(fg_plan* p) {
     g.tiles = (const int4*)(w + p->o_tiles);
     g.tile_ctr = (int*)(w + p->o_ctr);
     g.fast_cpml = 2 * p->th < p->nx && 2 * p->th < p->ny;
+    // shot lanes with no band whose cells (columns j0-1 .. j0+W) reach both y slabs
+    g.lean = p->shot && !p->pair && g.fast_cpml;
+    for (int b = 0; b < p->nb && g.lean; ++b) {
+        const int j0 = b * p->BW, j1 = j0 + p->BW;
+        if (p->th > 0 && j0 - 1 <= p->th && j1 >= p->ny - p->th) g.lean = 0;
+    }
     g.pf = p->pf;
     g.core0 = p->core0;
     g.slab0 = p->slab0;

@@ -68,6 +68,7 @@ struct Dev {
     int fast_cpml;                          // 2 th < nx and 2 th < ny: no cell in two slabs of one axis
     int core0;                              // first fetch position of the interior tiles (lean kernels)
     int slab0, yslab0;                      // x-slab tiles [slab0, yslab0), y-slab tiles [yslab0, core0)
+    int lean;                               // every band takes the shot-lane CPML rows (see fwd_step)
     int pf;                                 // lane march, shot lanes: prefetch a warp's next tile into L2
                                             // (0 no, 1 when the current tile starts, 2 at its middle row)
     const int* chunk_row;                   // (nc+1) row boundaries

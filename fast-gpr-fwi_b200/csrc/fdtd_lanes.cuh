@@ -381,7 +381,7 @@ __device__ __forceinline__ void fwd_receivers(const Dev& g, int i, int t, int j0
 
 // Row i of the forward step from its operands; carries ezc (Ez_old of row i,
 // columns j0-1 .. j0+W) and hyu (Hy_new of row i-1) to the next row.
-template <int W, int CS>
+template <int W, int CS, bool LEAN = false>
 __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const BandY& by, const FwdIn<W>& B,
                                         float (&ezc)[W + 2], float (&hyu)[W], int i, int t, int j0, int l, int slot,
                                         int s, bool bcore,
@@ -391,7 +391,7 @@ __device__ __forceinline__ void fwd_row(const Dev& g, const float* R, const Band
     float hxn[W + 1], hyn[W], ezn[W];
     if (bcore && i >= th + 1 && i <= nx - th - 1) {
         fwd_core<W>(B, ezc, hyu, hxn, hyn, ezn);
-    } else if (CS == 32 && by.lean) {
+    } else if (CS == 32 && (LEAN || by.lean)) {
         if constexpr (CS == 32)
             fwd_row_shot<W>(g, R, by, i, j0, l, B.hxo, B.hyo, B.en, ezc, hyu, B.ca, B.cb, B.ch, rd, wr, hxn, hyn, ezn);
     } else if (g.fast_cpml) {
@@ -485,7 +485,10 @@ __device__ __forceinline__ void issue_fwd(const Dev& g, uint64_t* bar, float* st
 // step's counter until none is left.  R: the CPML profile (shared or global
 // memory); smem: the block's dynamic shared memory (RING stages after the
 // profile).
-template <int W, bool SHOT, bool RING>
+// LEAN: every band of the plan takes the shot-lane CPML rows (the host checks
+// it: fast_cpml and no band with cells in both y slabs), so the generic
+// per-cell CPML paths are compiled out.
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 __device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned char* smem, const int t, const int D) {
     constexpr int CS = SHOT ? 32 : 1;
     using RG = RingGeom<W, SHOT>;
@@ -595,7 +598,7 @@ __device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned 
                     hyu[w] = ha[w];
                     dz[w] = __fsub_rn(ezc[w + 1], ea[w]);
                 }
-                if (SHOT && by.lean) {
+                if (SHOT && (LEAN || by.lean)) {
                     if constexpr (SHOT) fwd_hy_halo_shot<W>(g, R, by, ih, j0, l, hyu, dz, ca, rd);
                 } else if (g.fast_cpml) {
                     hy_cells<W, CS, false>(g, R, ih, j0, l, hyu, dz, ca, rd, rd);
@@ -654,7 +657,7 @@ __device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned 
                 load_row(i);
             }
             if (T.live)
-                fwd_row<W, CS>(g, R, by, B, ezc, hyu, i, t, j0, l, slot, T.s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr,
+                fwd_row<W, CS, LEAN>(g, R, by, B, ezc, hyu, i, t, j0, l, slot, T.s, bcore, ezW, hxW, hyW, hist, hrow, rd, wr,
                                sc, se, rc, re);
         }
         cur = nxt;
@@ -674,7 +677,7 @@ __device__ __forceinline__ void fwd_step(const Dev& g, const float* R, unsigned 
 // waits for it to complete (griddep_wait) before it touches anything the step
 // reads or writes, then lets the slab and interior kernels behind it start
 // (they read none of this launch's results; see fdtd_core.cuh).
-template <int W, bool SHOT, bool RING>
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* R = stage_profile(g, smem);   // the profile is fixed for the solve
@@ -682,7 +685,7 @@ __global__ void __launch_bounds__(128, 4) k_fwd(const Dev g, const int t, const 
     griddep_launch_dependents();
     // a stage of an earlier launch never landed: leave at once
     if (RING && *(volatile int*)g.err != 0) return;
-    fwd_step<W, SHOT, RING>(g, R, smem, t, D);
+    fwd_step<W, SHOT, RING, LEAN>(g, R, smem, t, D);
 }
 
 // ---------------------------------------------------------------------------
@@ -741,14 +744,14 @@ __device__ __forceinline__ void adj_e_core(const AdjEIn<W>& A, const float (&hyu
 // old H (hyu = Hy_old of row r-1).  Auxiliaries are stored for the thread's
 // own cells when `own` (row r inside the chunk); the halo column and the halo
 // row below the chunk only read theirs.
-template <int W, int CS>
+template <int W, int CS, bool LEAN = false>
 __device__ __forceinline__ void adj_e_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A, int r, int j0,
                                           int l, int slot, bool core, bool own, const float (&hyu)[W + 1], float (&out)[W + 1],
                                           long long resid_o, int& ic, int ie, const PsiG& rd, const PsiG& wr) {
     adj_inject<W>(g, A.ez, r, j0, slot, resid_o, ic, ie);
     if (core) {
         adj_e_core<W>(A, hyu, out);
-    } else if (CS == 32 && by.lean) {
+    } else if (CS == 32 && (LEAN || by.lean)) {
         if constexpr (CS == 32)
             adj_e_row_shot<W>(g, R, by, r, j0, l, own, A.ez, A.hxo, A.hyo, hyu, A.ca, A.cb, rd, wr, out);
     } else if (g.fast_cpml) {
@@ -853,7 +856,7 @@ __device__ __forceinline__ void adj_image(const Dev& g, const float (&f1)[W], co
 // chunk [.., i1), else the halo row below; nothing when r is the frame row),
 // H of row i from the new E, the imaging sums and the stores; then the
 // carried rows (new E, old H and old Ez of row i) move on to row r.
-template <int W, bool SHOT>
+template <int W, bool SHOT, bool LEAN = false>
 __device__ __forceinline__ void adj_row(const Dev& g, const float* R, const BandY& by, AdjEIn<W>& A,
                                         const float (&ch)[W], const float (&f1)[W], float (&ezc)[W + 1],
                                         float (&hxc)[W + 2], float (&hyc)[W + 1], float (&eoc)[W], int i, int i1,
@@ -868,7 +871,7 @@ __device__ __forceinline__ void adj_row(const Dev& g, const float* R, const Band
     if (r < nx) {
 #pragma unroll
         for (int w = 0; w < W; ++w) eor[w] = A.ez[w];
-        adj_e_row<W, CS>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyc, ezr,
+        adj_e_row<W, CS, LEAN>(g, R, by, A, r, j0, l, slot, bcore && r >= th + 1 && r <= nx - th - 1, r < i1, hyc, ezr,
                          resid_o, ic, ie, rd, wr);
     } else {
 #pragma unroll
@@ -882,7 +885,7 @@ __device__ __forceinline__ void adj_row(const Dev& g, const float* R, const Band
     float hx[W], hy[W];
     if (bcore && i >= th + 1 && i <= nx - th - 1) {
         adj_h_core<W>(ch, ezc, ezr, hxc, hyc, hx, hy);
-    } else if (SHOT && by.lean) {
+    } else if (SHOT && (LEAN || by.lean)) {
         float dzx[W], dzy[W];
 #pragma unroll
         for (int w = 0; w < W; ++w) {
@@ -968,7 +971,7 @@ __device__ __forceinline__ void issue_adj(const Dev& g, uint64_t* bar, float* st
 
 // Reference-mode adjoint iteration it (reading parity rp) of one solve by the
 // warps of this block; R and smem as for fwd_step.
-template <int W, bool SHOT, bool RING>
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 __device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned char* smem, const int it, const int rp,
                                          const int D) {
     constexpr int CS = SHOT ? 32 : 1;
@@ -1060,7 +1063,7 @@ __device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned 
             adj_e_load<W, CS>(g, A, T.i0, j0, l, ezR, hxR, hyR);
 #pragma unroll
             for (int w = 0; w < W; ++w) eoc[w] = A.ez[w];
-            adj_e_row<W, CS>(g, R, by, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
+            adj_e_row<W, CS, LEAN>(g, R, by, A, T.i0, j0, l, slot, bcore && T.i0 >= th + 1 && T.i0 <= nx - th - 1, true, hyu,
                              ezc, resid_o, ic, ie, rd, wr);
 #pragma unroll
             for (int k = 0; k < W + 2; ++k) hxc[k] = A.hxo[k];
@@ -1128,7 +1131,7 @@ __device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned 
                     for (int w = 0; w < W; ++w) f1[w] = 0.f;
                 }
             }
-            adj_row<W, SHOT>(g, R, by, A, ch, f1, ezc, hxc, hyc, eoc, i, T.i1, j0, l, slot, lane, bcore, resid_o, ic, ie, rd,
+            adj_row<W, SHOT, LEAN>(g, R, by, A, ch, f1, ezc, hxc, hyc, eoc, i, T.i1, j0, l, slot, lane, bcore, resid_o, ic, ie, rd,
                              wr, ezW, hxW, hyW, gae, gas);
         }
         cur = nxt;
@@ -1141,14 +1144,14 @@ __device__ __forceinline__ void adj_step(const Dev& g, const float* R, unsigned 
     }
 }
 
-template <int W, bool SHOT, bool RING>
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 __global__ void __launch_bounds__(128, 3) k_adj(const Dev g, const int it, const int rp, const int D) {
     extern __shared__ __align__(128) unsigned char smem[];
     const float* R = stage_profile(g, smem);
     griddep_wait();   // as k_fwd
     griddep_launch_dependents();
     if (RING && *(volatile int*)g.err != 0) return;
-    adj_step<W, SHOT, RING>(g, R, smem, it, rp, D);
+    adj_step<W, SHOT, RING, LEAN>(g, R, smem, it, rp, D);
 }
 
 // The last term of the summation by parts: g_eps -= sum_s Ez_f[0] lambda_1,

@@ -3,10 +3,10 @@
 
 namespace fgk {
 
-template <int W, bool SHOT, bool RING>
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 cudaError_t launch_adj_k(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
     const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, true) : 0);
-    auto kernel = fg::k_adj<W, SHOT, RING>;
+    auto kernel = fg::k_adj<W, SHOT, RING, LEAN>;
     if (*blocks == 0) {
         cudaError_t e = allow_smem(kernel, smem);
         if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
@@ -16,8 +16,10 @@ cudaError_t launch_adj_k(const Dev& g, int it, int rp, int wpb, int D, int* bloc
 }
 template <int W, bool SHOT>
 cudaError_t launch_adj(const Dev& g, int it, int rp, int wpb, int D, int* blocks, cudaStream_t st) {
-    return D == 0 ? launch_adj_k<W, SHOT, false>(g, it, rp, wpb, D, blocks, st)
-                  : launch_adj_k<W, SHOT, true>(g, it, rp, wpb, D, blocks, st);
+    if (D != 0) return launch_adj_k<W, SHOT, true>(g, it, rp, wpb, D, blocks, st);
+    if constexpr (SHOT)
+        if (g.lean) return launch_adj_k<W, SHOT, false, true>(g, it, rp, wpb, D, blocks, st);
+    return launch_adj_k<W, SHOT, false>(g, it, rp, wpb, D, blocks, st);
 }
 
 template <bool SHOT>

@@ -3,10 +3,10 @@
 
 namespace fgk {
 
-template <int W, bool SHOT, bool RING>
+template <int W, bool SHOT, bool RING, bool LEAN = false>
 cudaError_t launch_fwd_k(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
     const size_t smem = fg::prof_bytes(g.th) + (RING ? ring_smem<W, SHOT>(wpb, D, false) : 0);
-    auto kernel = fg::k_fwd<W, SHOT, RING>;
+    auto kernel = fg::k_fwd<W, SHOT, RING, LEAN>;
     if (*blocks == 0) {
         cudaError_t e = allow_smem(kernel, smem);
         if (e == cudaSuccess) e = persistent_blocks(kernel, wpb, smem, g.ntiles, blocks);
@@ -16,8 +16,10 @@ cudaError_t launch_fwd_k(const Dev& g, int t, int wpb, int D, int* blocks, cudaS
 }
 template <int W, bool SHOT>
 cudaError_t launch_fwd(const Dev& g, int t, int wpb, int D, int* blocks, cudaStream_t st) {
-    return D == 0 ? launch_fwd_k<W, SHOT, false>(g, t, wpb, D, blocks, st)
-                  : launch_fwd_k<W, SHOT, true>(g, t, wpb, D, blocks, st);
+    if (D != 0) return launch_fwd_k<W, SHOT, true>(g, t, wpb, D, blocks, st);
+    if constexpr (SHOT)
+        if (g.lean) return launch_fwd_k<W, SHOT, false, true>(g, t, wpb, D, blocks, st);
+    return launch_fwd_k<W, SHOT, false>(g, t, wpb, D, blocks, st);
 }
 template <bool SHOT>
 FwdFn pick_fwd_w(int W) {
