@@ -117,8 +117,8 @@ typedef struct fg_tuning {
      * a lean kernel of their own, side by side with the general kernel on the
      * other tiles.  -1 = off; 0 = default (on when nx * ny * shot groups is
      * at least 2e5 -- smaller steps do not pay for the second launch -- with
-     * the general kernel at 3 blocks per SM for the forward and 4 for the
-     * adjoint); 1..8 = on, the general kernel with that many blocks per SM. */
+     * the general kernel at 3 blocks per SM); 1..8 = on, the general
+     * kernel with that many blocks per SM. */
     int32_t interior;
     /* Lane march without stages or shot pairs: the whole time loop of a
      * solve in one persistent cooperative launch, the steps separated by a
