@@ -347,19 +347,21 @@ def run_ours(args, rank, local, world):
     bytes_launch = adj_b if dom == "adjoint" else fwd_b
     launch_ms = adj_launch_ms if dom == "adjoint" else fwd_launch_ms
     achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
-    # the interior split of the lane march (shot lanes, no stages, nx * ny * groups >= 2e5)
+    # the interior split of the lane march (shot lanes, no stages, not
+    # persistent, nx * ny * groups >= 12,000)
     t = tuning or {}
     shot = t.get("lanes", 1 if S >= 8 else 2) == 1
+    work = nx * ny * ((S + 31) // 32)
     split = (shot and t.get("interior", 0) != -1 and not t.get("stages") and t.get("kernel", 1) == 1
-             and (t.get("interior", 0) > 0 or nx * ny * ((S + 31) // 32) >= 200000))
+             and (t.get("interior", 0) > 0 or (work >= 12000 and t.get("persistent", 0) != 1)))
     kname = kernel_name(tuning, dom, split)
     # this library's kernels per fwd + adj step: the forward's (general, slab,
     # interior) per time step, the adjoint's (general, interior; slab when
-    # asked for) per iteration, two coefficient kernels, the imaging tail and
-    # three gradient reductions
+    # asked for or below 120,000 cells x groups) per iteration, two
+    # coefficient kernels, the imaging tail and three gradient reductions
     slab = t.get("slab", 0)
     fwd_k = (3 if slab != -1 else 2) if split else 1
-    adj_k = (3 if slab > 0 else 2) if split else 1
+    adj_k = (3 if slab > 0 or (slab == 0 and work < 120000) else 2) if split else 1
     launches_per_step = fwd_k * nt + adj_k * (nt - 1) + 6
     ncu = next((v for k, v in NCU_BYTES_PER_SHOT_CELL_STEP.items() if kname.startswith(k)), None)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",

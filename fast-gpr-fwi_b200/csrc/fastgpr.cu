@@ -721,15 +721,17 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
         delete p;
         return fail(FG_ERR_INVALID, "unsupported tuning: interior must be -1 .. 8");
     }
-    // by default only where a step is long enough to pay for its second launch
-    // (at least 2e5 cells x shot groups: the 440 x 340 x 2-group benchmark grid,
-    // not the small grids of the serving stream, whose steps take microseconds)
+    // by default wherever a step pays for the extra launches: at least 12,000
+    // cells x shot groups (measured, us per forward / adjoint step with the
+    // split against without: 140 x 100, 16 shots 15.3 / 24.5 against 19.5 /
+    // 25.9; 440 x 340, 32 shots 34.5 / 60.2 against 48.4 / 73.9; 100 x 80,
+    // 8 shots 19.3 against 18.0 forward), and not in a persistent plan, whose
+    // one launch takes every tile
     const long long work = (long long)p->nx * p->ny * ((p->S + 31) / 32);
     p->split = p->kernel == 1 && p->shot && !p->pair && p->D == 0 && pick_fwd_core(p->W) &&
-               (interior > 0 || (interior == 0 && work >= 200000));
-    // measured on the 64-shot 440 x 340 benchmark grid: the forward's general
-    // kernel is fastest beside the interior kernel with 3 blocks per SM (the
-    // adjoint's, on its own plan, with 4; fg_plan_create passes that)
+               (interior > 0 || (interior == 0 && work >= 12000 && persistent != 1));
+    // measured on the 64-shot 440 x 340 benchmark grid: the general kernel is
+    // fastest beside the interior kernel with 3 blocks per SM
     p->split_bpsm = interior > 0 ? interior : 3;
     const int slab = tune ? tune->slab : 0;
     if (slab < -1 || slab > 8) {
@@ -739,8 +741,8 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
     // measured on the 64-shot 440 x 340 benchmark grid (us per step): the
     // forward's slab kernel at 2 blocks per SM beside the others 68.1 against
     // 75.3 without it (1: 88.9, 3: 77.7, as many as fit: 83.9); the
-    // adjoint's (8 cells per thread, 168 registers) 109.3 against 98.5
-    // without it, so fg_plan_create leaves it off for the adjoint plan
+    // adjoint's (8 cells per thread) 109.3 against 98.5 without it, so
+    // fg_plan_create turns it on for the adjoint plan on small steps only
     p->slab_on = p->split && slab != -1;
     p->slab_bpsm = slab > 0 ? slab : 2;
     // beside the interior kernel the general kernel's next-tile prefetch only
@@ -808,8 +810,17 @@ int fg_plan_create(const fg_problem* prob, const fg_tuning* tune, fg_plan** out)
     at.prefetch = tune ? tune->prefetch : 0;
     at.interior = tune ? tune->interior : 0;
     at.persistent = tune ? tune->persistent : 0;
-    // the adjoint's slab kernel only when asked for (measured slower)
-    at.slab = tune && tune->slab ? tune->slab : -1;
+    // the adjoint's slab kernel (4 cells per thread) on small steps, where the
+    // general kernel's CPML tiles are most of the work; measured, us per
+    // adjoint step with 2 / 1 / 0 slab blocks per SM: 140 x 100, 16 shots
+    // 18.2 / 18.2 / 24.5; 280 x 200, 13 shots 19.9 / 21.5 / 28.1; 296 x 296,
+    // 32 shots 41.7 / 38.3 / 41.3; 440 x 340, 32 shots 78.2 / 63.0 / 60.2
+    if (tune && tune->slab) {
+        at.slab = tune->slab;
+    } else {
+        const long long work = (long long)prob->nx * prob->ny * ((prob->shots + 31) / 32);
+        at.slab = work < 50000 ? 2 : (work < 120000 ? 1 : -1);
+    }
     fg_plan* a = nullptr;
     rc = create_one(prob, &at, &a);
     if (rc) {

@@ -9,8 +9,12 @@ segment (the checkpointed solve, bit-identical results).  Admitted requests
 run side by side, each on a CUDA stream of its own driven by a worker
 thread (the library's launches release the GIL), so requests that arrive
 while others are on the GPU overlap with them on the device -- except a
-request whose steps fill the GPU on their own (EXCLUSIVE_WORK), which runs
-alone: side by side such solves only share the SMs and the L2.  Every result
+request whose steps fill the GPU on their own, which runs alone: a step of
+at least EXCLUSIVE_WORK cells x shot groups, or a shot-lane step of at least
+SPLIT_WORK, whose step kernels (general, slab and interior beside each other)
+are sized for the whole GPU.  Side by side such solves only share the SMs
+and the L2, and their early-launched dependent kernels hold SM slots the
+other streams could use.  Every result
 is computed by the same kernels in the same order as the request alone, so
 it is the same alone and in the mix, bit for bit.
 
@@ -24,13 +28,15 @@ it).  Gradient requests are not merged: the imaging sums add the shots of
 a shot group together, and a request's gradient must hold its own shots
 only.
 
-Small requests in shot lanes (at least 8 shots, a step below EXCLUSIVE_WORK)
+Small requests in shot lanes (at least 8 shots, a step below SPLIT_WORK)
 that queue together -- different grids, models and step counts -- are
 batched into one persistent launch per direction (fg_forward_batch and
-fg_adjoint_reference_batch, up to 8 requests): measured on eight uneven
-small models, 15.0 against 12.6 Gcell-steps/s one after another.  The
-persistent launch computes the bits of the launch per step, so each request
-again gets what it gets alone.
+fg_adjoint_reference_batch, up to 8 requests).  The persistent launch
+computes the bits of the launch per step, so each request again gets what
+it gets alone.  Larger shot-lane requests are not batched: with the
+interior split, one after another they are faster than in one persistent
+launch (measured on eight uneven models of 140 x 100 to 296 x 296 cells and
+8-32 shots: 19.1 against 15.6 Gcell-steps/s).
 
 Throughput counts a request's nx * ny * shots * nt cell-steps once, forward
 or gradient (a forward + adjoint pair counted once, the benchmark's unit).
@@ -107,13 +113,21 @@ MERGE_SHOTS = 64   # shots of one merged forward solve at most (two groups of 32
 # such requests ran at 30 Gcell-steps/s four at a time against 36 one at a
 # time).  Such a request runs alone; smaller ones share the GPU.
 EXCLUSIVE_WORK = 150_000
+# A shot-lane step of at least this many cells x shot groups runs the
+# interior split by default (fg_tuning.interior): its general, slab and
+# interior kernels are each sized for the whole GPU and launched early
+# behind one another, so it too runs alone (measured on a burst of 16 small
+# shot-lane gradient and forward requests: 11.6 Gcell-steps/s four at a
+# time against 26.6 one at a time).
+SPLIT_WORK = 12_000
 
 
 def _weight(job: "_Job", max_active: int) -> int:
     """Slots a job takes: all of them for a step that fills the GPU, else one."""
     s = job.solve.setup
-    groups = (s.shots + 31) // 32 if s.shots >= 8 else s.shots
-    return max_active if s.nx * s.ny * groups >= EXCLUSIVE_WORK else 1
+    shot = s.shots >= 8
+    work = s.nx * s.ny * ((s.shots + 31) // 32 if shot else s.shots)
+    return max_active if work >= EXCLUSIVE_WORK or (shot and work >= SPLIT_WORK) else 1
 
 
 def _mergeable(a: "_Job", b: "_Job") -> bool:

@@ -116,9 +116,9 @@ typedef struct fg_tuning {
      * cell in the tile or its halo, no source, receiver or injection) run in
      * a lean kernel of their own, side by side with the general kernel on the
      * other tiles.  -1 = off; 0 = default (on when nx * ny * shot groups is
-     * at least 2e5 -- smaller steps do not pay for the second launch -- with
-     * the general kernel at 3 blocks per SM); 1..8 = on, the general
-     * kernel with that many blocks per SM. */
+     * at least 12,000 -- smaller steps do not pay for the extra launches --
+     * and persistent is not 1, with the general kernel at 3 blocks per SM);
+     * 1..8 = on, the general kernel with that many blocks per SM. */
     int32_t interior;
     /* Lane march without stages or shot pairs: the whole time loop of a
      * solve in one persistent cooperative launch, the steps separated by a
@@ -132,8 +132,10 @@ typedef struct fg_tuning {
     /* With the interior split: the slab tiles (in one CPML slab, no event)
      * run in a lean kernel of their own between the general and the interior
      * kernel.  -1 = off (they stay in the general kernel); 0 = default (the
-     * forward's on with at most 2 blocks per SM, the adjoint's off); 1..8 =
-     * on for both, at most that many blocks per SM. */
+     * forward's on with at most 2 blocks per SM; the adjoint's with at most
+     * 2 blocks per SM when nx * ny * shot groups is below 50,000, 1 below
+     * 120,000, off above); 1..8 = on for both, at most that many blocks per
+     * SM. */
     int32_t slab;
 } fg_tuning;
 
