@@ -653,7 +653,20 @@ static int create_one(const fg_problem* prob, const fg_tuning* tune, fg_plan** o
         return fail(FG_ERR_INVALID, "unsupported tuning: kernel must be 0 (tiles), 1 (lane march) or 2 (band pipeline)");
     }
     p->W = tune && tune->cells_per_thread ? tune->cells_per_thread : (p->shot ? 4 : 2);
-    p->TI = tune && tune->rows_per_tile ? tune->rows_per_tile : (p->kernel == 2 ? 32 : 4);
+    // rows per tile: 4, but 2 for the shot-lane lane march on steps below
+    // 1.2e5 cells x shot groups, where the general kernel holds only a few
+    // hundred tiles, one per warp, and a tile's serial latency is the step's
+    // (measured, us per forward step with 2 / 4 rows: 100 x 80, 8 shots 11.6 /
+    // 18.1; 240 x 160, 13 shots 14.2 / 16.7; 296 x 296, 32 shots 22.5 / 27.5;
+    // 440 x 340, 32 shots 36.9 / 34.8)
+    const bool small_step = (long long)q.nx * q.ny * ((q.shots + 31) / 32) < 120000;
+    p->TI = tune && tune->rows_per_tile
+                ? tune->rows_per_tile
+                : (p->kernel == 2 ? 32
+                                  : (p->kernel == 1 && p->shot && !p->pair && !(tune && tune->stages) &&
+                                             persistent != 1 && small_step
+                                         ? 2
+                                         : 4));
     p->WPB = tune && tune->warps_per_block ? tune->warps_per_block : (p->kernel == 0 ? std::min(p->TI, 4) : 4);
     p->D = tune ? tune->stages : 0;
     if (p->kernel == 0 && p->pair) {

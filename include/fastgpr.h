@@ -79,7 +79,8 @@ typedef struct fg_tuning {
                                   3 = shot pairs: 64 shots of the same cells, two per lane
                                   (lane march only, cells_per_thread 2 or 4, no stages) */
     int32_t cells_per_thread;  /* 2, 4 or 8 (default 4 with shot lanes, 2 with column lanes) */
-    int32_t rows_per_tile;     /* rows of one tile, >= 1 (default 4) */
+    int32_t rows_per_tile;     /* rows of one tile, >= 1 (default 4; 2 for the shot-lane
+                                  lane march below 1.2e5 cells x shot groups) */
     int32_t warps_per_block;   /* 1, 2 or 4 (default 4) */
     int32_t stages;            /* lane march: 0 = operands loaded into registers row by row;
                                   2..8 = a ring of this many rows per warp in shared memory,
