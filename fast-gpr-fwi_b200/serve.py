@@ -36,7 +36,7 @@ computes the bits of the launch per step, so each request again gets what
 it gets alone.  Larger shot-lane requests are not batched: with the
 interior split, one after another they are faster than in one persistent
 launch (measured on eight uneven models of 140 x 100 to 296 x 296 cells and
-8-32 shots: 19.1 against 15.6 Gcell-steps/s).
+8-32 shots: 20.4 against 15.8 Gcell-steps/s).
 
 Throughput counts a request's nx * ny * shots * nt cell-steps once, forward
 or gradient (a forward + adjoint pair counted once, the benchmark's unit).
