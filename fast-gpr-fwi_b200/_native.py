@@ -31,7 +31,7 @@ EXPORTS = (
     "fg_forward_static", "fg_tv_workspace_bytes", "fg_total_variation",
     "fg_plan_checkpoint_bytes", "fg_forward_checkpointed", "fg_adjoint_reference_checkpointed",
     "fg_fir_causal", "fg_adjoint_reference_l1", "fg_adjoint_exact",
-    "fg_forward_batch", "fg_adjoint_reference_batch", "fg_plan_set_profile",
+    "fg_forward_batch", "fg_adjoint_reference_batch", "fg_plan_set_profile", "fg_plan_shape",
 )
 
 BATCH_MAX = 8   # FG_BATCH_MAX
@@ -103,6 +103,8 @@ def lib() -> ctypes.CDLL:
     L.fg_plan_hist_shape.restype = ctypes.c_int
     L.fg_plan_workspace_bytes.argtypes = [vp]
     L.fg_plan_workspace_bytes.restype = i64
+    L.fg_plan_shape.argtypes = [vp, ctypes.POINTER(i32)]
+    L.fg_plan_shape.restype = ctypes.c_int
     L.fg_plan_bind.argtypes = [vp, vp, i64, vp]
     L.fg_plan_bind.restype = ctypes.c_int
     L.fg_coefficients.argtypes = [vp, vp, vp, i32, i32, f32, f32, i32, vp, i32, vp]
@@ -205,6 +207,18 @@ class Plan:
             self.workspace = torch.empty(self.workspace_bytes, dtype=torch.uint8, device=self.device)
             check(lib().fg_plan_bind(self._h, self.workspace.data_ptr(), self.workspace_bytes,
                                      stream_handle(self.device)))
+
+    SHAPE_KEYS = ("kernel", "lanes", "cells_per_thread", "rows_per_tile", "warps_per_block", "stages",
+                  "interior_split", "slab_blocks_per_sm", "persistent")
+
+    def shape(self) -> dict:
+        """The launch shapes the plan chose (fg_plan_shape), host-side:
+        {'forward': {...}, 'adjoint': {...}} with the keys of SHAPE_KEYS."""
+        out = (ctypes.c_int32 * 18)()
+        check(lib().fg_plan_shape(self._h, out))
+        n = len(self.SHAPE_KEYS)
+        return {d: dict(zip(self.SHAPE_KEYS, (int(v) for v in out[k * n:(k + 1) * n])))
+                for k, d in enumerate(("forward", "adjoint"))}
 
     @property
     def handle(self):

@@ -862,6 +862,25 @@ int64_t fg_plan_workspace_bytes(const fg_plan* plan) {
     return (int64_t)(own_bytes(plan) + (plan->adj ? plan->adj->total : 0));
 }
 
+int fg_plan_shape(const fg_plan* plan, int32_t* out) {
+    if (!plan || !out) return fail(FG_ERR_INVALID, "fg_plan_shape: NULL argument");
+    const fg_plan* ps[2] = {plan, plan->adj ? plan->adj : plan};
+    for (int k = 0; k < 2; ++k) {
+        const fg_plan* p = ps[k];
+        int32_t* o = out + 9 * k;
+        o[0] = p->kernel;
+        o[1] = p->pair ? 3 : (p->shot ? 1 : 2);
+        o[2] = p->W;
+        o[3] = p->TI;
+        o[4] = p->WPB;
+        o[5] = p->D;
+        o[6] = p->split ? 1 : 0;
+        o[7] = p->slab_on ? p->slab_bpsm : 0;
+        o[8] = p->persist ? 1 : 0;
+    }
+    return FG_OK;
+}
+
 int fg_plan_hist_shape(const fg_plan* p, int64_t shape[5]) {
     if (!p || !shape) return fail(FG_ERR_INVALID, "fg_plan_hist_shape: NULL argument");
     shape[0] = p->nt;

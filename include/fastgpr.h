@@ -158,6 +158,15 @@ int fg_plan_hist_shape(const fg_plan* plan, int64_t shape[5]);
 /* Device scratch a plan needs (its own and its adjoint plan's), in bytes
  * (>= 0), or -1 on a NULL plan. */
 int64_t fg_plan_workspace_bytes(const fg_plan* plan);
+/* The launch shape a plan chose (host-side, no device work): FG_SHAPE_FIELDS
+ * int32 values, the forward's nine and then the adjoint's nine, each
+ *   kernel (0 tile pipeline, 1 lane march, 2 band pipeline), lanes (1 shot
+ *   lanes, 2 column lanes, 3 shot pairs), cells_per_thread, rows_per_tile,
+ *   warps_per_block, stages, interior split (1 = the interior tiles run in
+ *   their own kernel), slab kernel (its blocks per SM, 0 = off),
+ *   persistent launch (1 = the whole time loop in one launch). */
+#define FG_SHAPE_FIELDS 18
+int fg_plan_shape(const fg_plan* plan, int32_t* out);
 /* Attach a workspace (256-byte aligned device memory of at least
  * fg_plan_workspace_bytes bytes) and upload the plan's tables into it. */
 int fg_plan_bind(fg_plan* plan, void* workspace, int64_t bytes, void* stream);

@@ -102,3 +102,50 @@ def test_checkpoint_sizes_and_adjoint_tuning_without_gpu(fg):
     ok = nat.FgTuning(*([0] * 6 + [2, 3, 2, 0]))      # lane-march adjoint
     assert L.fg_plan_create(ctypes.byref(prob), ctypes.byref(ok), ctypes.byref(h)) == nat.FG_OK
     L.fg_plan_destroy(h)
+
+
+def _shape_of(nat, nx, ny, shots, tuning=None, th=20):
+    """Launch shapes of a plan (host-side) for an nx x ny grid with `shots` shots."""
+    import numpy as np
+    src = np.zeros((shots, 1, 3), np.int32)
+    src[:, 0, 0] = th + 2
+    src[:, 0, 1] = np.arange(shots) % (ny - 2 * th - 4) + th + 2
+    rx = np.zeros((shots, 1, 3), np.int32)
+    rx[:, 0, 0] = nx - th - 3
+    rx[:, 0, 1] = ny // 2
+    p = nat.Plan(nx, ny, shots, 8, th, 0.025, 4e-11, src, rx, np.ones((1, 8), np.float32),
+                 np.zeros(8 * th, np.float32), "cuda:0", tuning=tuning, bind=False)
+    return p.shape()
+
+
+def test_default_launch_shapes_by_step_size(fg):
+    """The size-dependent defaults (host-side, no GPU): interior split from
+    12,000 cells x shot groups; the adjoint's slab kernel at 2 / 1 blocks per
+    SM below 5e4 / 1.2e5; forward tiles of 2 rows below 1.2e5; the adjoint's
+    8 cells per thread from 2e5; column lanes below 8 shots; no split in a
+    persistent plan."""
+    nat = __import__("importlib").import_module("fast-gpr-fwi_b200._native")
+    tiny = _shape_of(nat, 100, 80, 8)                      # 8,000 cells x 1 group
+    assert tiny["forward"]["interior_split"] == 0 and tiny["adjoint"]["interior_split"] == 0
+    assert tiny["forward"]["rows_per_tile"] == 2 and tiny["adjoint"]["rows_per_tile"] == 4
+    small = _shape_of(nat, 140, 100, 16)                   # 14,000
+    assert small["forward"]["interior_split"] == 1 and small["adjoint"]["interior_split"] == 1
+    assert small["forward"]["slab_blocks_per_sm"] == 2 and small["adjoint"]["slab_blocks_per_sm"] == 2
+    assert small["forward"]["rows_per_tile"] == 2 and small["adjoint"]["cells_per_thread"] == 4
+    mid = _shape_of(nat, 296, 296, 32)                     # 87,616
+    assert mid["adjoint"]["slab_blocks_per_sm"] == 1 and mid["forward"]["rows_per_tile"] == 2
+    one_group = _shape_of(nat, 440, 340, 32)               # 149,600
+    assert one_group["adjoint"]["slab_blocks_per_sm"] == 0 and one_group["forward"]["rows_per_tile"] == 4
+    assert one_group["adjoint"]["cells_per_thread"] == 4
+    bench = _shape_of(nat, 440, 340, 64)                   # 299,200: the benchmark grid
+    assert bench["forward"] == dict(kernel=1, lanes=1, cells_per_thread=4, rows_per_tile=4, warps_per_block=4,
+                                    stages=0, interior_split=1, slab_blocks_per_sm=2, persistent=0)
+    assert bench["adjoint"] == dict(kernel=1, lanes=1, cells_per_thread=8, rows_per_tile=4, warps_per_block=4,
+                                    stages=0, interior_split=1, slab_blocks_per_sm=0, persistent=0)
+    pers = _shape_of(nat, 140, 100, 16, tuning={"lanes": 1, "persistent": 1})
+    assert pers["forward"]["persistent"] == 1 and pers["forward"]["interior_split"] == 0
+    assert pers["forward"]["rows_per_tile"] == 4
+    col = _shape_of(nat, 440, 340, 3)
+    assert col["forward"]["lanes"] == 2 and col["forward"]["kernel"] == 0 and col["forward"]["interior_split"] == 0
+    forced = _shape_of(nat, 440, 340, 64, tuning={"interior": -1, "slab": -1})
+    assert forced["forward"]["interior_split"] == 0 and forced["adjoint"]["interior_split"] == 0
