@@ -318,3 +318,30 @@ def test_division_ranges_vs_oracle(fg, orc, dev, scale, dx, tuning):
     oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
     assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
     assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
+
+
+@pytest.mark.parametrize("grid", [(130, 100, 9), (200, 170, 33)])
+def test_default_shapes_on_split_sized_grids_vs_oracle(fg, orc, dev, grid):
+    """The default launch shapes of shot-lane steps of at least 12,000 cells x
+    shot groups (interior split, the adjoint's slab kernel at 2 / 1 blocks
+    per SM, 2-row forward tiles): traces and history bit-exact against the
+    oracle, gradients within 1e-6."""
+    nx, ny, shots = grid
+    wl = fg.workloads.small(seed=nx + ny, nx=nx, ny=ny, shots=shots, nt=40, pml=10, nrx=7, fixed=True)
+    wl.source_step = [0.05, 0.03, 0.0]
+    prob, setup = helpers.oracle_problem_from_gpu(fg, wl, dev)
+    solve = fg.Solve(dev, setup, tv=False)
+    shape = solve.plan.shape()
+    assert shape["forward"]["interior_split"] == 1 and shape["forward"]["rows_per_tile"] == 2
+    assert shape["adjoint"]["interior_split"] == 1 and shape["adjoint"]["slab_blocks_per_sm"] in (1, 2)
+    er, se, mr = (torch.tensor(a, device=dev) for a in (wl.er, wl.se, wl.mr))
+    traces, hist = solve.forward(er, se, mr)
+    o_tr, o_hist = orc.forward(prob, np.float32)
+    np.testing.assert_array_equal(traces.cpu().numpy(), o_tr)
+    np.testing.assert_array_equal(solve.plan.hist_view(hist).cpu().numpy(), o_hist)
+    rng = np.random.default_rng(8)
+    resid = rng.standard_normal(traces.shape).astype(np.float32)
+    ge, gs = solve.gradient(er, se, mr, hist, torch.tensor(resid, device=dev), normalize=False)
+    oe, os_ = orc.adjoint_reference(prob, o_hist, resid, np.float64)
+    assert helpers.rel_l2(ge.cpu().numpy(), oe) < 1e-6
+    assert helpers.rel_l2(gs.cpu().numpy(), os_) < 1e-6
