@@ -38,6 +38,19 @@ cudaError_t launch_adj_core(const Dev& g, int it, int rp, int, int pdl, int* blo
     if (*blocks == 0) {
         const cudaError_t e = persistent_blocks(kernel, 4, 0, g.ntiles - g.core0, blocks);
         if (e != cudaSuccess) return e;
+        // Without a slab kernel, the general kernel on every boundary tile
+        // sets the step's length; interior warps beyond 2 blocks per SM only
+        // take its issue slots (measured, us per adjoint step with at most 2
+        // blocks per SM / as many as fit: 440 x 340, 64 shots 89.3 / 90.5;
+        // 440 x 340, 32 shots 57.5 / 59.6; beside a slab kernel, 296 x 296,
+        // 32 shots 40.5 / 38.9, so the cap applies only without one)
+        if (g.core0 == g.slab0) {
+            int dev = 0, sms = 0;
+            cudaError_t e2 = cudaGetDevice(&dev);
+            if (e2 == cudaSuccess) e2 = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e2 != cudaSuccess) return e2;
+            *blocks = std::max(1, std::min(*blocks, 2 * sms));
+        }
     }
     return launch_core(kernel, *blocks, pdl != 0, st, g, it, rp);
 }
